@@ -1,0 +1,151 @@
+/* B200 backend of the STARS-H TLR approximation path: entry points added by
+ * libstarsh_b200.so beside the STARS-H API in starsh.h.
+ *
+ * The first group has exactly the signatures of the reference's function
+ * pointer types, so a STARS-H build registers them in its dispatch table
+ * (src/control/init.c dlr[][], include/control/init.h:111-190) under
+ * STARSH_BACKEND_B200; the B200 library's own starsh_init() does so
+ * already.  They accept STARSH_blrf/STARSH_problem structures built either
+ * by this library or by the reference library, because the layouts are the
+ * same.  Kernel functions are recognised by symbol name (dladdr), so the
+ * reference's own kernel pointers select the matching device generator;
+ * an unknown kernel pointer is an error (STARSH_WRONG_PARAMETER), there is
+ * no CPU fallback.
+ */
+#ifndef STARSH_B200_H
+#define STARSH_B200_H
+
+#include "starsh.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ----------------------------------------------- drop-in entry points */
+
+/* Randomized-SVD TLR approximation, every step FP64 on the GPU.
+ * Signature of STARSH_blrm_approximate; replaces starsh_blrm__drsdd_omp
+ * (reference src/backends/openmp/blrm/drsdd.c:16-307) and its dense engine
+ * starsh_dense_dlrrsdd (src/backends/sequential/dense/drsdd.c:16-93).
+ * The returned matrix has host factors (alloc_type '1', compact: far_U[i]
+ * is nrows x rank) and keeps a device copy for starsh_blrm__dmml_b200. */
+int starsh_blrm__drsdd_b200(STARSH_blrm **matrix, STARSH_blrf *format,
+        int maxrank, double tol, int onfly);
+
+/* Same contract; the Gaussian sketch Y = D*Omega runs on the tcgen05 tensor
+ * cores in split BF16 (hi/lo parts, three products, FP32 accumulation per
+ * K-chunk, FP64 sum of chunks) with D generated in shared memory.
+ * Orthogonalisation, projection, small SVD and the rank decision are FP64.
+ * Selected by STARSH_LRENGINE=RSVD_MP on the B200 backend. */
+int starsh_blrm__drsdd_b200_mp(STARSH_blrm **matrix, STARSH_blrf *format,
+        int maxrank, double tol, int onfly);
+
+/* B = alpha*M*A + beta*B with host A/B (N x nrhs, cluster order).
+ * Signature and semantics of starsh_blrm__dmml (reference include/
+ * starsh.h:602-603, src/backends/sequential/blrm/dmml.c:16-145); M may come
+ * from the B200 engine (device factors are reused) or from any other
+ * engine (factors are uploaded).  Returns STARSH_SUCCESS or an error. */
+int starsh_blrm__dmml_b200(STARSH_blrm *matrix, int nrhs, double alpha,
+        double *A, int lda, double beta, double *B, int ldb);
+
+/* Relative Frobenius error of M, every block regenerated in FP64 on the GPU
+ * (reference src/backends/sequential/blrm/dfe.c:16-134).  -1 on error. */
+double starsh_blrm__dfe_b200(STARSH_blrm *matrix);
+
+/* ---------------------------------------------- device-resident results */
+
+/* Engine selectors for starsh_b200_approximate(). */
+enum STARSH_B200_ENGINE
+{
+    STARSH_B200_FP64 = 0,   /* starsh_blrm__drsdd_b200 */
+    STARSH_B200_MIXED = 1,  /* starsh_blrm__drsdd_b200_mp */
+};
+
+/* Flags for starsh_b200_approximate(). */
+enum STARSH_B200_FLAGS
+{
+    /* Copy factors and dense blocks to host memory before returning
+     * (the drop-in entry points always set it). */
+    STARSH_B200_HOST_MIRROR = 1,
+};
+
+/* Approximation with an explicit engine and flags.  Without
+ * STARSH_B200_HOST_MIRROR the returned matrix has ranks and shapes on the
+ * host but far_U[i]->data, far_V[i]->data and near_D[i]->data are NULL
+ * until starsh_b200_blrm_download() fills them; the factors stay on the
+ * device for starsh_b200_blrm_dmml_device().  maxrank, tol, onfly and the
+ * in-place update of *format on rank failure are as in
+ * starsh_blrm__drsdd_b200. */
+int starsh_b200_approximate(STARSH_blrm **matrix, STARSH_blrf *format,
+        int maxrank, double tol, int onfly, int engine, int flags);
+
+/* Fills the host mirror of a device-resident matrix (no-op if present). */
+int starsh_b200_blrm_download(STARSH_blrm *matrix);
+
+/* Releases the device copy of M.  starsh_blrm_free() of this library does
+ * it as well; call this one when M is freed by the reference library. */
+void starsh_b200_blrm_release(STARSH_blrm *matrix);
+
+/* dmml with device pointers dA (lda) and dB (ldb) on `stream`
+ * (a cudaStream_t, NULL for the default stream).  Asynchronous. */
+int starsh_b200_blrm_dmml_device(STARSH_blrm *matrix, int nrhs,
+        double alpha, const double *dA, int lda, double beta, double *dB,
+        int ldb, void *stream);
+
+/* ------------------------------------------------- kernel registration */
+
+/* Device kernel families. */
+enum STARSH_B200_FAMILY
+{
+    STARSH_B200_FAMILY_EXP = 1,
+    STARSH_B200_FAMILY_SQREXP = 2,
+    STARSH_B200_FAMILY_MATERN = 3,
+    STARSH_B200_FAMILY_MATERN2 = 4,
+    STARSH_B200_FAMILY_COULOMB = 5,
+    STARSH_B200_FAMILY_SIN = 6,
+    STARSH_B200_FAMILY_COS = 7,
+    STARSH_B200_FAMILY_RBF = 8,
+};
+
+/* Associates a host kernel pointer with a device family.  For
+ * STARSH_B200_FAMILY_COULOMB, `param` is the value of the r = 0 entries
+ * (the reference emits 0; regularised problems use 1).  `param` is ignored
+ * for the other families, whose parameters come from row_data.  Returns
+ * STARSH_SUCCESS, or STARSH_WRONG_PARAMETER when the table is full. */
+int starsh_b200_kernel_register(STARSH_kernel *kernel, int family,
+        double param);
+
+/* Family recognised for `kernel` (0 if none).  For a recognised kernel
+ * *ndim_hint is the dimension fixed by its name (0 for "_nd"). */
+int starsh_b200_kernel_family(STARSH_kernel *kernel, int *ndim_hint);
+
+/* ------------------------------------------------------- diagnostics */
+
+/* Timings and counters of the last approximation on this host thread. */
+typedef struct starsh_b200_stats
+{
+    double total_ms;          /* whole call, host clock                 */
+    double device_ms;         /* device time of the compression phases  */
+    double sketch_ms;         /* device time in the sketch kernels      */
+    double project_ms;        /* device time in the projection kernels  */
+    double sketch_flops;      /* algorithmic flops of the sketch        */
+    double project_flops;     /* flops the projection GEMMs performed   */
+    long long tiles;          /* far-field tiles compressed             */
+    long long false_far;      /* tiles that exceeded maxrank            */
+    long long entries;        /* sum of m*n over all admissible blocks  */
+    long long kernel_launches;/* device kernels launched by the call    */
+    long long rank_sum;       /* sum of accepted ranks                  */
+    int max_rank;             /* largest accepted rank                  */
+    long long h2d_bytes;      /* host to device bytes                   */
+    long long d2h_bytes;      /* device to host bytes                   */
+} starsh_b200_stats;
+int starsh_b200_get_stats(starsh_b200_stats *stats);
+
+/* Last CUDA or watchdog error as text ("" if none). */
+const char *starsh_b200_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,53 @@
+// Process-wide device context of libstarsh_b200: the CUDA stream all work
+// runs on, grow-only device buffers that are reused across calls, the last
+// error string and the statistics of the last approximation.
+#pragma once
+#include <cuda_runtime.h>
+#include <mutex>
+#include <string>
+#include "starsh-b200.h"
+
+namespace b200 {
+
+struct DeviceBuffer {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    // Ensures capacity; contents are not preserved.  Returns false on OOM.
+    bool reserve(size_t need);
+    void release();
+};
+
+struct Context {
+    int device = -1;
+    cudaStream_t stream = nullptr;
+    DeviceBuffer workspace;    // per-slot scratch of the engine
+    DeviceBuffer tiles;        // TileWork array of a batch
+    DeviceBuffer descs;        // GemmDesc array of a batch
+    DeviceBuffer omega;        // Gaussian sketch matrix
+    size_t omega_count = 0;
+    unsigned long long omega_seed = 0;
+    std::mutex lock;           // one approximation / dmml at a time
+};
+
+// Initialises (once) and returns the context; nullptr if no usable GPU.
+Context *context();
+
+// Records a CUDA error (with the call site) as the library's last error and
+// returns the matching STARSH error code.
+int cuda_fail(cudaError_t err, const char *what);
+void set_error(const std::string &msg);
+
+// Statistics of the last approximation on this thread.
+starsh_b200_stats &thread_stats();
+
+// Counts launches of the library's own kernels (for reporting).
+void count_launch(long long n = 1);
+long long launch_count();
+
+}  // namespace b200
+
+#define B200_CUDA(call, what)                                   \
+    do {                                                        \
+        cudaError_t e_ = (call);                                \
+        if (e_ != cudaSuccess) return b200::cuda_fail(e_, what); \
+    } while (0)

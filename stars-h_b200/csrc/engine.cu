@@ -1,0 +1,787 @@
+// Host driver of the B200 TLR approximation: starsh_b200_approximate() and
+// the drop-in entry points, the device-resident matrix records, host
+// mirrors, and the host-callable block generator.
+//
+// Control flow follows starsh_blrm__drsdd_omp (reference
+// src/backends/openmp/blrm/drsdd.c:16-307): compress every far-field block;
+// blocks whose rank exceeds maxrank become near-field blocks and the format
+// is rebuilt and swapped into *format in place (:146-212); near-field
+// blocks are generated densely unless onfly (:214-256); ranks and factors
+// are compacted (:259-282).  The per-block loop runs as batches of tiles
+// through the device pipeline of rsvd_kernels.cu.
+#include <algorithm>
+#include <atomic>
+#include <mutex>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <unordered_map>
+#include <vector>
+
+#include "device_ctx.cuh"
+#include "engine.cuh"
+#include "records.cuh"
+#include "b200_host.h"
+#include "starsh-b200.h"
+
+namespace b200 {
+
+// --------------------------------------------------------------- context
+
+bool DeviceBuffer::reserve(size_t need)
+{
+    if (need <= bytes) return true;
+    release();
+    if (cudaMalloc(&ptr, need) != cudaSuccess) {
+        cudaGetLastError();
+        ptr = nullptr;
+        bytes = 0;
+        return false;
+    }
+    bytes = need;
+    return true;
+}
+
+void DeviceBuffer::release()
+{
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+}
+
+static Context g_ctx;
+static std::once_flag g_ctx_once;
+static bool g_ctx_ok = false;
+static thread_local std::string t_error;
+static thread_local starsh_b200_stats t_stats;
+static std::atomic<long long> g_launches{0};
+
+Context *context()
+{
+    std::call_once(g_ctx_once, [] {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess) {
+            cudaGetLastError();
+            set_error("no CUDA device available");
+            return;
+        }
+        g_ctx.device = dev;
+        if (cudaStreamCreateWithFlags(&g_ctx.stream, cudaStreamNonBlocking)
+                != cudaSuccess) {
+            cudaGetLastError();
+            set_error("cudaStreamCreate failed");
+            return;
+        }
+        g_ctx_ok = true;
+    });
+    return g_ctx_ok ? &g_ctx : nullptr;
+}
+
+void set_error(const std::string &msg)
+{
+    t_error = msg;
+    fprintf(stderr, "STARSH B200 ERROR: %s\n", msg.c_str());
+}
+
+int cuda_fail(cudaError_t err, const char *what)
+{
+    set_error(std::string(what) + ": " + cudaGetErrorString(err));
+    return err == cudaErrorMemoryAllocation ? STARSH_MALLOC_ERROR
+                                            : STARSH_UNKNOWN_ERROR;
+}
+
+starsh_b200_stats &thread_stats() { return t_stats; }
+void count_launch(long long n) { g_launches += n; }
+long long launch_count() { return g_launches.load(); }
+
+// --------------------------------------------------------- device points
+
+void fill_kernel(DevKernel &K, const b200_kspec &sp)
+{
+    K.family = sp.family;
+    K.ndim = sp.ndim;
+    K.aos = sp.aos;
+    K.rbf_kind = sp.rbf_kind;
+    K.isreg = sp.isreg;
+    K.zero_mode = sp.zero_mode;
+    K.sigma = sp.sigma;
+    K.beta = sp.beta;
+    K.nu = sp.nu;
+    K.noise = sp.noise;
+    K.matern_coef = sp.matern_coef;
+    K.matern_scale = sp.matern_scale;
+    K.wave_k = sp.wave_k;
+    K.diag = sp.diag;
+    K.rad = sp.rad;
+    K.reg = sp.reg;
+}
+
+// Uploads the point sets of a problem and the cluster pivots.
+int upload_problem(DevicePoints &dp, STARSH_problem *P,
+                          STARSH_cluster *R, STARSH_cluster *C,
+                          cudaStream_t s)
+{
+    b200_kspec spec;
+    const double *rp, *cp;
+    STARSH_int rc, cc;
+    int info = b200_resolve_kernel(P->kernel, P->row_data, &spec, &rp, &rc,
+                                   &cp, &cc, P->col_data);
+    if (info != STARSH_SUCCESS) return info;
+    fill_kernel(dp.K, spec);
+    const void *d;
+    const size_t per = (size_t)spec.ndim * sizeof(double);
+    if ((info = dp.upload(rp, rc * per, &d, s))) return info;
+    dp.K.row_pt = (const double *)d;
+    dp.K.row_count = rc;
+    if (cp == rp && cc == rc) {
+        dp.K.col_pt = dp.K.row_pt;
+    } else {
+        if ((info = dp.upload(cp, cc * per, &d, s))) return info;
+        dp.K.col_pt = (const double *)d;
+    }
+    dp.K.col_count = cc;
+    if ((info = dp.upload(R->pivot, R->ndata * sizeof(STARSH_int), &d, s)))
+        return info;
+    dp.K.row_piv = (const long long *)d;
+    if (C == R) {
+        dp.K.col_piv = dp.K.row_piv;
+    } else {
+        if ((info = dp.upload(C->pivot, C->ndata * sizeof(STARSH_int), &d, s)))
+            return info;
+        dp.K.col_piv = (const long long *)d;
+    }
+    return STARSH_SUCCESS;
+}
+
+// ---------------------------------------------------- dense block writer
+
+__global__ void k_gen_blocks(DevKernel K, const BlockJob *__restrict__ jobs)
+{
+    const BlockJob jb = jobs[blockIdx.z];
+    const int i = blockIdx.x * 64 + (threadIdx.x & 63);
+    const int j0 = blockIdx.y * 64 + (threadIdx.x >> 6);
+    if (i >= jb.m) return;
+    for (int c = 0; c < 16; ++c) {
+        const int j = j0 + 4 * c;
+        if (j < jb.n)
+            jb.out[(size_t)j * jb.m + i] = block_entry(K, jb.row0, jb.col0, i, j);
+    }
+}
+
+int gen_blocks(const DevKernel &K, const std::vector<BlockJob> &jobs,
+                      cudaStream_t s)
+{
+    if (jobs.empty()) return STARSH_SUCCESS;
+    int mmax = 0, nmax = 0;
+    for (const auto &j : jobs) {
+        mmax = std::max(mmax, j.m);
+        nmax = std::max(nmax, j.n);
+    }
+    BlockJob *dj = nullptr;
+    B200_CUDA(cudaMallocAsync((void **)&dj, jobs.size() * sizeof(BlockJob), s),
+              "cudaMallocAsync(jobs)");
+    cudaMemcpyAsync(dj, jobs.data(), jobs.size() * sizeof(BlockJob),
+                    cudaMemcpyHostToDevice, s);
+    for (size_t b0 = 0; b0 < jobs.size(); b0 += 65535) {
+        const unsigned nb = (unsigned)std::min<size_t>(65535, jobs.size() - b0);
+        dim3 grid((mmax + 63) / 64, (nmax + 63) / 64, nb);
+        k_gen_blocks<<<grid, 256, 0, s>>>(K, dj + b0);
+        count_launch();
+    }
+    cudaFreeAsync(dj, s);
+    B200_CUDA(cudaGetLastError(), "k_gen_blocks");
+    return STARSH_SUCCESS;
+}
+
+// ------------------------------------------------------ device records
+
+static std::mutex g_rec_lock;
+static std::unordered_map<const STARSH_blrm *, Record *> g_records;
+
+void add_record(const STARSH_blrm *M, Record *rec)
+{
+    std::lock_guard<std::mutex> g(g_rec_lock);
+    g_records[M] = rec;
+}
+
+Record *find_record(const STARSH_blrm *M)
+{
+    std::lock_guard<std::mutex> g(g_rec_lock);
+    auto it = g_records.find(M);
+    return it == g_records.end() ? nullptr : it->second;
+}
+
+// -------------------------------------------------------------- engine
+
+static const unsigned long long kOmegaSeed = 0x5354415253480001ull;
+
+struct EngineParams {
+    int maxrank;
+    double tol;
+    int oversample;
+    int engine;
+};
+
+// Runs the device pipeline over all far blocks of F.  Fills ranks (host)
+// and per-block device pointers of U and V inside `rec`.
+static int compress_far(Context &ctx, const DevKernel &K, STARSH_blrf *F,
+                        const EngineParams &ep, std::vector<int> &rank,
+                        Record &rec)
+{
+    cudaStream_t s = ctx.stream;
+    STARSH_cluster *R = F->row_cluster, *C = F->col_cluster;
+    const STARSH_int nfar = F->nblocks_far;
+    rank.assign(nfar, 0);
+    rec.dU.assign(nfar, nullptr);
+    rec.dV.assign(nfar, nullptr);
+    if (nfar == 0) return STARSH_SUCCESS;
+    starsh_b200_stats &st = thread_stats();
+
+    std::vector<TileWork> all(nfar);
+    int m_max = 0, n_max = 0, k_max = 0;
+    for (STARSH_int b = 0; b < nfar; ++b) {
+        const STARSH_int i = F->block_far[2 * b], j = F->block_far[2 * b + 1];
+        TileWork &t = all[b];
+        memset(&t, 0, sizeof(t));
+        t.row0 = R->start[i];
+        t.col0 = C->start[j];
+        t.m = (int)R->size[i];
+        t.n = (int)C->size[j];
+        t.k = std::min(ep.maxrank + ep.oversample, std::min(t.m, t.n));
+        m_max = std::max(m_max, t.m);
+        n_max = std::max(n_max, t.n);
+        k_max = std::max(k_max, t.k);
+        st.entries += (long long)t.m * t.n;
+    }
+    if (k_max > 1024) {
+        set_error("maxrank + oversample above 1024 is not supported");
+        return STARSH_WRONG_PARAMETER;
+    }
+    // Gaussian sketch, shared by every tile (as the reference reuses the
+    // same iseed for every block): n_max x k_max, ld n_max.
+    const size_t om_count = (size_t)n_max * k_max;
+    if (ctx.omega_count != om_count || ctx.omega_seed != kOmegaSeed) {
+        if (!ctx.omega.reserve(om_count * sizeof(double)))
+            return cuda_fail(cudaErrorMemoryAllocation, "omega");
+        launch_gaussian((double *)ctx.omega.ptr, (long long)om_count,
+                        kOmegaSeed, s);
+        count_launch();
+        ctx.omega_count = om_count;
+        ctx.omega_seed = kOmegaSeed;
+    }
+    const double *omega = (const double *)ctx.omega.ptr;
+
+    Workspace ws{};
+    const size_t stride = workspace_layout(ws, m_max, n_max, k_max, true);
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    size_t budget = std::min<size_t>(free_b / 2, (size_t)24 << 30);
+    if (const char *e = getenv("STARSH_B200_WORKSPACE_MB"))
+        budget = std::min<size_t>(budget, (size_t)atoll(e) << 20);
+    long long slots = (long long)(budget / (stride * sizeof(double)));
+    slots = std::max<long long>(1, std::min<long long>(slots, nfar));
+    slots = std::min<long long>(slots, 4096);
+    if (!ctx.workspace.reserve((size_t)slots * stride * sizeof(double)))
+        return cuda_fail(cudaErrorMemoryAllocation, "workspace");
+    ws.base = (double *)ctx.workspace.ptr;
+    ws.stride = stride;
+    if (!ctx.tiles.reserve((size_t)slots * sizeof(TileWork)) ||
+        !ctx.descs.reserve((size_t)slots * sizeof(GemmDesc)))
+        return cuda_fail(cudaErrorMemoryAllocation, "batch arrays");
+    TileWork *dt = (TileWork *)ctx.tiles.ptr;
+    GemmDesc *dd = (GemmDesc *)ctx.descs.ptr;
+
+    cudaEvent_t ev[4];
+    for (auto &e : ev) cudaEventCreate(&e);
+    OutArena none{nullptr, nullptr};
+    int info = STARSH_SUCCESS;
+
+    auto gemm = [&](GemmStep step, bool ta, bool tb, int nt, int mm, int nn,
+                    OutArena out) -> int {
+        make_gemm_descs(step, dt, nt, ws, omega, n_max, out, dd, s);
+        count_launch(2);
+        return gemm_f64_batched(ta, tb, dd, nt, mm, nn, s) == cudaSuccess
+                   ? STARSH_SUCCESS
+                   : cuda_fail(cudaGetLastError(), "gemm_f64_batched");
+    };
+
+    for (STARSH_int b0 = 0; b0 < nfar && info == STARSH_SUCCESS; b0 += slots) {
+        const int nt = (int)std::min<STARSH_int>(slots, nfar - b0);
+        for (int t = 0; t < nt; ++t) all[b0 + t].slot = t;
+        cudaMemcpyAsync(dt, &all[b0], nt * sizeof(TileWork),
+                        cudaMemcpyHostToDevice, s);
+        launch_gen_tiles(K, dt, nt, ws, s);
+        count_launch();
+        cudaEventRecord(ev[0], s);
+        if ((info = gemm(STEP_SKETCH, false, false, nt, m_max, k_max, none))) break;
+        cudaEventRecord(ev[1], s);
+        // basis: pass A
+        if ((info = gemm(STEP_GRAM_Y, true, false, nt, k_max, k_max, none))) break;
+        launch_pivchol(0, dt, dt, nt, ws, ep.tol, s);
+        launch_gather_cols(0, dt, nt, ws, s);
+        count_launch(2);
+        if ((info = gemm(STEP_Q1, false, false, nt, m_max, k_max, none))) break;
+        if ((info = gemm(STEP_GRAM_Q1, true, false, nt, k_max, k_max, none))) break;
+        launch_chol_inv(0, dt, nt, ws, s);
+        count_launch();
+        if ((info = gemm(STEP_Q, false, false, nt, m_max, k_max, none))) break;
+        // basis: pass B (tiles that do not need it have empty GEMMs)
+        if ((info = gemm(STEP_RES_Z, true, false, nt, k_max, k_max, none))) break;
+        if ((info = gemm(STEP_RES_Y, false, false, nt, m_max, k_max, none))) break;
+        if ((info = gemm(STEP_GRAM_YR, true, false, nt, k_max, k_max, none))) break;
+        launch_pivchol(1, dt, dt, nt, ws, ep.tol, s);
+        launch_gather_cols(1, dt, nt, ws, s);
+        count_launch(2);
+        if ((info = gemm(STEP_Q1B, false, false, nt, m_max, k_max, none))) break;
+        if ((info = gemm(STEP_RES_Z2, true, false, nt, k_max, k_max, none))) break;
+        if ((info = gemm(STEP_RES_Q1B, false, false, nt, m_max, k_max, none))) break;
+        if ((info = gemm(STEP_GRAM_Q1B, true, false, nt, k_max, k_max, none))) break;
+        launch_chol_inv(1, dt, nt, ws, s);
+        count_launch();
+        if ((info = gemm(STEP_QB, false, false, nt, m_max, k_max, none))) break;
+        launch_merge_basis(dt, nt, s);
+        count_launch();
+        // projection and small SVD
+        cudaEventRecord(ev[2], s);
+        if ((info = gemm(STEP_PROJECT, true, false, nt, k_max, n_max, none))) break;
+        cudaEventRecord(ev[3], s);
+        if ((info = gemm(STEP_GRAM_B, false, true, nt, k_max, k_max, none))) break;
+        launch_pivchol(2, dt, dt, nt, ws, ep.tol, s);
+        launch_jacobi(dt, nt, ws, s);
+        count_launch(2);
+        if ((info = gemm(STEP_ROTATE, true, false, nt, k_max, n_max, none))) break;
+        launch_rank_cut(dt, nt, ws, ep.tol, ep.maxrank, s);
+        count_launch();
+        B200_CUDA(cudaMemcpyAsync(&all[b0], dt, nt * sizeof(TileWork),
+                                  cudaMemcpyDeviceToHost, s),
+                  "cudaMemcpyAsync(tiles)");
+        B200_CUDA(cudaStreamSynchronize(s), "compression pipeline");
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ev[0], ev[1]);
+        st.sketch_ms += ms;
+        cudaEventElapsedTime(&ms, ev[2], ev[3]);
+        st.project_ms += ms;
+        // Output placement of this batch: one device chunk for U and V.
+        size_t nu = 0, nv = 0;
+        for (int t = 0; t < nt; ++t) {
+            TileWork &w = all[b0 + t];
+            st.sketch_flops += 2.0 * w.m * w.n * w.k;
+            st.project_flops += 2.0 * w.m * w.n * w.k1;
+            if (w.status & TILE_CHOL_FAIL) {
+                set_error("re-orthogonalisation failed on a tile");
+                info = STARSH_UNKNOWN_ERROR;
+            }
+            rank[b0 + t] = w.rank;
+            if (w.rank > 0) {
+                w.off_u = (long long)nu;
+                w.off_v = (long long)nv;
+                nu += (size_t)w.m * w.rank;
+                nv += (size_t)w.n * w.rank;
+            }
+        }
+        if (info) break;
+        double *chunk = nullptr;
+        if (nu + nv > 0) {
+            B200_CUDA(cudaMalloc(&chunk, (nu + nv) * sizeof(double)),
+                      "cudaMalloc(factors)");
+            rec.chunks.push_back(chunk);
+        }
+        OutArena out{chunk, chunk ? chunk + nu : nullptr};
+        for (int t = 0; t < nt; ++t) {
+            const TileWork &w = all[b0 + t];
+            if (w.rank > 0) {
+                rec.dU[b0 + t] = out.U + w.off_u;
+                rec.dV[b0 + t] = out.V + w.off_v;
+            }
+        }
+        rec.u_total += nu;
+        rec.v_total += nv;
+        if (nu + nv > 0) {
+            cudaMemcpyAsync(dt, &all[b0], nt * sizeof(TileWork),
+                            cudaMemcpyHostToDevice, s);
+            launch_select_w(dt, nt, ws, s);
+            count_launch();
+            if ((info = gemm(STEP_OUT_U, false, false, nt, m_max, k_max, out))) break;
+            launch_write_v(dt, nt, ws, out, s);
+            count_launch();
+        }
+        st.tiles += nt;
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
+    if (info == STARSH_SUCCESS)
+        B200_CUDA(cudaStreamSynchronize(s), "factor output");
+    return info;
+}
+
+// Host Array view helper (shape m x n, column-major).
+static int make_view(Array **A, int m, int n, double *data)
+{
+    int shape[2] = {m, n};
+    return array_from_buffer(A, 2, shape, 'd', 'F', data);
+}
+
+static int fill_host_mirror(STARSH_blrm *M, Record &rec, cudaStream_t s)
+{
+    if (rec.host_filled) return STARSH_SUCCESS;
+    STARSH_blrf *F = M->format;
+    starsh_b200_stats &st = thread_stats();
+    double *hU = (double *)malloc(std::max<size_t>(rec.u_total, 1) * sizeof(double));
+    double *hV = (double *)malloc(std::max<size_t>(rec.v_total, 1) * sizeof(double));
+    double *hD = nullptr;
+    if (!hU || !hV) {
+        free(hU);
+        free(hV);
+        return STARSH_MALLOC_ERROR;
+    }
+    size_t ou = 0, ov = 0;
+    for (STARSH_int b = 0; b < F->nblocks_far; ++b) {
+        const int r = M->far_rank[b];
+        const size_t nu = (size_t)M->far_U[b]->shape[0] * r;
+        const size_t nv = (size_t)M->far_V[b]->shape[0] * r;
+        if (r > 0) {
+            cudaMemcpyAsync(hU + ou, rec.dU[b], nu * sizeof(double),
+                            cudaMemcpyDeviceToHost, s);
+            cudaMemcpyAsync(hV + ov, rec.dV[b], nv * sizeof(double),
+                            cudaMemcpyDeviceToHost, s);
+        }
+        M->far_U[b]->data = hU + ou;
+        M->far_V[b]->data = hV + ov;
+        ou += nu;
+        ov += nv;
+    }
+    if (M->onfly == 0 && F->nblocks_near > 0) {
+        hD = (double *)malloc(std::max<size_t>(rec.d_total, 1) * sizeof(double));
+        if (!hD) {
+            free(hU);
+            free(hV);
+            return STARSH_MALLOC_ERROR;
+        }
+        size_t od = 0;
+        for (STARSH_int b = 0; b < F->nblocks_near; ++b) {
+            const size_t nd = M->near_D[b]->size;
+            cudaMemcpyAsync(hD + od, rec.dD[b], nd * sizeof(double),
+                            cudaMemcpyDeviceToHost, s);
+            M->near_D[b]->data = hD + od;
+            od += nd;
+        }
+    }
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        free(hU);
+        free(hV);
+        free(hD);
+        return cuda_fail(e, "host mirror copy");
+    }
+    st.d2h_bytes += (long long)(rec.u_total + rec.v_total + rec.d_total) * 8;
+    M->alloc_U = hU;
+    M->alloc_V = hV;
+    M->alloc_D = hD;
+    rec.host_filled = true;
+    return STARSH_SUCCESS;
+}
+
+static int approximate(STARSH_blrm **matrix, STARSH_blrf *F, int maxrank,
+                       double tol, int onfly, int engine, int flags)
+{
+    auto t_start = std::chrono::steady_clock::now();
+    starsh_b200_stats &st = thread_stats();
+    memset(&st, 0, sizeof(st));
+    const long long launches0 = launch_count();
+    if (matrix == nullptr || F == nullptr || maxrank < 0 || !(tol >= 0.0) ||
+        (onfly != 0 && onfly != 1)) {
+        set_error("invalid argument");
+        return STARSH_WRONG_PARAMETER;
+    }
+    if (engine != STARSH_B200_FP64) {
+        set_error("engine not available in this build");
+        return STARSH_WRONG_PARAMETER;
+    }
+    Context *ctx = context();
+    if (!ctx) return STARSH_UNKNOWN_ERROR;
+    std::lock_guard<std::mutex> guard(ctx->lock);
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    STARSH_problem *P = F->problem;
+    STARSH_cluster *R = F->row_cluster, *C = F->col_cluster;
+    if (P == nullptr || R == nullptr || C == nullptr || P->ndim != 2 ||
+        P->dtype != 'd') {
+        set_error("only scalar double-precision problems are supported");
+        return STARSH_WRONG_PARAMETER;
+    }
+
+    auto *points = new DevicePoints();
+    int info = upload_problem(*points, P, R, C, s);
+    if (info) {
+        delete points;
+        return info;
+    }
+    st.h2d_bytes += points->h2d;
+    auto *rec = new Record();
+    rec->points = points;
+    std::vector<int> rank;
+    EngineParams ep{maxrank, tol, b200_oversample(), engine};
+    info = compress_far(*ctx, points->K, F, ep, rank, *rec);
+    if (info) {
+        delete rec;
+        return info;
+    }
+
+    // False far-field blocks (rank -1) become near-field; the format is
+    // rebuilt and swapped into *F, the old lists freed.
+    const STARSH_int nfar = F->nblocks_far, nnear = F->nblocks_near;
+    std::vector<STARSH_int> keep, demote;
+    for (STARSH_int b = 0; b < nfar; ++b)
+        (rank[b] < 0 ? demote : keep).push_back(b);
+    st.false_far = (long long)demote.size();
+    std::vector<double *> dU, dV;
+    std::vector<int> far_rank;
+    for (STARSH_int b : keep) {
+        dU.push_back(rec->dU[b]);
+        dV.push_back(rec->dV[b]);
+        far_rank.push_back(rank[b]);
+        st.rank_sum += rank[b];
+        st.max_rank = std::max(st.max_rank, rank[b]);
+    }
+    if (!demote.empty()) {
+        const STARSH_int new_near = nnear + (STARSH_int)demote.size();
+        const STARSH_int new_far = (STARSH_int)keep.size();
+        STARSH_int *bn = (STARSH_int *)malloc(sizeof(STARSH_int) * 2 * new_near);
+        STARSH_int *bf = new_far > 0
+            ? (STARSH_int *)malloc(sizeof(STARSH_int) * 2 * new_far) : nullptr;
+        if (!bn || (new_far > 0 && !bf)) {
+            free(bn);
+            free(bf);
+            delete rec;
+            return STARSH_MALLOC_ERROR;
+        }
+        for (STARSH_int b = 0; b < 2 * nnear; ++b) bn[b] = F->block_near[b];
+        for (size_t q = 0; q < demote.size(); ++q) {
+            bn[2 * (nnear + q)] = F->block_far[2 * demote[q]];
+            bn[2 * (nnear + q) + 1] = F->block_far[2 * demote[q] + 1];
+        }
+        for (size_t q = 0; q < keep.size(); ++q) {
+            bf[2 * q] = F->block_far[2 * keep[q]];
+            bf[2 * q + 1] = F->block_far[2 * keep[q] + 1];
+        }
+        STARSH_blrf *F2 = nullptr;
+        info = starsh_blrf_new_from_coo(&F2, P, F->symm, R, C, new_far, bf,
+                                        new_near, bn, F->type);
+        if (info) {
+            free(bn);
+            free(bf);
+            delete rec;
+            return info;
+        }
+        STARSH_blrf tmp = *F;
+        *F = *F2;
+        *F2 = tmp;
+        starsh_blrf_free(F2);
+    }
+    rec->dU = dU;
+    rec->dV = dV;
+
+    // Near-field blocks: dense on the device unless onfly.
+    const STARSH_int near = F->nblocks_near;
+    rec->dD.assign(near, nullptr);
+    if (onfly == 0 && near > 0) {
+        size_t total = 0;
+        for (STARSH_int b = 0; b < near; ++b)
+            total += (size_t)R->size[F->block_near[2 * b]] *
+                     C->size[F->block_near[2 * b + 1]];
+        double *dD = nullptr;
+        cudaError_t e = cudaMalloc(&dD, total * sizeof(double));
+        if (e != cudaSuccess) {
+            delete rec;
+            return cuda_fail(e, "cudaMalloc(near blocks)");
+        }
+        rec->chunks.push_back(dD);
+        rec->d_total = total;
+        std::vector<BlockJob> jobs;
+        size_t off = 0;
+        for (STARSH_int b = 0; b < near; ++b) {
+            const STARSH_int i = F->block_near[2 * b], j = F->block_near[2 * b + 1];
+            BlockJob jb{R->start[i], C->start[j], (int)R->size[i],
+                        (int)C->size[j], dD + off};
+            rec->dD[b] = dD + off;
+            jobs.push_back(jb);
+            off += (size_t)jb.m * jb.n;
+            st.entries += (long long)jb.m * jb.n;
+        }
+        if ((info = gen_blocks(points->K, jobs, s))) {
+            delete rec;
+            return info;
+        }
+    } else {
+        for (STARSH_int b = 0; b < near; ++b)
+            st.entries += (long long)R->size[F->block_near[2 * b]] *
+                          C->size[F->block_near[2 * b + 1]];
+    }
+
+    // Host STARSH_blrm with views (data filled by the host mirror).
+    const STARSH_int nf = F->nblocks_far;
+    int *fr = nf > 0 ? (int *)malloc(sizeof(int) * nf) : nullptr;
+    Array **fU = nf > 0 ? (Array **)calloc(nf, sizeof(Array *)) : nullptr;
+    Array **fV = nf > 0 ? (Array **)calloc(nf, sizeof(Array *)) : nullptr;
+    Array **nD = (onfly == 0 && near > 0)
+                     ? (Array **)calloc(near, sizeof(Array *)) : nullptr;
+    for (STARSH_int b = 0; b < nf; ++b) {
+        fr[b] = far_rank[b];
+        const int m = (int)R->size[F->block_far[2 * b]];
+        const int n = (int)C->size[F->block_far[2 * b + 1]];
+        make_view(&fU[b], m, fr[b], nullptr);
+        make_view(&fV[b], n, fr[b], nullptr);
+    }
+    for (STARSH_int b = 0; nD && b < near; ++b) {
+        const int m = (int)R->size[F->block_near[2 * b]];
+        const int n = (int)C->size[F->block_near[2 * b + 1]];
+        make_view(&nD[b], m, n, nullptr);
+    }
+    STARSH_blrm *M = nullptr;
+    info = starsh_blrm_new(&M, F, fr, fU, fV, onfly, nD, nullptr, nullptr,
+                           nullptr, '1');
+    if (info) {
+        delete rec;
+        return info;
+    }
+    add_record(M, rec);
+    if (flags & STARSH_B200_HOST_MIRROR) {
+        info = fill_host_mirror(M, *rec, s);
+        if (info) return info;
+    } else {
+        B200_CUDA(cudaStreamSynchronize(s), "near blocks");
+    }
+    *matrix = M;
+    st.kernel_launches = launch_count() - launches0;
+    st.device_ms = st.sketch_ms + st.project_ms;
+    st.total_ms = std::chrono::duration<double, std::milli>(
+                      std::chrono::steady_clock::now() - t_start).count();
+    return STARSH_SUCCESS;
+}
+
+}  // namespace b200
+
+using namespace b200;
+
+// ------------------------------------------------------------ C entries
+
+extern "C" int starsh_b200_approximate(STARSH_blrm **matrix,
+                                       STARSH_blrf *format, int maxrank,
+                                       double tol, int onfly, int engine,
+                                       int flags)
+{
+    return approximate(matrix, format, maxrank, tol, onfly, engine, flags);
+}
+
+extern "C" int starsh_blrm__drsdd_b200(STARSH_blrm **matrix,
+                                       STARSH_blrf *format, int maxrank,
+                                       double tol, int onfly)
+{
+    return approximate(matrix, format, maxrank, tol, onfly, STARSH_B200_FP64,
+                       STARSH_B200_HOST_MIRROR);
+}
+
+extern "C" int starsh_blrm__drsdd_b200_mp(STARSH_blrm **matrix,
+                                          STARSH_blrf *format, int maxrank,
+                                          double tol, int onfly)
+{
+    return approximate(matrix, format, maxrank, tol, onfly, STARSH_B200_MIXED,
+                       STARSH_B200_HOST_MIRROR);
+}
+
+extern "C" int starsh_b200_blrm_download(STARSH_blrm *matrix)
+{
+    if (matrix == nullptr) return STARSH_WRONG_PARAMETER;
+    Record *rec = find_record(matrix);
+    if (rec == nullptr || rec->host_filled) return STARSH_SUCCESS;
+    Context *ctx = context();
+    if (!ctx) return STARSH_UNKNOWN_ERROR;
+    std::lock_guard<std::mutex> guard(ctx->lock);
+    return fill_host_mirror(matrix, *rec, ctx->stream);
+}
+
+extern "C" void starsh_b200_blrm_release(STARSH_blrm *matrix)
+{
+    Record *rec = nullptr;
+    {
+        std::lock_guard<std::mutex> g(g_rec_lock);
+        auto it = g_records.find(matrix);
+        if (it == g_records.end()) return;
+        rec = it->second;
+        g_records.erase(it);
+    }
+    Context *ctx = context();
+    if (ctx) cudaStreamSynchronize(ctx->stream);
+    delete rec;
+}
+
+extern "C" int starsh_b200_get_stats(starsh_b200_stats *stats)
+{
+    if (stats == nullptr) return STARSH_WRONG_PARAMETER;
+    *stats = thread_stats();
+    return STARSH_SUCCESS;
+}
+
+extern "C" const char *starsh_b200_last_error(void)
+{
+    return t_error.c_str();
+}
+
+// Host-callable kernel entry points: the block is generated on the GPU from
+// caller-given row and column index lists and copied back.
+extern "C" void b200_eval_block_host(STARSH_kernel *kernel, int nrows,
+                                     int ncols, STARSH_int *irow,
+                                     STARSH_int *icol, void *row_data,
+                                     void *col_data, double *result, int ld)
+{
+    if (nrows <= 0 || ncols <= 0) return;
+    Context *ctx = context();
+    if (!ctx) {
+        fprintf(stderr, "STARSH B200: kernel called without a GPU\n");
+        abort();
+    }
+    std::lock_guard<std::mutex> guard(ctx->lock);
+    cudaStream_t s = ctx->stream;
+    b200_kspec spec;
+    const double *rp, *cp;
+    STARSH_int rc, cc;
+    if (b200_resolve_kernel(kernel, row_data, &spec, &rp, &rc, &cp, &cc,
+                            col_data) != STARSH_SUCCESS) {
+        fprintf(stderr, "STARSH B200: unrecognised kernel\n");
+        abort();
+    }
+    DevicePoints dp;
+    fill_kernel(dp.K, spec);
+    const void *d;
+    const size_t per = (size_t)spec.ndim * sizeof(double);
+    int info = dp.upload(rp, rc * per, &d, s);
+    dp.K.row_pt = (const double *)d;
+    dp.K.row_count = rc;
+    if (!info) info = dp.upload(cp, cc * per, &d, s);
+    dp.K.col_pt = (const double *)d;
+    dp.K.col_count = cc;
+    if (!info) info = dp.upload(irow, nrows * sizeof(STARSH_int), &d, s);
+    dp.K.row_piv = (const long long *)d;
+    if (!info) info = dp.upload(icol, ncols * sizeof(STARSH_int), &d, s);
+    dp.K.col_piv = (const long long *)d;
+    double *out = nullptr;
+    if (!info && cudaMalloc(&out, (size_t)nrows * ncols * sizeof(double)) !=
+                     cudaSuccess)
+        info = STARSH_MALLOC_ERROR;
+    if (!info) {
+        std::vector<BlockJob> jobs{BlockJob{0, 0, nrows, ncols, out}};
+        info = gen_blocks(dp.K, jobs, s);
+    }
+    if (!info)
+        info = cudaMemcpy2DAsync(result, (size_t)ld * sizeof(double), out,
+                                 (size_t)nrows * sizeof(double),
+                                 (size_t)nrows * sizeof(double), ncols,
+                                 cudaMemcpyDeviceToHost, s) == cudaSuccess
+                   ? cudaStreamSynchronize(s) : STARSH_UNKNOWN_ERROR;
+    if (out) cudaFree(out);
+    if (info) {
+        fprintf(stderr, "STARSH B200: block generation failed: %s\n",
+                t_error.c_str());
+        abort();
+    }
+}

@@ -1,0 +1,117 @@
+// Shared definitions of the batched randomized-SVD engine: per-tile state,
+// workspace layout and the launchers of the per-tile kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include "gemm_f64.cuh"
+#include "kernel_entry.cuh"
+
+namespace b200 {
+
+// Status bits of a tile.
+enum : int {
+    TILE_OK = 0,
+    TILE_CHOL_FAIL = 1,    // Cholesky of a re-orthogonalisation Gram failed
+    TILE_JACOBI_SLOW = 2,  // Jacobi sweeps hit their cap
+    TILE_TAIL_LEFT = 4,    // deflated energy alone exceeded the tolerance
+};
+
+// One far-field tile of a batch.
+struct TileWork {
+    long long row0, col0;   // offsets into the row/column cluster pivots
+    int m, n, k;            // block shape and sketch width
+    int slot;               // workspace slot
+    int k1;                 // orthonormal basis columns after deflation
+    int kb;                 // columns added by the residual pass
+    int k2;                 // Gram factor columns for the small SVD
+    int rank;               // accepted rank, or -1 (false far-field)
+    int status;
+    int need_pass_b;        // residual pass required by tol
+    double tr_g;            // trace of the sketch Gram Y^T Y
+    double tr_h;            // ||B||_F^2 = trace of B B^T
+    long long off_u, off_v; // output offsets (doubles)
+};
+
+// Per-slot workspace.  All matrices are column-major with the leading
+// dimensions below; ints live in double-sized cells.
+struct Workspace {
+    double *base;
+    size_t stride;          // doubles per slot
+    int m_max, n_max, k_max;
+    size_t oD, oY, oQ1, oQ, oS, oL, oT, oB, oC, oE, oSig, oPiv, oOrd;
+
+    __host__ __device__ double *D(int s) const { return base + s * stride + oD; }
+    __host__ __device__ double *Y(int s) const { return base + s * stride + oY; }
+    __host__ __device__ double *Q1(int s) const { return base + s * stride + oQ1; }
+    __host__ __device__ double *Q(int s) const { return base + s * stride + oQ; }
+    __host__ __device__ double *S(int s) const { return base + s * stride + oS; }
+    __host__ __device__ double *L(int s) const { return base + s * stride + oL; }
+    __host__ __device__ double *T(int s) const { return base + s * stride + oT; }
+    __host__ __device__ double *B(int s) const { return base + s * stride + oB; }
+    __host__ __device__ double *C(int s) const { return base + s * stride + oC; }
+    __host__ __device__ double *E(int s) const { return base + s * stride + oE; }
+    __host__ __device__ double *Sig(int s) const { return base + s * stride + oSig; }
+    __host__ __device__ int *Piv(int s) const { return (int *)(base + s * stride + oPiv); }
+    __host__ __device__ int *Ord(int s) const { return (int *)(base + s * stride + oOrd); }
+    // leading dimensions
+    __host__ __device__ int ldD() const { return m_max; }
+    __host__ __device__ int ldM() const { return m_max; }   // Y, Q1, Q
+    __host__ __device__ int ldK() const { return k_max; }   // S, L, T, B, C
+};
+
+// Layout for the given maxima; returns doubles per slot.
+size_t workspace_layout(Workspace &w, int m_max, int n_max, int k_max,
+                        bool store_d);
+
+// GEMM steps of the pipeline, each turned into descriptors on the device.
+enum GemmStep : int {
+    STEP_SKETCH = 0,     // Y  = D Omega                  (m x k)
+    STEP_GRAM_Y,         // S  = Y^T Y                    (k x k)
+    STEP_Q1,             // Q1 = Yg T                     (m x k1)
+    STEP_GRAM_Q1,        // S  = Q1^T Q1                  (k1 x k1)
+    STEP_Q,              // Q  = Q1 T                     (m x k1)
+    STEP_RES_Z,          // S  = Q^T Y                    (k1 x k)   pass B
+    STEP_RES_Y,          // Y -= Q S                      (m x k)    pass B
+    STEP_GRAM_YR,        // S  = Y^T Y of the residual    (k x k)    pass B
+    STEP_Q1B,            // Q1 = Yg T                     (m x kb)   pass B
+    STEP_RES_Z2,         // S  = Q^T Q1                   (k1 x kb)  pass B
+    STEP_RES_Q1B,        // Q1 -= Q S                     (m x kb)   pass B
+    STEP_GRAM_Q1B,       // S  = Q1^T Q1                  (kb x kb)  pass B
+    STEP_QB,             // Q[:, k1:] = Q1 T              (m x kb)   pass B
+    STEP_PROJECT,        // B  = Q^T D                    (k1 x n)
+    STEP_GRAM_B,         // S  = B B^T                    (k1 x k1)
+    STEP_ROTATE,         // C  = W^T B   (W in T)         (k2 x n)
+    STEP_OUT_U,          // U  = Q Wsel  (Wsel in L)      (m x r)
+};
+
+struct OutArena {
+    double *U;
+    double *V;
+};
+
+// Builds the descriptors of `step` for every tile of the batch.
+void make_gemm_descs(GemmStep step, const TileWork *d_tiles, int ntiles,
+                     Workspace ws, const double *d_omega, int ld_omega,
+                     OutArena out, GemmDesc *d_desc, cudaStream_t stream);
+
+// Per-tile kernels (one CTA per tile).
+void launch_gen_tiles(const DevKernel &K, const TileWork *d_tiles,
+                      int ntiles, Workspace ws, cudaStream_t stream);
+void launch_pivchol(int phase, const TileWork *d_tiles, TileWork *d_tiles_rw,
+                    int ntiles, Workspace ws, double tol, cudaStream_t s);
+void launch_gather_cols(int phase, const TileWork *d_tiles, int ntiles,
+                        Workspace ws, cudaStream_t stream);
+void launch_chol_inv(int phase, TileWork *d_tiles, int ntiles, Workspace ws,
+                     cudaStream_t stream);
+void launch_jacobi(TileWork *d_tiles, int ntiles, Workspace ws,
+                   cudaStream_t stream);
+void launch_rank_cut(TileWork *d_tiles, int ntiles, Workspace ws,
+                     double tol, int maxrank, cudaStream_t stream);
+void launch_merge_basis(TileWork *d_tiles, int ntiles, cudaStream_t stream);
+void launch_select_w(const TileWork *d_tiles, int ntiles, Workspace ws,
+                     cudaStream_t stream);
+void launch_write_v(const TileWork *d_tiles, int ntiles, Workspace ws,
+                    OutArena out, cudaStream_t stream);
+void launch_gaussian(double *d_omega, long long count, unsigned long long seed,
+                     cudaStream_t stream);
+
+}  // namespace b200

@@ -1,0 +1,273 @@
+// Device evaluation of one kernel-matrix entry, shared by the tile
+// generator, the fused sketch kernels and the error kernel.
+//
+// Each family computes the same expression, in the same operation order,
+// as the reference kernel of that name (src/applications/spatial/
+// kernel_{exp,sqrexp,matern,matern2}.c, electrostatics/
+// kernel_coulomb_potential.c, electrodynamics/kernel_{sin,cos}.c,
+// mesh_deformation/virus.c + kernels_rbf.c), so that generated blocks agree
+// with the reference to a few ulp: the squared distance is accumulated
+// dimension by dimension without FMA contraction, and divisions are true
+// IEEE divisions.  The Matérn families need K_nu, which the reference takes
+// from GSL; bessel_knu() below is this library's own implementation.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace b200 {
+
+// Families (values of STARSH_B200_FAMILY_* in starsh-b200.h).
+enum : int {
+    FAM_EXP = 1, FAM_SQREXP = 2, FAM_MATERN = 3, FAM_MATERN2 = 4,
+    FAM_COULOMB = 5, FAM_SIN = 6, FAM_COS = 7, FAM_RBF = 8
+};
+
+// Everything a device generator needs: family parameters and device
+// pointers to the coordinates and the cluster pivots.
+struct DevKernel {
+    int family;
+    int ndim;
+    int aos;          // RBF: point-major coordinates
+    int rbf_kind;
+    int isreg;
+    int zero_mode;    // Coulomb: r = 0 gives `diag` instead of 0
+    double sigma, beta, nu, noise;
+    double matern_coef, matern_scale;
+    double wave_k, diag;
+    double rad, reg;
+    const double *row_pt;     // coordinates of the row point set
+    const double *col_pt;     // coordinates of the column point set
+    long long row_count, col_count;
+    const long long *row_piv; // cluster pivots (STARSH_int)
+    const long long *col_piv;
+};
+
+// Taylor coefficients of 1/Gamma(1+z) about z = 0 (a_0 = 1, a_1 = Euler's
+// gamma, ...), computed with mpmath at 50 digits by
+// stars-h_b200/csrc/gen_rgamma_coeffs.py.
+__device__ __constant__ static const double kRGammaCoef[29] = {
+    1.0,
+    0.5772156649015328606065121,
+    -0.6558780715202538810770195,
+    -0.04200263503409523552900393,
+    0.1665386113822914895017008,
+    -0.0421977345555443367482083,
+    -0.009621971527876973562114922,
+    0.00721894324666309954239501,
+    -0.001165167591859065112113971,
+    -0.00021524167411495097281573,
+    0.0001280502823881161861531986,
+    -0.00002013485478078823865568939,
+    -0.000001250493482142670657345359,
+    0.00000113302723198169588237413,
+    -0.0000002056338416977607103450154,
+    6.116095104481415817862499e-9,
+    5.002007644469222930055665e-9,
+    -1.181274570487020144588127e-9,
+    1.04342671169110051049154e-10,
+    7.782263439905071254049937e-12,
+    -3.696805618642205708187816e-12,
+    5.100370287454475979015481e-13,
+    -2.05832605356650678322243e-14,
+    -5.348122539423017982370017e-15,
+    1.226778628238260790158894e-15,
+    -1.181259301697458769513765e-16,
+    1.186692254751600332579777e-18,
+    1.412380655318031781555804e-18,
+    -2.298745684435370206592479e-19,
+};
+
+// K_mu(x) and K_{mu+1}(x) for |mu| <= 1/2, 0 < x <= 2, by Temme's series
+// (N. M. Temme, J. Comput. Phys. 19 (1975) 324-337):
+//   K_mu     = sum_k c_k f_k,      K_{mu+1} = (2/x) sum_k c_k h_k,
+//   c_k = (x^2/4)^k / k!,
+//   f_0 = (mu pi / sin(mu pi)) [cosh(s) G1 + sinh(s)/s * ln(2/x) G2],
+//         s = mu ln(2/x),
+//   p_0 = (x/2)^-mu Gamma(1+mu) / 2,  q_0 = (x/2)^mu Gamma(1-mu) / 2,
+//   f_k = (k f_{k-1} + p_{k-1} + q_{k-1}) / (k^2 - mu^2),
+//   p_k = p_{k-1} / (k - mu),  q_k = q_{k-1} / (k + mu),  h_k = p_k - k f_k,
+// with G1 = (1/Gamma(1-mu) - 1/Gamma(1+mu)) / (2 mu) and
+// G2 = (1/Gamma(1-mu) + 1/Gamma(1+mu)) / 2 taken from the odd and even
+// parts of the power series of 1/Gamma(1+z), which avoids the cancellation
+// of the difference quotient at small mu.
+__device__ inline void bessel_k_temme(double mu, double x, double *kmu,
+                                      double *kmu1)
+{
+    double g1 = 0.0, g2 = 0.0, mu2 = mu * mu, pw = 1.0;
+    // even coefficients -> G2, odd coefficients -> -G1
+    #pragma unroll
+    for (int j = 0; j < 29; j += 2) {
+        g2 += kRGammaCoef[j] * pw;
+        if (j + 1 < 29) g1 -= kRGammaCoef[j + 1] * pw;
+        pw *= mu2;
+    }
+    // 1/Gamma(1+mu) = G2 - mu*G1 ; 1/Gamma(1-mu) = G2 + mu*G1
+    const double rg_plus = g2 - mu * g1;
+    const double rg_minus = g2 + mu * g1;
+    const double half_x = 0.5 * x;
+    const double lg = -log(half_x);               // ln(2/x)
+    const double s = mu * lg;
+    const double pimu = M_PI * mu;
+    const double fact = fabs(pimu) < 1e-15 ? 1.0 : pimu / sin(pimu);
+    const double shs = fabs(s) < 1e-15 ? 1.0 : sinh(s) / s;
+    double f = fact * (g1 * cosh(s) + g2 * lg * shs);
+    const double e = exp(s);                      // (x/2)^-mu
+    double p = 0.5 * e / rg_plus;
+    double q = 0.5 / (e * rg_minus);
+    double c = 1.0;
+    const double c_step = half_x * half_x;
+    double sum = f, sum1 = p;
+    for (int k = 1; k < 500; ++k) {
+        const double dk = (double)k;
+        f = (dk * f + p + q) / (dk * dk - mu2);
+        c *= c_step / dk;
+        p /= (dk - mu);
+        q /= (dk + mu);
+        const double t = c * f;
+        sum += t;
+        sum1 += c * (p - dk * f);
+        if (fabs(t) < 1e-17 * fabs(sum)) break;
+    }
+    *kmu = sum;
+    *kmu1 = sum1 * (2.0 / x);
+}
+
+// K_nu(x) for x > 2 from the integral K_nu(x) = int_0^inf exp(-x cosh t)
+// cosh(nu t) dt.  With s = sqrt(2x) sinh(t/2):
+//   e^x K_nu(x) = int_0^inf e^{-s^2} cosh(2 nu asinh(y)) 2 / sqrt(2x+s^2) ds,
+//   y = s / sqrt(2x),
+// an integrand analytic in the strip |Im s| < d = sqrt(2x) with Gaussian
+// decay, for which the trapezoidal rule converges geometrically
+// (L. N. Trefethen and J. A. C. Weideman, SIAM Review 56 (2014) 385-458).
+// On a line Im s = c the Gaussian grows like e^{c^2}, so the error is about
+// exp(-2 pi c / h + c^2) for c <= d; h = min(0.49, 2 pi d / (41 + d^2))
+// keeps it below ~1e-17 (checked against mpmath to 1e-14 relative for
+// 0.1 <= nu <= 4.7, 2 < x <= 300).  Nodes stop where e^{-s^2} < 1e-19.
+__device__ inline double bessel_k_large(double nu, double x)
+{
+    const double two_x = 2.0 * x;
+    const double d = sqrt(two_x);
+    const double h = fmin(0.49, 2.0 * M_PI * d / (41.0 + two_x));
+    const double inv_d = 1.0 / d;
+    double sum = 0.0;
+    for (int k = 0; k < 64; ++k) {
+        const double s = k * h;
+        const double w = exp(-s * s);
+        if (w < 1e-19) break;
+        const double y = s * inv_d;
+        const double a = y + sqrt(1.0 + y * y);   // exp(asinh(y))
+        const double ap = exp(2.0 * nu * log(a));  // a^(2 nu)
+        const double g = 0.5 * (ap + 1.0 / ap) * 2.0 / sqrt(two_x + s * s);
+        sum += (k == 0 ? 0.5 : 1.0) * w * g;
+    }
+    return h * sum * exp(-x);
+}
+
+// K_nu(x), nu >= 0, x > 0.  Small arguments: Temme's series at
+// mu = nu - round(nu) and upward recurrence
+// K_{m+1} = K_{m-1} + (2 m / x) K_m; large arguments: the integral above.
+__device__ inline double bessel_knu(double nu, double x)
+{
+    if (x > 2.0) return bessel_k_large(nu, x);
+    const int nl = (int)(nu + 0.5);
+    const double mu = nu - nl;
+    double k0, k1;
+    bessel_k_temme(mu, x, &k0, &k1);
+    for (int i = 1; i <= nl; ++i) {
+        const double k2 = k0 + (2.0 * (mu + i) / x) * k1;
+        k0 = k1;
+        k1 = k2;
+    }
+    return k0;
+}
+
+// Squared distance accumulated as the reference does: tmp = a - b;
+// dist += tmp*tmp, one dimension after another, no fused multiply-add.
+__device__ __forceinline__ double sq_dist(const DevKernel &K, long long ir,
+                                          long long jc)
+{
+    double dist = 0.0;
+    if (K.aos) {
+        #pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const double t = __dsub_rn(K.row_pt[3 * ir + d],
+                                       K.col_pt[3 * jc + d]);
+            dist = __dadd_rn(dist, __dmul_rn(t, t));
+        }
+    } else {
+        for (int d = 0; d < K.ndim; ++d) {
+            const double t = __dsub_rn(K.row_pt[d * K.row_count + ir],
+                                       K.col_pt[d * K.col_count + jc]);
+            dist = __dadd_rn(dist, __dmul_rn(t, t));
+        }
+    }
+    return dist;
+}
+
+// Entry value from the squared distance and the two point indices.
+__device__ __forceinline__ double entry_from_dist(const DevKernel &K,
+                                                  double dist, long long ir,
+                                                  long long jc)
+{
+    switch (K.family) {
+    case FAM_EXP: {
+        const double v = __ddiv_rn(sqrt(dist), -K.beta);
+        return v == 0.0 ? K.sigma + K.noise : K.sigma * exp(v);
+    }
+    case FAM_SQREXP: {
+        const double v = __ddiv_rn(dist, (-2.0 * K.beta) * K.beta);
+        return v == 0.0 ? K.sigma + K.noise : K.sigma * exp(v);
+    }
+    case FAM_MATERN:
+    case FAM_MATERN2: {
+        const double x = K.family == FAM_MATERN
+            ? __dmul_rn(sqrt(dist), K.matern_scale)
+            : __ddiv_rn(sqrt(dist), K.beta);
+        if (x == 0.0) return K.sigma + K.noise;
+        return K.matern_coef * pow(x, K.nu) * bessel_knu(K.nu, x);
+    }
+    case FAM_COULOMB:
+        if (dist == 0.0) return K.zero_mode ? K.diag : 0.0;
+        return __ddiv_rn(1.0, sqrt(dist));
+    case FAM_SIN:
+    case FAM_COS: {
+        if (dist == 0.0) return K.diag;
+        const double r = sqrt(dist);
+        const double a = K.wave_k * r;
+        return __ddiv_rn(K.family == FAM_SIN ? sin(a) : cos(a), r);
+    }
+    case FAM_RBF: {
+        const double x = __ddiv_rn(sqrt(dist), K.rad);
+        double v;
+        switch (K.rbf_kind) {
+        case 0: v = exp(-(x * x)); break;
+        case 1: v = exp(-x); break;
+        case 2: v = __ddiv_rn(1.0, 1.0 + x * x); break;
+        case 3: v = __ddiv_rn(1.0, sqrt(1.0 + x * x)); break;
+        case 4:
+        case 5: v = exp(-x) + (1.0 + x); break;
+        case 6: v = (x * x) * log(x); break;
+        case 7: v = x > 1.0 ? 0.0 : pow(1.0 - x, 5.0); break;
+        case 8: v = 1.0 + x * x; break;
+        default: v = x > 1.0 ? 0.0 : pow(1.0 - x, 4.0) * (4.0 * x + 1.0);
+        }
+        // virus.c compares the truncated int point indices
+        if (K.isreg && (int)ir == (int)jc) v += K.reg;
+        return v;
+    }
+    }
+    return 0.0;
+}
+
+// Entry (i, j) of the block whose rows are row_piv[row0 + i] and columns
+// col_piv[col0 + j].
+__device__ __forceinline__ double block_entry(const DevKernel &K,
+                                              long long row0, long long col0,
+                                              int i, int j)
+{
+    const long long ir = K.row_piv[row0 + i];
+    const long long jc = K.col_piv[col0 + j];
+    return entry_from_dist(K, sq_dist(K, ir, jc), ir, jc);
+}
+
+}  // namespace b200

@@ -1,0 +1,69 @@
+// Internal declarations shared by the engine and the TLR-product/error
+// kernels: device copies of a problem's points, dense block jobs, and the
+// device-resident record kept per STARSH_blrm.
+#pragma once
+#include <cuda_runtime.h>
+#include <vector>
+#include "device_ctx.cuh"
+#include "kernel_entry.cuh"
+#include "b200_host.h"
+
+namespace b200 {
+
+// Device copies of the coordinates and pivots a kernel reads.
+struct DevicePoints {
+    DevKernel K{};
+    std::vector<void *> owned;
+    size_t h2d = 0;
+    ~DevicePoints()
+    {
+        for (void *p : owned) cudaFree(p);
+    }
+    int upload(const void *host, size_t bytes, const void **dev,
+               cudaStream_t s)
+    {
+        void *d = nullptr;
+        B200_CUDA(cudaMalloc(&d, bytes ? bytes : 8), "cudaMalloc(points)");
+        owned.push_back(d);
+        if (bytes)
+            B200_CUDA(cudaMemcpyAsync(d, host, bytes, cudaMemcpyHostToDevice, s),
+                      "cudaMemcpyAsync(points)");
+        h2d += bytes;
+        *dev = d;
+        return STARSH_SUCCESS;
+    }
+};
+
+struct BlockJob {
+    long long row0, col0;
+    int m, n;
+    double *out;   // column-major, ld = m
+};
+
+// Device-resident factors of one STARSH_blrm.
+struct Record {
+    std::vector<void *> chunks;        // device allocations
+    std::vector<double *> dU, dV;      // per far block (device)
+    std::vector<double *> dD;          // per near block (device, or null)
+    size_t u_total = 0, v_total = 0, d_total = 0;
+    bool host_filled = false;
+    DevicePoints *points = nullptr;    // kept for onfly near blocks
+    ~Record()
+    {
+        for (void *p : chunks) cudaFree(p);
+        delete points;
+    }
+};
+
+void fill_kernel(DevKernel &K, const b200_kspec &sp);
+int upload_problem(DevicePoints &dp, STARSH_problem *P, STARSH_cluster *R,
+                   STARSH_cluster *C, cudaStream_t s);
+// Generates dense blocks (column-major, ld = m) on stream s.
+int gen_blocks(const DevKernel &K, const std::vector<BlockJob> &jobs,
+               cudaStream_t s);
+Record *find_record(const STARSH_blrm *M);
+// Registers a record for M (replacing none); used for matrices whose
+// factors were uploaded from the host.
+void add_record(const STARSH_blrm *M, Record *rec);
+
+}  // namespace b200

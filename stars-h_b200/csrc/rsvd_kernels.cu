@@ -1,0 +1,791 @@
+// Device kernels of the batched randomized-SVD engine (FP64 path).
+//
+// Per tile (D: m x n block, Omega: n x k Gaussian, k = min(maxrank +
+// oversample, m, n)) the engine computes the same factorisation as the
+// reference's starsh_dense_dlrrsdd (src/backends/sequential/dense/
+// drsdd.c:16-93): Y = D Omega, an orthonormal basis Q of range(Y),
+// B = Q^T D, the SVD of B, the rank cut of starsh_dense_dsvfr
+// (src/backends/sequential/dense/dsvfr.c:16-47) and U = Q Us_r,
+// V = (S_r Vs_r)^T.  The orthogonalisation and the small SVD are done with
+// Gram matrices so that every O(m n k) and O(m k^2) step is a GEMM:
+//   * basis: pivoted Cholesky of Y^T Y drops directions below the FP64
+//     squared-noise floor or below (tol/10)^2 of the sketch energy, CholQR2
+//     on the kept columns; when tol^2 is below the squared-noise floor a
+//     second pass orthogonalises the explicit residual Y - Q Q^T Y, which
+//     recovers the directions the squared Gram could not resolve;
+//   * small SVD: B B^T = L L^T (pivoted Cholesky), one-sided Jacobi on L
+//     gives the left singular vectors W of B; the energies of the rotated
+//     rows C = W^T B are summed in FP64 directly from C, so the tail that
+//     decides the rank is exact to FP64 rounding even where the Gram's
+//     eigenvalues are not.
+#include <cfloat>
+#include "engine.cuh"
+
+namespace b200 {
+
+// ------------------------------------------------------------ layout
+
+size_t workspace_layout(Workspace &w, int m_max, int n_max, int k_max,
+                        bool store_d)
+{
+    size_t o = 0;
+    auto take = [&](size_t n) {
+        const size_t r = o;
+        o += (n + 31) & ~(size_t)31;   // 256-byte aligned fields
+        return r;
+    };
+    w.m_max = m_max;
+    w.n_max = n_max;
+    w.k_max = k_max;
+    w.oD = store_d ? take((size_t)m_max * n_max) : 0;
+    w.oY = take((size_t)m_max * k_max);
+    w.oQ1 = take((size_t)m_max * k_max);
+    w.oQ = take((size_t)m_max * k_max);
+    w.oS = take((size_t)k_max * k_max);
+    w.oL = take((size_t)k_max * k_max);
+    w.oT = take((size_t)k_max * k_max);
+    w.oB = take((size_t)k_max * n_max);
+    w.oC = take((size_t)k_max * n_max);
+    w.oE = take(k_max);
+    w.oSig = take(k_max);
+    w.oPiv = take((k_max + 1) / 2);
+    w.oOrd = take((k_max + 1) / 2);
+    w.stride = o;
+    return o;
+}
+
+// -------------------------------------------------------- generation
+
+// D(slot) = block of the tile, column-major with ld = m_max.  Threads run
+// down a column so that stores are coalesced.
+__global__ void __launch_bounds__(256)
+k_gen_tiles(DevKernel K, const TileWork *__restrict__ tiles, Workspace ws)
+{
+    const TileWork tw = tiles[blockIdx.z];
+    const int i = blockIdx.x * 64 + (threadIdx.x & 63);
+    const int jb = blockIdx.y * 64 + (threadIdx.x >> 6);
+    if (blockIdx.x * 64 >= tw.m || blockIdx.y * 64 >= tw.n) return;
+    double *D = ws.D(tw.slot);
+    const int ld = ws.ldD();
+    if (i >= tw.m) return;
+    for (int c = 0; c < 16; ++c) {
+        const int j = jb + 4 * c;
+        if (j < tw.n) D[(size_t)j * ld + i] = block_entry(K, tw.row0, tw.col0, i, j);
+    }
+}
+
+void launch_gen_tiles(const DevKernel &K, const TileWork *d_tiles,
+                      int ntiles, Workspace ws, cudaStream_t stream)
+{
+    dim3 grid((ws.m_max + 63) / 64, (ws.n_max + 63) / 64, ntiles);
+    k_gen_tiles<<<grid, 256, 0, stream>>>(K, d_tiles, ws);
+}
+
+// ---------------------------------------------------- Gaussian sketch
+
+// Philox4x32-10 counter-based generator (J. K. Salmon, M. A. Moraes,
+// R. O. Dror, D. E. Shaw, "Parallel random numbers: as easy as 1, 2, 3",
+// SC'11); multipliers and Weyl increments are the published constants.
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k)
+{
+    #pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const unsigned lo0 = 0xD2511F53u * c.x;
+        const unsigned hi0 = __umulhi(0xD2511F53u, c.x);
+        const unsigned lo1 = 0xCD9E8D57u * c.z;
+        const unsigned hi1 = __umulhi(0xCD9E8D57u, c.z);
+        c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+        k.x += 0x9E3779B9u;
+        k.y += 0xBB67AE85u;
+    }
+    return c;
+}
+
+// Omega entries N(0,1): one Philox block -> two 53-bit uniforms in (0,1]
+// -> one Box-Muller pair (G. E. P. Box, M. E. Muller, Ann. Math. Stat. 29
+// (1958) 610-611).
+__global__ void k_gaussian(double *out, long long count,
+                           unsigned long long seed)
+{
+    const long long pair = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (2 * pair >= count) return;
+    const uint4 c = make_uint4((unsigned)pair, (unsigned)(pair >> 32), 0u, 0u);
+    const uint4 r = philox4x32_10(c, make_uint2((unsigned)seed,
+                                                (unsigned)(seed >> 32)));
+    const unsigned long long b1 = ((unsigned long long)r.x << 32) | r.y;
+    const unsigned long long b2 = ((unsigned long long)r.z << 32) | r.w;
+    const double u1 = ((b1 >> 11) + 1) * 0x1.0p-53;   // (0, 1]
+    const double u2 = (b2 >> 11) * 0x1.0p-53;         // [0, 1)
+    const double rad = sqrt(-2.0 * log(u1));
+    double s, co;
+    sincospi(2.0 * u2, &s, &co);
+    out[2 * pair] = rad * co;
+    if (2 * pair + 1 < count) out[2 * pair + 1] = rad * s;
+}
+
+void launch_gaussian(double *d_omega, long long count,
+                     unsigned long long seed, cudaStream_t stream)
+{
+    const long long pairs = (count + 1) / 2;
+    k_gaussian<<<(unsigned)((pairs + 255) / 256), 256, 0, stream>>>(
+        d_omega, count, seed);
+}
+
+// ------------------------------------------------- GEMM descriptors
+
+__global__ void k_make_desc(GemmStep step, const TileWork *__restrict__ tiles,
+                            int ntiles, Workspace ws,
+                            const double *__restrict__ omega, int ld_omega,
+                            OutArena out, GemmDesc *__restrict__ desc)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntiles) return;
+    const TileWork tw = tiles[t];
+    const int s = tw.slot;
+    GemmDesc d;
+    d.alpha = 1.0;
+    d.beta = 0.0;
+    d.M = d.N = d.K = 0;
+    d.A = d.B = nullptr;
+    d.C = nullptr;
+    d.lda = d.ldb = d.ldc = 1;
+    const int ldm = ws.ldM(), ldk = ws.ldK();
+    switch (step) {
+    case STEP_SKETCH:
+        d.A = ws.D(s); d.lda = ws.ldD();
+        d.B = omega; d.ldb = ld_omega;
+        d.C = ws.Y(s); d.ldc = ldm;
+        d.M = tw.m; d.N = tw.k; d.K = tw.n;
+        break;
+    case STEP_GRAM_YR:  // TN, residual of pass B
+        if (!tw.need_pass_b) break;
+        d.A = ws.Y(s); d.lda = ldm;
+        d.B = ws.Y(s); d.ldb = ldm;
+        d.C = ws.S(s); d.ldc = ldk;
+        d.M = tw.k; d.N = tw.k; d.K = tw.m;
+        break;
+    case STEP_GRAM_Y:   // TN
+        d.A = ws.Y(s); d.lda = ldm;
+        d.B = ws.Y(s); d.ldb = ldm;
+        d.C = ws.S(s); d.ldc = ldk;
+        d.M = tw.k; d.N = tw.k; d.K = tw.m;
+        break;
+    case STEP_Q1:       // NN: Q1buf = Qbuf(gathered) * T
+        d.A = ws.Q(s); d.lda = ldm;
+        d.B = ws.T(s); d.ldb = ldk;
+        d.C = ws.Q1(s); d.ldc = ldm;
+        d.M = tw.m; d.N = tw.k1; d.K = tw.k1;
+        break;
+    case STEP_GRAM_Q1:  // TN
+        d.A = ws.Q1(s); d.lda = ldm;
+        d.B = ws.Q1(s); d.ldb = ldm;
+        d.C = ws.S(s); d.ldc = ldk;
+        d.M = tw.k1; d.N = tw.k1; d.K = tw.m;
+        break;
+    case STEP_Q:        // NN: Qbuf = Q1buf * T
+        d.A = ws.Q1(s); d.lda = ldm;
+        d.B = ws.T(s); d.ldb = ldk;
+        d.C = ws.Q(s); d.ldc = ldm;
+        d.M = tw.m; d.N = tw.k1; d.K = tw.k1;
+        break;
+    case STEP_RES_Z:    // TN: S = Q^T Y
+        if (!tw.need_pass_b) break;
+        d.A = ws.Q(s); d.lda = ldm;
+        d.B = ws.Y(s); d.ldb = ldm;
+        d.C = ws.S(s); d.ldc = ldk;
+        d.M = tw.k1; d.N = tw.k; d.K = tw.m;
+        break;
+    case STEP_RES_Y:    // NN: Y -= Q S
+        if (!tw.need_pass_b) break;
+        d.A = ws.Q(s); d.lda = ldm;
+        d.B = ws.S(s); d.ldb = ldk;
+        d.C = ws.Y(s); d.ldc = ldm;
+        d.alpha = -1.0; d.beta = 1.0;
+        d.M = tw.m; d.N = tw.k; d.K = tw.k1;
+        break;
+    case STEP_Q1B:      // NN: Ybuf = Q1buf(gathered residual) * T
+        if (tw.kb <= 0) break;
+        d.A = ws.Q1(s); d.lda = ldm;
+        d.B = ws.T(s); d.ldb = ldk;
+        d.C = ws.Y(s); d.ldc = ldm;
+        d.M = tw.m; d.N = tw.kb; d.K = tw.kb;
+        break;
+    case STEP_RES_Z2:   // TN: S = Q^T Ybuf
+        if (tw.kb <= 0) break;
+        d.A = ws.Q(s); d.lda = ldm;
+        d.B = ws.Y(s); d.ldb = ldm;
+        d.C = ws.S(s); d.ldc = ldk;
+        d.M = tw.k1; d.N = tw.kb; d.K = tw.m;
+        break;
+    case STEP_RES_Q1B:  // NN: Ybuf -= Q S
+        if (tw.kb <= 0) break;
+        d.A = ws.Q(s); d.lda = ldm;
+        d.B = ws.S(s); d.ldb = ldk;
+        d.C = ws.Y(s); d.ldc = ldm;
+        d.alpha = -1.0; d.beta = 1.0;
+        d.M = tw.m; d.N = tw.kb; d.K = tw.k1;
+        break;
+    case STEP_GRAM_Q1B: // TN
+        if (tw.kb <= 0) break;
+        d.A = ws.Y(s); d.lda = ldm;
+        d.B = ws.Y(s); d.ldb = ldm;
+        d.C = ws.S(s); d.ldc = ldk;
+        d.M = tw.kb; d.N = tw.kb; d.K = tw.m;
+        break;
+    case STEP_QB:       // NN: Q[:, k1:k1+kb] = Ybuf T
+        if (tw.kb <= 0) break;
+        d.A = ws.Y(s); d.lda = ldm;
+        d.B = ws.T(s); d.ldb = ldk;
+        d.C = ws.Q(s) + (size_t)tw.k1 * ldm; d.ldc = ldm;
+        d.M = tw.m; d.N = tw.kb; d.K = tw.kb;
+        break;
+    case STEP_PROJECT:  // TN: B = Q^T D
+        d.A = ws.Q(s); d.lda = ldm;
+        d.B = ws.D(s); d.ldb = ws.ldD();
+        d.C = ws.B(s); d.ldc = ldk;
+        d.M = tw.k1; d.N = tw.n; d.K = tw.m;
+        break;
+    case STEP_GRAM_B:   // NT: S = B B^T
+        d.A = ws.B(s); d.lda = ldk;
+        d.B = ws.B(s); d.ldb = ldk;
+        d.C = ws.S(s); d.ldc = ldk;
+        d.M = tw.k1; d.N = tw.k1; d.K = tw.n;
+        break;
+    case STEP_ROTATE:   // TN: C = W^T B, W in T
+        d.A = ws.T(s); d.lda = ldk;
+        d.B = ws.B(s); d.ldb = ldk;
+        d.C = ws.C(s); d.ldc = ldk;
+        d.M = tw.k2; d.N = tw.n; d.K = tw.k1;
+        break;
+    case STEP_OUT_U:    // NN: U = Q Wsel, Wsel in L
+        if (tw.rank <= 0) break;
+        d.A = ws.Q(s); d.lda = ldm;
+        d.B = ws.L(s); d.ldb = ldk;
+        d.C = out.U + tw.off_u; d.ldc = tw.m;
+        d.M = tw.m; d.N = tw.rank; d.K = tw.k1;
+        break;
+    }
+    desc[t] = d;
+}
+
+void make_gemm_descs(GemmStep step, const TileWork *d_tiles, int ntiles,
+                     Workspace ws, const double *d_omega, int ld_omega,
+                     OutArena out, GemmDesc *d_desc, cudaStream_t stream)
+{
+    k_make_desc<<<(ntiles + 127) / 128, 128, 0, stream>>>(
+        step, d_tiles, ntiles, ws, d_omega, ld_omega, out, d_desc);
+}
+
+// ------------------------------------------------- block reductions
+
+struct MaxLoc {
+    double v;
+    int i;
+};
+
+// Block-wide argmax (largest value, then smallest index).  `red` holds one
+// entry per warp.  All threads get the result.
+__device__ MaxLoc block_argmax(MaxLoc x, MaxLoc *red)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        MaxLoc y;
+        y.v = __shfl_down_sync(0xffffffffu, x.v, o);
+        y.i = __shfl_down_sync(0xffffffffu, x.i, o);
+        if (y.v > x.v || (y.v == x.v && y.i < x.i)) x = y;
+    }
+    __syncthreads();
+    if (lane == 0) red[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        x = lane < (int)(blockDim.x >> 5) ? red[lane] : MaxLoc{-DBL_MAX, 1 << 30};
+        #pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            MaxLoc y;
+            y.v = __shfl_down_sync(0xffffffffu, x.v, o);
+            y.i = __shfl_down_sync(0xffffffffu, x.i, o);
+            if (y.v > x.v || (y.v == x.v && y.i < x.i)) x = y;
+        }
+        if (lane == 0) red[0] = x;
+    }
+    __syncthreads();
+    MaxLoc r = red[0];
+    __syncthreads();
+    return r;
+}
+
+__device__ double block_sum(double x, double *red)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    __syncthreads();
+    if (lane == 0) red[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        x = lane < (int)(blockDim.x >> 5) ? red[lane] : 0.0;
+        #pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if (lane == 0) red[0] = x;
+    }
+    __syncthreads();
+    const double r = red[0];
+    __syncthreads();
+    return r;
+}
+
+// ------------------------------------------------ pivoted Cholesky
+
+enum : int { PH_A = 0, PH_B = 1, PH_H = 2 };
+
+constexpr int kSmallThreads = 256;
+constexpr int kMaxK = 1024;   // largest sketch width handled by one CTA
+
+// Left-looking pivoted Cholesky of the Gram in S(slot) (dimension nn):
+// P^T G P ~ L L^T, L stored in L(slot) with rows in the original order
+// (column j holds the multipliers of pivot j).  Stops when the largest
+// remaining diagonal entry is <= thr.  For the basis phases (A, B) the
+// pivot block R11 = L[piv, :]^T is inverted into T(slot).
+__global__ void __launch_bounds__(kSmallThreads)
+k_pivchol(TileWork *__restrict__ tiles, Workspace ws, int phase, double tol)
+{
+    TileWork &tw = tiles[blockIdx.x];
+    const int s = tw.slot;
+    __shared__ double dg[kMaxK];
+    __shared__ double lp[kMaxK];
+    __shared__ unsigned char used[kMaxK];
+    __shared__ MaxLoc red[32];
+    __shared__ double redd[32];
+
+    int nn;
+    if (phase == PH_H) nn = tw.k1;
+    else nn = tw.k;
+    if (phase == PH_B && !tw.need_pass_b) {
+        if (threadIdx.x == 0) tw.kb = 0;
+        return;
+    }
+    const double *G = ws.S(s);
+    const int ld = ws.ldK();
+    double *L = ws.L(s);
+    int *piv = ws.Piv(s);
+
+    double loc = 0.0;
+    for (int i = threadIdx.x; i < nn; i += blockDim.x) {
+        dg[i] = G[(size_t)i * ld + i];
+        used[i] = 0;
+        loc += dg[i];
+    }
+    const double trace = block_sum(loc, redd);
+    MaxLoc mx{-DBL_MAX, 1 << 30};
+    for (int i = threadIdx.x; i < nn; i += blockDim.x)
+        if (dg[i] > mx.v) mx = MaxLoc{dg[i], i};
+    const double dmax = block_argmax(mx, red).v;
+
+    double thr;
+    int cap = nn;
+    if (phase == PH_A) {
+        const double tol_floor = 0.01 * tol * tol * trace / nn;
+        const double noise = 1e-15 * dmax;
+        thr = fmax(noise, tol_floor);
+        if (threadIdx.x == 0) {
+            tw.tr_g = trace;
+            tw.need_pass_b = noise > tol_floor && trace > 0.0;
+        }
+    } else if (phase == PH_B) {
+        thr = fmax(1e-15 * dmax, 0.01 * tol * tol * tw.tr_g / tw.k);
+        cap = tw.k - tw.k1;
+    } else {
+        thr = 1e-18 * dmax;
+        if (threadIdx.x == 0) tw.tr_h = trace;
+    }
+    if (!(dmax > 0.0)) thr = DBL_MAX;   // zero or invalid Gram: rank 0
+
+    int j = 0;
+    for (; j < cap; ++j) {
+        MaxLoc cand{-DBL_MAX, 1 << 30};
+        for (int i = threadIdx.x; i < nn; i += blockDim.x)
+            if (!used[i] && dg[i] > cand.v) cand = MaxLoc{dg[i], i};
+        const MaxLoc best = block_argmax(cand, red);
+        if (!(best.v > thr)) break;
+        const int p = best.i;
+        const double sp = sqrt(best.v);
+        for (int l = threadIdx.x; l < j; l += blockDim.x)
+            lp[l] = L[(size_t)l * ld + p];
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            piv[j] = p;
+            used[p] = 1;
+        }
+        for (int i = threadIdx.x; i < nn; i += blockDim.x) {
+            double v;
+            if (i == p) {
+                v = sp;
+            } else if (used[i]) {
+                v = 0.0;
+            } else {
+                double acc = G[(size_t)p * ld + i];
+                for (int l = 0; l < j; ++l) acc -= L[(size_t)l * ld + i] * lp[l];
+                v = acc / sp;
+                dg[i] -= v * v;
+            }
+            L[(size_t)j * ld + i] = v;
+        }
+        __syncthreads();
+    }
+    const int cnt = j;
+    if (threadIdx.x == 0) {
+        if (phase == PH_A) tw.k1 = cnt;
+        else if (phase == PH_B) tw.kb = cnt;
+        else tw.k2 = cnt;
+    }
+    if (phase == PH_H) return;
+    // T = R11^{-1}, R11(a, b) = L(piv[b], a) for a <= b (upper triangular).
+    double *T = ws.T(s);
+    for (int c = threadIdx.x; c < cnt; c += blockDim.x) {
+        double *x = T + (size_t)c * ld;
+        for (int a = c + 1; a < cnt; ++a) x[a] = 0.0;
+        x[c] = 1.0 / L[(size_t)c * ld + piv[c]];
+        for (int a = c - 1; a >= 0; --a) {
+            double acc = 0.0;
+            for (int b = a + 1; b <= c; ++b) acc += L[(size_t)a * ld + piv[b]] * x[b];
+            x[a] = -acc / L[(size_t)a * ld + piv[a]];
+        }
+    }
+}
+
+void launch_pivchol(int phase, const TileWork *, TileWork *d_tiles_rw,
+                    int ntiles, Workspace ws, double tol, cudaStream_t s)
+{
+    k_pivchol<<<ntiles, kSmallThreads, 0, s>>>(d_tiles_rw, ws, phase, tol);
+}
+
+// Gathers the pivot columns of Y into the Q buffer (phase A) or the Q1
+// buffer (phase B).
+__global__ void k_gather_cols(const TileWork *__restrict__ tiles,
+                              Workspace ws, int phase)
+{
+    const TileWork tw = tiles[blockIdx.x];
+    const int s = tw.slot;
+    const int cnt = phase == PH_A ? tw.k1 : tw.kb;
+    if (cnt <= 0) return;
+    const int *piv = ws.Piv(s);
+    const double *Y = ws.Y(s);
+    double *dst = phase == PH_A ? ws.Q(s) : ws.Q1(s);
+    const int ld = ws.ldM();
+    for (int c = blockIdx.y; c < cnt; c += gridDim.y) {
+        const double *src = Y + (size_t)piv[c] * ld;
+        for (int i = threadIdx.x; i < tw.m; i += blockDim.x)
+            dst[(size_t)c * ld + i] = src[i];
+    }
+}
+
+void launch_gather_cols(int phase, const TileWork *d_tiles, int ntiles,
+                        Workspace ws, cudaStream_t stream)
+{
+    dim3 grid(ntiles, 16);
+    k_gather_cols<<<grid, 256, 0, stream>>>(d_tiles, ws, phase);
+}
+
+// Cholesky G = R^T R of the re-orthogonalisation Gram in S(slot)
+// (dimension k1 for phase A, kb for phase B), R into L(slot), then
+// T(slot) = R^{-1}.  For phase B the new columns are appended to the basis
+// afterwards by the caller's merge step.
+__global__ void __launch_bounds__(kSmallThreads)
+k_chol_inv(TileWork *__restrict__ tiles, Workspace ws, int phase)
+{
+    TileWork &tw = tiles[blockIdx.x];
+    const int s = tw.slot;
+    const int nn = phase == PH_A ? tw.k1 : tw.kb;
+    if (nn <= 0) return;
+    const double *G = ws.S(s);
+    double *R = ws.L(s);
+    double *T = ws.T(s);
+    const int ld = ws.ldK();
+    __shared__ double diag;
+    __shared__ int fail;
+    if (threadIdx.x == 0) fail = 0;
+    __syncthreads();
+    for (int j = 0; j < nn; ++j) {
+        if (threadIdx.x == 0) {
+            double acc = G[(size_t)j * ld + j];
+            for (int l = 0; l < j; ++l) {
+                const double r = R[(size_t)j * ld + l];
+                acc -= r * r;
+            }
+            if (!(acc > 0.0)) { fail = 1; acc = 1.0; }
+            diag = sqrt(acc);
+            R[(size_t)j * ld + j] = diag;
+        }
+        __syncthreads();
+        const double rjj = diag;
+        for (int c = j + 1 + threadIdx.x; c < nn; c += blockDim.x) {
+            double acc = G[(size_t)c * ld + j];
+            for (int l = 0; l < j; ++l)
+                acc -= R[(size_t)j * ld + l] * R[(size_t)c * ld + l];
+            R[(size_t)c * ld + j] = acc / rjj;
+        }
+        __syncthreads();
+    }
+    for (int c = threadIdx.x; c < nn; c += blockDim.x) {
+        double *x = T + (size_t)c * ld;
+        for (int a = c + 1; a < nn; ++a) x[a] = 0.0;
+        x[c] = 1.0 / R[(size_t)c * ld + c];
+        for (int a = c - 1; a >= 0; --a) {
+            double acc = 0.0;
+            for (int b = a + 1; b <= c; ++b) acc += R[(size_t)b * ld + a] * x[b];
+            x[a] = -acc / R[(size_t)a * ld + a];
+        }
+    }
+    if (threadIdx.x == 0 && fail) tw.status |= TILE_CHOL_FAIL;
+}
+
+void launch_chol_inv(int phase, TileWork *d_tiles, int ntiles, Workspace ws,
+                     cudaStream_t stream)
+{
+    k_chol_inv<<<ntiles, kSmallThreads, 0, stream>>>(d_tiles, ws, phase);
+}
+
+// -------------------------------------------------- one-sided Jacobi
+
+// One-sided Jacobi (Hestenes) on the columns of A = L(slot) (k1 x k2):
+// column pairs are rotated until mutually orthogonal; then the columns
+// of A V are the eigenvectors of L L^T scaled by the singular values.
+// Pairs follow the round-robin tournament ordering, k2/2 disjoint pairs per
+// step, one warp per pair.  W (normalised columns) goes to T(slot), the
+// squared column norms to Sig(slot).  A tile whose columns fit in the
+// dynamic shared memory is rotated there; a larger one in place in global
+// memory (L2-resident).
+constexpr size_t kJacobiSmem = 200 * 1024;
+
+__global__ void __launch_bounds__(kSmallThreads)
+k_jacobi(TileWork *__restrict__ tiles, Workspace ws)
+{
+    extern __shared__ double sm[];
+    __shared__ int rotated;
+    TileWork &tw = tiles[blockIdx.x];
+    const int s = tw.slot;
+    const int rows = tw.k1, cols = tw.k2;
+    if (cols <= 0) return;
+    const int ldg = ws.ldK();
+    const int lds = rows | 1;   // odd stride: fewer bank conflicts
+    const bool in_smem = (size_t)lds * cols * sizeof(double) <= kJacobiSmem;
+    double *A = in_smem ? sm : ws.L(s);
+    const int lda = in_smem ? lds : ldg;
+    if (in_smem) {
+        const double *Lg = ws.L(s);
+        for (int c = 0; c < cols; ++c)
+            for (int i = threadIdx.x; i < rows; i += blockDim.x)
+                A[(size_t)c * lda + i] = Lg[(size_t)c * ldg + i];
+        __syncthreads();
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nwarps = blockDim.x >> 5;
+    const int nc = cols + (cols & 1);      // players, with a bye if odd
+    const int npairs = nc / 2;
+    int sweep = 0;
+    for (; sweep < 40; ++sweep) {
+        if (threadIdx.x == 0) rotated = 0;
+        __syncthreads();
+        for (int step = 0; step < nc - 1; ++step) {
+            for (int p = warp; p < npairs; p += nwarps) {
+                const int a = p == 0 ? 0 : 1 + (p - 1 + step) % (nc - 1);
+                const int b = 1 + (nc - 2 - p + step) % (nc - 1);
+                if (a >= cols || b >= cols) continue;
+                double *ca = A + (size_t)a * lda, *cb = A + (size_t)b * lda;
+                double al = 0.0, be = 0.0, ga = 0.0;
+                for (int i = lane; i < rows; i += 32) {
+                    const double x = ca[i], y = cb[i];
+                    al += x * x;
+                    be += y * y;
+                    ga += x * y;
+                }
+                #pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    al += __shfl_xor_sync(0xffffffffu, al, o);
+                    be += __shfl_xor_sync(0xffffffffu, be, o);
+                    ga += __shfl_xor_sync(0xffffffffu, ga, o);
+                }
+                if (!(fabs(ga) > 1e-15 * sqrt(al * be)) || al == 0.0 || be == 0.0)
+                    continue;
+                const double zeta = (be - al) / (2.0 * ga);
+                const double t = (zeta >= 0.0 ? 1.0 : -1.0) /
+                                 (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+                const double c = 1.0 / sqrt(1.0 + t * t);
+                const double sn = c * t;
+                for (int i = lane; i < rows; i += 32) {
+                    const double x = ca[i], y = cb[i];
+                    ca[i] = c * x - sn * y;
+                    cb[i] = sn * x + c * y;
+                }
+                if (lane == 0) rotated = 1;
+            }
+            __syncthreads();
+        }
+        if (!rotated) break;
+        __syncthreads();
+    }
+    // Normalise into W = T(slot); squared norms into Sig.
+    double *W = ws.T(s);
+    double *sig = ws.Sig(s);
+    for (int c = warp; c < cols; c += nwarps) {
+        const double *ca = A + (size_t)c * lda;
+        double nrm = 0.0;
+        for (int i = lane; i < rows; i += 32) nrm += ca[i] * ca[i];
+        #pragma unroll
+        for (int o = 16; o > 0; o >>= 1) nrm += __shfl_xor_sync(0xffffffffu, nrm, o);
+        const double inv = nrm > 0.0 ? 1.0 / sqrt(nrm) : 0.0;
+        for (int i = lane; i < rows; i += 32) W[(size_t)c * ldg + i] = ca[i] * inv;
+        if (lane == 0) sig[c] = nrm;
+    }
+    if (threadIdx.x == 0 && sweep >= 40) tw.status |= TILE_JACOBI_SLOW;
+}
+
+void launch_jacobi(TileWork *d_tiles, int ntiles, Workspace ws,
+                   cudaStream_t stream)
+{
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kJacobiSmem);
+        attr_set = true;
+    }
+    k_jacobi<<<ntiles, kSmallThreads, kJacobiSmem, stream>>>(d_tiles, ws);
+}
+
+// Appends the residual-pass columns to the basis: k1 += kb.
+__global__ void k_merge_basis(TileWork *__restrict__ tiles, int ntiles)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < ntiles && tiles[t].kb > 0) {
+        tiles[t].k1 += tiles[t].kb;
+        tiles[t].kb = 0;
+    }
+}
+
+void launch_merge_basis(TileWork *d_tiles, int ntiles, cudaStream_t stream)
+{
+    k_merge_basis<<<(ntiles + 127) / 128, 128, 0, stream>>>(d_tiles, ntiles);
+}
+
+// --------------------------------------------------------- rank cut
+
+// Energies e_c = ||C(c, :)||^2 of the rotated rows, order by decreasing
+// energy, then the smallest r >= 1 with
+//   sum_{c >= r} e_c + (||B||_F^2 - sum_c e_c)  <=  tol^2 ||B||_F^2,
+// i.e. starsh_dense_dsvfr applied to the exact energies (0 if B = 0).
+// rank = r if r <= maxrank, else -1.
+__global__ void __launch_bounds__(kSmallThreads)
+k_rank_cut(TileWork *__restrict__ tiles, Workspace ws, double tol,
+           int maxrank)
+{
+    TileWork &tw = tiles[blockIdx.x];
+    const int s = tw.slot;
+    const int k2 = tw.k2;
+    __shared__ double e[kMaxK];
+    __shared__ int ord[kMaxK];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const double *C = ws.C(s);
+    const int ld = ws.ldK();
+    for (int c = warp; c < k2; c += blockDim.x >> 5) {
+        double acc = 0.0;
+        for (int j = lane; j < tw.n; j += 32) {
+            const double v = C[(size_t)j * ld + c];
+            acc += v * v;
+        }
+        #pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) e[c] = acc;
+    }
+    __syncthreads();
+    // Position of c = number of entries ranked before it.
+    for (int c = threadIdx.x; c < k2; c += blockDim.x) {
+        int pos = 0;
+        const double ec = e[c];
+        for (int o = 0; o < k2; ++o)
+            pos += (e[o] > ec) || (e[o] == ec && o < c);
+        ord[pos] = c;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int *gord = ws.Ord(s);
+        double *ge = ws.E(s);
+        double total = 0.0;
+        for (int c = 0; c < k2; ++c) {
+            gord[c] = ord[c];
+            ge[c] = e[ord[c]];
+            total += e[c];
+        }
+        const double energy = tw.tr_h;
+        int r;
+        if (!(energy > 0.0) || k2 == 0) {
+            r = 0;
+        } else {
+            const double budget = tol * tol * energy;
+            const double missing = fmax(0.0, energy - total);
+            // tail(r) for r = k2 down to 1; keep the smallest r that fits
+            double tail = missing;
+            r = -1;
+            if (tail <= budget) r = k2;
+            for (int c = k2 - 1; c >= 1; --c) {
+                tail += ge[c];
+                if (tail <= budget) r = c;
+                else break;
+            }
+            if (r < 0) { r = k2; tw.status |= TILE_TAIL_LEFT; }
+        }
+        tw.rank = r <= maxrank ? r : -1;
+    }
+}
+
+void launch_rank_cut(TileWork *d_tiles, int ntiles, Workspace ws, double tol,
+                     int maxrank, cudaStream_t stream)
+{
+    k_rank_cut<<<ntiles, kSmallThreads, 0, stream>>>(d_tiles, ws, tol, maxrank);
+}
+
+// Wsel(:, c) = W(:, ord[c]) for c < rank, into L(slot).
+__global__ void k_select_w(const TileWork *__restrict__ tiles, Workspace ws)
+{
+    const TileWork tw = tiles[blockIdx.x];
+    if (tw.rank <= 0) return;
+    const int s = tw.slot, ld = ws.ldK();
+    const int *ord = ws.Ord(s);
+    const double *W = ws.T(s);
+    double *dst = ws.L(s);
+    for (int c = 0; c < tw.rank; ++c)
+        for (int i = threadIdx.x; i < tw.k1; i += blockDim.x)
+            dst[(size_t)c * ld + i] = W[(size_t)ord[c] * ld + i];
+}
+
+void launch_select_w(const TileWork *d_tiles, int ntiles, Workspace ws,
+                     cudaStream_t stream)
+{
+    k_select_w<<<ntiles, 256, 0, stream>>>(d_tiles, ws);
+}
+
+// V(j, c) = C(ord[c], j): V is n x rank, leading dimension n.
+__global__ void k_write_v(const TileWork *__restrict__ tiles, Workspace ws,
+                          OutArena out)
+{
+    const TileWork tw = tiles[blockIdx.x];
+    if (tw.rank <= 0) return;
+    const int s = tw.slot, ld = ws.ldK();
+    const int *ord = ws.Ord(s);
+    const double *C = ws.C(s);
+    double *V = out.V + tw.off_v;
+    for (int c = blockIdx.y; c < tw.rank; c += gridDim.y) {
+        const int row = ord[c];
+        for (int j = threadIdx.x; j < tw.n; j += blockDim.x)
+            V[(size_t)c * tw.n + j] = C[(size_t)j * ld + row];
+    }
+}
+
+void launch_write_v(const TileWork *d_tiles, int ntiles, Workspace ws,
+                    OutArena out, cudaStream_t stream)
+{
+    dim3 grid(ntiles, 8);
+    k_write_v<<<grid, 256, 0, stream>>>(d_tiles, ws, out);
+}
+
+}  // namespace b200

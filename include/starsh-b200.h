@@ -119,6 +119,17 @@ int starsh_b200_kernel_register(STARSH_kernel *kernel, int family,
  * *ndim_hint is the dimension fixed by its name (0 for "_nd"). */
 int starsh_b200_kernel_family(STARSH_kernel *kernel, int *ndim_hint);
 
+/* ------------------------------------------------------------ device */
+
+/* Selects the CUDA device the library uses; must be called before any
+ * other B200 call of the process (default: device 0, or the device current
+ * at the first call).  Returns STARSH_SUCCESS or STARSH_WRONG_PARAMETER. */
+int starsh_b200_set_device(int device);
+
+/* The cudaStream_t every library kernel is launched on (for timing with
+ * events and for ordering user work). */
+void *starsh_b200_stream(void);
+
 /* ------------------------------------------------------- diagnostics */
 
 /* Timings and counters of the last approximation on this host thread. */
@@ -138,6 +149,7 @@ typedef struct starsh_b200_stats
     int max_rank;             /* largest accepted rank                  */
     long long h2d_bytes;      /* host to device bytes                   */
     long long d2h_bytes;      /* device to host bytes                   */
+    long long batches;        /* tile batches (launches of each GEMM step) */
 } starsh_b200_stats;
 int starsh_b200_get_stats(starsh_b200_stats *stats);
 

@@ -53,6 +53,7 @@ void DeviceBuffer::release()
 static Context g_ctx;
 static std::once_flag g_ctx_once;
 static bool g_ctx_ok = false;
+static int g_requested_device = -1;
 static thread_local std::string t_error;
 static thread_local starsh_b200_stats t_stats;
 static std::atomic<long long> g_launches{0};
@@ -61,6 +62,12 @@ Context *context()
 {
     std::call_once(g_ctx_once, [] {
         int dev = 0;
+        if (g_requested_device >= 0 &&
+            cudaSetDevice(g_requested_device) != cudaSuccess) {
+            cudaGetLastError();
+            set_error("cudaSetDevice failed");
+            return;
+        }
         if (cudaGetDevice(&dev) != cudaSuccess) {
             cudaGetLastError();
             set_error("no CUDA device available");
@@ -407,6 +414,7 @@ static int compress_far(Context &ctx, const DevKernel &K, STARSH_blrf *F,
             count_launch();
         }
         st.tiles += nt;
+        st.batches += 1;
     }
     for (auto &e : ev) cudaEventDestroy(e);
     if (info == STARSH_SUCCESS)
@@ -713,6 +721,25 @@ extern "C" void starsh_b200_blrm_release(STARSH_blrm *matrix)
     Context *ctx = context();
     if (ctx) cudaStreamSynchronize(ctx->stream);
     delete rec;
+}
+
+extern "C" int starsh_b200_set_device(int device)
+{
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 ||
+        device >= count) {
+        cudaGetLastError();
+        return STARSH_WRONG_PARAMETER;
+    }
+    if (g_ctx_ok && g_ctx.device != device) return STARSH_WRONG_PARAMETER;
+    g_requested_device = device;
+    return STARSH_SUCCESS;
+}
+
+extern "C" void *starsh_b200_stream(void)
+{
+    Context *ctx = context();
+    return ctx ? (void *)ctx->stream : nullptr;
 }
 
 extern "C" int starsh_b200_get_stats(starsh_b200_stats *stats)

@@ -124,7 +124,8 @@ class Stats(Structure):
                 ("tiles", c_longlong), ("false_far", c_longlong),
                 ("entries", c_longlong), ("kernel_launches", c_longlong),
                 ("rank_sum", c_longlong), ("max_rank", c_int),
-                ("h2d_bytes", c_longlong), ("d2h_bytes", c_longlong)]
+                ("h2d_bytes", c_longlong), ("d2h_bytes", c_longlong),
+                ("batches", c_longlong)]
 
 
 def _proto(lib):
@@ -171,6 +172,8 @@ def _proto(lib):
         "starsh_b200_kernel_register": (c_int, [c_void_p, c_int, c_double]),
         "starsh_b200_kernel_family": (c_int, [c_void_p, P(c_int)]),
         "starsh_b200_get_stats": (c_int, [P(Stats)]),
+        "starsh_b200_set_device": (c_int, [c_int]),
+        "starsh_b200_stream": (c_void_p, []),
         "starsh_b200_last_error": (c_char_p, []),
         "starsh_ssdata_init": (c_int, [P(P(SSData)), STARSH_int, c_int,
                                        P(c_double), c_double, c_double,

@@ -395,6 +395,7 @@ static int compress_far(Context &ctx, const DevKernel &K, STARSH_blrf *F,
             rec.chunks.push_back(chunk);
         }
         OutArena out{chunk, chunk ? chunk + nu : nullptr};
+        if (chunk) rec.parts.push_back({out.U, nu, out.V, nv});
         for (int t = 0; t < nt; ++t) {
             const TileWork &w = all[b0 + t];
             if (w.rank > 0) {
@@ -442,21 +443,23 @@ static int fill_host_mirror(STARSH_blrm *M, Record &rec, cudaStream_t s)
         free(hV);
         return STARSH_MALLOC_ERROR;
     }
+    // One copy per factor chunk; views follow the same order.
     size_t ou = 0, ov = 0;
+    for (const Record::Part &pt : rec.parts) {
+        cudaMemcpyAsync(hU + ou, pt.U, pt.nu * sizeof(double),
+                        cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(hV + ov, pt.V, pt.nv * sizeof(double),
+                        cudaMemcpyDeviceToHost, s);
+        ou += pt.nu;
+        ov += pt.nv;
+    }
+    ou = ov = 0;
     for (STARSH_int b = 0; b < F->nblocks_far; ++b) {
         const int r = M->far_rank[b];
-        const size_t nu = (size_t)M->far_U[b]->shape[0] * r;
-        const size_t nv = (size_t)M->far_V[b]->shape[0] * r;
-        if (r > 0) {
-            cudaMemcpyAsync(hU + ou, rec.dU[b], nu * sizeof(double),
-                            cudaMemcpyDeviceToHost, s);
-            cudaMemcpyAsync(hV + ov, rec.dV[b], nv * sizeof(double),
-                            cudaMemcpyDeviceToHost, s);
-        }
         M->far_U[b]->data = hU + ou;
         M->far_V[b]->data = hV + ov;
-        ou += nu;
-        ov += nv;
+        ou += (size_t)M->far_U[b]->shape[0] * r;
+        ov += (size_t)M->far_V[b]->shape[0] * r;
     }
     if (M->onfly == 0 && F->nblocks_near > 0) {
         hD = (double *)malloc(std::max<size_t>(rec.d_total, 1) * sizeof(double));
@@ -465,13 +468,14 @@ static int fill_host_mirror(STARSH_blrm *M, Record &rec, cudaStream_t s)
             free(hV);
             return STARSH_MALLOC_ERROR;
         }
+        // near blocks live in one contiguous device allocation
+        if (rec.d_total)
+            cudaMemcpyAsync(hD, rec.dD[0], rec.d_total * sizeof(double),
+                            cudaMemcpyDeviceToHost, s);
         size_t od = 0;
         for (STARSH_int b = 0; b < F->nblocks_near; ++b) {
-            const size_t nd = M->near_D[b]->size;
-            cudaMemcpyAsync(hD + od, rec.dD[b], nd * sizeof(double),
-                            cudaMemcpyDeviceToHost, s);
             M->near_D[b]->data = hD + od;
-            od += nd;
+            od += M->near_D[b]->size;
         }
     }
     cudaError_t e = cudaStreamSynchronize(s);

@@ -45,6 +45,10 @@ struct Record {
     std::vector<void *> chunks;        // device allocations
     std::vector<double *> dU, dV;      // per far block (device)
     std::vector<double *> dD;          // per near block (device, or null)
+    // Factor chunks in far-block order: the host mirror of U (V) is the
+    // concatenation of the chunks' U (V) parts.
+    struct Part { const double *U; size_t nu; const double *V; size_t nv; };
+    std::vector<Part> parts;
     size_t u_total = 0, v_total = 0, d_total = 0;
     bool host_filled = false;
     DevicePoints *points = nullptr;    // kept for onfly near blocks

@@ -119,6 +119,31 @@ int starsh_b200_kernel_register(STARSH_kernel *kernel, int family,
  * *ndim_hint is the dimension fixed by its name (0 for "_nd"). */
 int starsh_b200_kernel_family(STARSH_kernel *kernel, int *ndim_hint);
 
+/* ------------------------------------------------ no-allocation variant */
+
+/* Randomized-SVD compression of one dense tile already on the device,
+ * without allocating any device memory.  No counterpart in the reference:
+ * it is for callers that cannot call cudaMalloc (inside a stream capture,
+ * under an allocator that owns all device memory, or on threads that must
+ * not wait for the allocator's implicit synchronisation).  Same algorithm,
+ * Gaussian sketch and rank rule as starsh_blrm__drsdd_b200 applied to that
+ * tile; its scratch is a fixed __device__ array of about 1.9 MB that every
+ * GPU loading the library keeps until the process exits.
+ *   dD      nrows x ncols tile, column-major, leading dimension ldd;
+ *   dU      receives nrows x rank, leading dimension nrows;
+ *   dV      receives ncols x rank, leading dimension ncols (U V^T ~ D);
+ *           both need room for maxrank columns;
+ *   d_rank  device int: the rank, or -1 when it exceeds maxrank;
+ *   stream  cudaStream_t (NULL: default stream); the call is asynchronous.
+ * Limits: nrows, ncols <= 256 and min(maxrank + oversample, nrows, ncols)
+ * <= 96; beyond them STARSH_WRONG_PARAMETER.  The first call on a device
+ * looks up the scratch address (cudaGetSymbolAddress) and should come
+ * before any stream capture.  All calls share the scratch: calls that
+ * overlap on the GPU race. */
+int starsh_b200_dense_rsvd_noalloc(const double *dD, int nrows, int ncols,
+        int ldd, int maxrank, int oversample, double tol, double *dU,
+        double *dV, int *d_rank, void *stream);
+
 /* ------------------------------------------------------------ device */
 
 /* Selects the CUDA device the library uses; must be called before any

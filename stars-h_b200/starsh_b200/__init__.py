@@ -173,6 +173,11 @@ def _proto(lib):
         "starsh_b200_kernel_family": (c_int, [c_void_p, P(c_int)]),
         "starsh_b200_get_stats": (c_int, [P(Stats)]),
         "starsh_b200_set_device": (c_int, [c_int]),
+        "starsh_b200_dense_rsvd_noalloc": (c_int, [c_void_p, c_int, c_int,
+                                                   c_int, c_int, c_int,
+                                                   c_double, c_void_p,
+                                                   c_void_p, c_void_p,
+                                                   c_void_p]),
         "starsh_b200_stream": (c_void_p, []),
         "starsh_b200_last_error": (c_char_p, []),
         "starsh_ssdata_init": (c_int, [P(P(SSData)), STARSH_int, c_int,

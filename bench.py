@@ -197,6 +197,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--engine", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--n", type=int, default=WORKLOAD["N"],
+                    help="points (a smaller N profiles the same kernels)")
+    ap.add_argument("--no-cpu", action="store_true",
+                    help="skip the CPU baseline leg")
     ap.add_argument("--_cpu-run", type=int, default=0, dest="cpu_run")
     args = ap.parse_args()
     if args.cpu_run:
@@ -206,7 +210,10 @@ def main():
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local = int(os.environ.get("LOCAL_RANK", 0))
-    wl = WORKLOAD
+    wl = dict(WORKLOAD)
+    if args.n != wl["N"]:
+        wl["N"] = args.n
+        wl["workload"] = wl["workload"].replace("N102400", f"N{args.n}")
     threads = len(os.sched_getaffinity(0))
 
     if args.impl == "reference":
@@ -357,7 +364,7 @@ def main():
                      "traffic": None},
         "clocks": clocks.summary(),
     }
-    if world == 1:
+    if world == 1 and not args.no_cpu:
         try:
             r = cpu_reference_run(CPU_SAMPLE_N, threads, wl)
             line["cpu_baseline"] = {

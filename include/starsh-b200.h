@@ -175,6 +175,7 @@ typedef struct starsh_b200_stats
     long long h2d_bytes;      /* host to device bytes                   */
     long long d2h_bytes;      /* device to host bytes                   */
     long long batches;        /* tile batches (launches of each GEMM step) */
+    long long sketch_launches;/* sketch GEMM launches (timed by sketch_ms) */
 } starsh_b200_stats;
 int starsh_b200_get_stats(starsh_b200_stats *stats);
 

@@ -24,6 +24,7 @@ struct Context {
     DeviceBuffer tiles;        // TileWork array of a batch
     DeviceBuffer descs;        // GemmDesc array of a batch
     DeviceBuffer omega;        // Gaussian sketch matrix
+    DeviceBuffer flag;         // round flag of the adaptive sketch
     size_t omega_count = 0;
     unsigned long long omega_seed = 0;
     std::mutex lock;           // one approximation / dmml at a time

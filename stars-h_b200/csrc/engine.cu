@@ -228,6 +228,8 @@ struct EngineParams {
     double tol;
     int oversample;
     int engine;
+    int block;      // adaptive sketch: columns of the first round
+    int block_next; // ... and of every later round
 };
 
 // Runs the device pipeline over all far blocks of F.  Fills ranks (host)
@@ -294,7 +296,8 @@ static int compress_far(Context &ctx, const DevKernel &K, STARSH_blrf *F,
     ws.base = (double *)ctx.workspace.ptr;
     ws.stride = stride;
     if (!ctx.tiles.reserve((size_t)slots * sizeof(TileWork)) ||
-        !ctx.descs.reserve((size_t)slots * sizeof(GemmDesc)))
+        !ctx.descs.reserve((size_t)slots * sizeof(GemmDesc)) ||
+        !ctx.flag.reserve(256))
         return cuda_fail(cudaErrorMemoryAllocation, "batch arrays");
     TileWork *dt = (TileWork *)ctx.tiles.ptr;
     GemmDesc *dd = (GemmDesc *)ctx.descs.ptr;
@@ -320,6 +323,7 @@ static int compress_far(Context &ctx, const DevKernel &K, STARSH_blrf *F,
                         cudaMemcpyHostToDevice, s);
         launch_gen_tiles(K, dt, nt, ws, s);
         count_launch();
+        if (ep.engine == STARSH_B200_FP64) {
         cudaEventRecord(ev[0], s);
         if ((info = gemm(STEP_SKETCH, false, false, nt, m_max, k_max, none))) break;
         cudaEventRecord(ev[1], s);
@@ -349,6 +353,81 @@ static int compress_far(Context &ctx, const DevKernel &K, STARSH_blrf *F,
         if ((info = gemm(STEP_QB, false, false, nt, m_max, k_max, none))) break;
         launch_merge_basis(dt, nt, s);
         count_launch();
+        float ms = 0.f;
+        cudaEventSynchronize(ev[1]);
+        cudaEventElapsedTime(&ms, ev[0], ev[1]);
+        st.sketch_ms += ms;
+        st.sketch_launches += 1;
+        } else {
+        // Adaptive sketch: sample Omega in blocks; each round projects the
+        // new sample off the basis, keeps the residual directions above
+        // (tol/10)^2 ||D||_F^2 and stops a tile when a round adds none
+        // (the residual estimate of N. Halko, P.-G. Martinsson, J. A. Tropp,
+        // SIAM Review 53 (2011) sec. 4.3) or after k columns.
+        launch_block_norms(dt, dt, nt, ws, s);
+        count_launch();
+        int *d_active = (int *)ctx.flag.ptr;
+        // a repeat pass can only be needed when (tol/10)^2 lies below the
+        // squared-noise floor of a Gram
+        const bool may_repeat = 0.01 * ep.tol * ep.tol < 1e-15;
+        auto append = [&](int bmax) -> int {
+            // orthonormalise the selected residual columns (kb of them)
+            // against the basis and append them: CholQR of R_J, one more
+            // projection, CholQR again (CGS2)
+            int e;
+            launch_gather_cols(1, dt, nt, ws, s);
+            count_launch();
+            if ((e = gemm(STEP_A_Q1B, false, false, nt, m_max, bmax, none))) return e;
+            if ((e = gemm(STEP_A_ORTH_Z, true, false, nt, k_max, bmax, none))) return e;
+            if ((e = gemm(STEP_A_ORTH_R, false, false, nt, m_max, bmax, none))) return e;
+            if ((e = gemm(STEP_A_GRAM_R, true, false, nt, bmax, bmax, none))) return e;
+            launch_chol_inv(1, dt, nt, ws, s);
+            count_launch();
+            if ((e = gemm(STEP_A_QB, false, false, nt, m_max, bmax, none))) return e;
+            launch_merge_basis(dt, nt, s);
+            count_launch();
+            return STARSH_SUCCESS;
+        };
+        for (int round = 0; info == STARSH_SUCCESS; ++round) {
+            const int block = round == 0 ? ep.block : ep.block_next;
+            launch_round_setup(dt, nt, block, d_active, s);
+            count_launch();
+            int active = 0;
+            B200_CUDA(cudaMemcpyAsync(&active, d_active, sizeof(int),
+                                      cudaMemcpyDeviceToHost, s), "round flag");
+            B200_CUDA(cudaStreamSynchronize(s), "round flag");
+            if (!active) break;
+            const int bmax = std::min(block, k_max);
+            cudaEventRecord(ev[0], s);
+            if ((info = gemm(STEP_A_SKETCH, false, false, nt, m_max, bmax, none))) break;
+            cudaEventRecord(ev[1], s);
+            if (round > 0) {
+                if ((info = gemm(STEP_A_RES_Z, true, false, nt, k_max, bmax, none))) break;
+                if ((info = gemm(STEP_A_RES_Y, false, false, nt, m_max, bmax, none))) break;
+            }
+            if ((info = gemm(STEP_A_GRAM, true, false, nt, bmax, bmax, none))) break;
+            launch_round_pivchol(dt, nt, ws, ep.tol, 0, s);
+            count_launch();
+            if ((info = append(bmax))) break;
+            if (may_repeat) {
+                // same sample, projected off the grown basis once more
+                if ((info = gemm(STEP_A_RES_Z2, true, false, nt, k_max, bmax, none))) break;
+                if ((info = gemm(STEP_A_RES_Y2, false, false, nt, m_max, bmax, none))) break;
+                if ((info = gemm(STEP_A_GRAM2, true, false, nt, bmax, bmax, none))) break;
+                launch_round_pivchol(dt, nt, ws, ep.tol, 1, s);
+                count_launch();
+                if ((info = append(bmax))) break;
+            }
+            launch_round_end(dt, nt, s);
+            count_launch();
+            float ms = 0.f;
+            cudaEventSynchronize(ev[1]);
+            cudaEventElapsedTime(&ms, ev[0], ev[1]);
+            st.sketch_ms += ms;
+            st.sketch_launches += 1;
+        }
+        if (info) break;
+        }
         // projection and small SVD
         cudaEventRecord(ev[2], s);
         if ((info = gemm(STEP_PROJECT, true, false, nt, k_max, n_max, none))) break;
@@ -365,15 +444,14 @@ static int compress_far(Context &ctx, const DevKernel &K, STARSH_blrf *F,
                   "cudaMemcpyAsync(tiles)");
         B200_CUDA(cudaStreamSynchronize(s), "compression pipeline");
         float ms = 0.f;
-        cudaEventElapsedTime(&ms, ev[0], ev[1]);
-        st.sketch_ms += ms;
         cudaEventElapsedTime(&ms, ev[2], ev[3]);
         st.project_ms += ms;
         // Output placement of this batch: one device chunk for U and V.
         size_t nu = 0, nv = 0;
         for (int t = 0; t < nt; ++t) {
             TileWork &w = all[b0 + t];
-            st.sketch_flops += 2.0 * w.m * w.n * w.k;
+            st.sketch_flops += 2.0 * w.m * w.n *
+                (ep.engine == STARSH_B200_FP64 ? w.k : w.cols_done);
             st.project_flops += 2.0 * w.m * w.n * w.k1;
             if (w.status & TILE_CHOL_FAIL) {
                 set_error("re-orthogonalisation failed on a tile");
@@ -505,8 +583,8 @@ static int approximate(STARSH_blrm **matrix, STARSH_blrf *F, int maxrank,
         set_error("invalid argument");
         return STARSH_WRONG_PARAMETER;
     }
-    if (engine != STARSH_B200_FP64) {
-        set_error("engine not available in this build");
+    if (engine != STARSH_B200_FP64 && engine != STARSH_B200_MIXED) {
+        set_error("unknown engine");
         return STARSH_WRONG_PARAMETER;
     }
     Context *ctx = context();
@@ -532,7 +610,13 @@ static int approximate(STARSH_blrm **matrix, STARSH_blrf *F, int maxrank,
     auto *rec = new Record();
     rec->points = points;
     std::vector<int> rank;
-    EngineParams ep{maxrank, tol, b200_oversample(), engine};
+    int block = 64, block_next = 32;
+    if (const char *e = getenv("STARSH_B200_SKETCH_BLOCK"))
+        block = std::max(8, std::min(1024, atoi(e)));
+    if (const char *e = getenv("STARSH_B200_SKETCH_STEP"))
+        block_next = std::max(8, std::min(1024, atoi(e)));
+    EngineParams ep{maxrank, tol, b200_oversample(), engine, block,
+                    block_next};
     info = compress_far(*ctx, points->K, F, ep, rank, *rec);
     if (info) {
         delete rec;

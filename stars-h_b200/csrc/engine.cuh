@@ -28,6 +28,12 @@ struct TileWork {
     int need_pass_b;        // residual pass required by tol
     double tr_g;            // trace of the sketch Gram Y^T Y
     double tr_h;            // ||B||_F^2 = trace of B B^T
+    // adaptive sketch (mixed engine)
+    double dnorm2;          // ||D||_F^2 of the block, exact (FP64)
+    int cols_done;          // sketch columns consumed so far
+    int bcur;               // columns of the current round (0: inactive)
+    int done;               // sampling finished (converged or capped)
+    int kround;             // directions the current round's sample added
     long long off_u, off_v; // output offsets (doubles)
 };
 
@@ -37,7 +43,7 @@ struct Workspace {
     double *base;
     size_t stride;          // doubles per slot
     int m_max, n_max, k_max;
-    size_t oD, oY, oQ1, oQ, oS, oL, oT, oB, oC, oE, oSig, oPiv, oOrd;
+    size_t oD, oY, oQ1, oQ, oS, oL, oT, oB, oC, oE, oSig, oPiv, oOrd, oNrm, oR;
 
     __host__ __device__ double *D(int s) const { return base + s * stride + oD; }
     __host__ __device__ double *Y(int s) const { return base + s * stride + oY; }
@@ -52,6 +58,10 @@ struct Workspace {
     __host__ __device__ double *Sig(int s) const { return base + s * stride + oSig; }
     __host__ __device__ int *Piv(int s) const { return (int *)(base + s * stride + oPiv); }
     __host__ __device__ int *Ord(int s) const { return (int *)(base + s * stride + oOrd); }
+    // per-CTA partial sums of squares of the generated block
+    __host__ __device__ double *Nrm(int s) const { return base + s * stride + oNrm; }
+    // m x k temporary of the adaptive rounds (ld = m_max)
+    __host__ __device__ double *R(int s) const { return base + s * stride + oR; }
     // leading dimensions
     __host__ __device__ int ldD() const { return m_max; }
     __host__ __device__ int ldM() const { return m_max; }   // Y, Q1, Q
@@ -81,6 +91,18 @@ enum GemmStep : int {
     STEP_GRAM_B,         // S  = B B^T                    (k1 x k1)
     STEP_ROTATE,         // C  = W^T B   (W in T)         (k2 x n)
     STEP_OUT_U,          // U  = Q Wsel  (Wsel in L)      (m x r)
+    STEP_A_SKETCH,       // Y  = D Omega[:, c:c+b]        (m x b)    adaptive
+    STEP_A_RES_Z,        // S  = Q^T Y                    (k1 x b)   adaptive
+    STEP_A_RES_Y,        // Y -= Q S                      (m x b)    adaptive
+    STEP_A_GRAM,         // S  = Y^T Y                    (b x b)    adaptive
+    STEP_A_RES_Z2,       // second projection of the same sample (repeat
+    STEP_A_RES_Y2,       //   pass, tiles flagged need_pass_b)
+    STEP_A_GRAM2,
+    STEP_A_Q1B,          // R  = Q1 T   (gathered residual columns)
+    STEP_A_ORTH_Z,       // S  = Q^T R
+    STEP_A_ORTH_R,       // R -= Q S
+    STEP_A_GRAM_R,       // S  = R^T R
+    STEP_A_QB,           // Q[:, k1:k1+kb] = R T
 };
 
 struct OutArena {
@@ -107,6 +129,16 @@ void launch_jacobi(TileWork *d_tiles, int ntiles, Workspace ws,
 void launch_rank_cut(TileWork *d_tiles, int ntiles, Workspace ws,
                      double tol, int maxrank, cudaStream_t stream);
 void launch_merge_basis(TileWork *d_tiles, int ntiles, cudaStream_t stream);
+// Adaptive sketch: squared Frobenius norms of the generated blocks, round
+// set-up (returns through d_active whether any tile still samples) and the
+// per-round pivoted Cholesky of the residual block's Gram.
+void launch_block_norms(const TileWork *d_tiles, TileWork *d_rw, int ntiles,
+                        Workspace ws, cudaStream_t stream);
+void launch_round_setup(TileWork *d_tiles, int ntiles, int block,
+                        int *d_active, cudaStream_t stream);
+void launch_round_end(TileWork *d_tiles, int ntiles, cudaStream_t stream);
+void launch_round_pivchol(TileWork *d_tiles, int ntiles, Workspace ws,
+                          double tol, int repeat, cudaStream_t stream);
 void launch_select_w(const TileWork *d_tiles, int ntiles, Workspace ws,
                      cudaStream_t stream);
 void launch_write_v(const TileWork *d_tiles, int ntiles, Workspace ws,

@@ -50,27 +50,82 @@ size_t workspace_layout(Workspace &w, int m_max, int n_max, int k_max,
     w.oSig = take(k_max);
     w.oPiv = take((k_max + 1) / 2);
     w.oOrd = take((k_max + 1) / 2);
+    w.oNrm = take((size_t)((m_max + 63) / 64) * ((n_max + 63) / 64));
+    w.oR = take((size_t)m_max * k_max);
     w.stride = o;
     return o;
 }
 
 // -------------------------------------------------------- generation
 
-// D(slot) = block of the tile, column-major with ld = m_max.  Threads run
-// down a column so that stores are coalesced.
+// D(slot) = block of the tile, column-major with ld = m_max.  A CTA owns a
+// 64 x 64 sub-block: the coordinates of its 64 rows and 64 columns are
+// gathered through the cluster pivots into shared memory once (point-major
+// layouts and dimensions above kStageDim read global memory directly),
+// then each thread evaluates 16 entries of one row, so stores run down the
+// columns and are coalesced.  The CTA also writes the sum of squares of its
+// entries to Nrm(slot) (deterministic per-tile norms for the adaptive
+// sketch).
+constexpr int kStageDim = 4;
+
 __global__ void __launch_bounds__(256)
 k_gen_tiles(DevKernel K, const TileWork *__restrict__ tiles, Workspace ws)
 {
     const TileWork tw = tiles[blockIdx.z];
-    const int i = blockIdx.x * 64 + (threadIdx.x & 63);
-    const int jb = blockIdx.y * 64 + (threadIdx.x >> 6);
     if (blockIdx.x * 64 >= tw.m || blockIdx.y * 64 >= tw.n) return;
+    __shared__ double rc[kStageDim][64], cc[kStageDim][64];
+    __shared__ long long ri[64], ci[64];
+    __shared__ double red[8];
+    const int t = threadIdx.x;
+    const int i0 = blockIdx.x * 64, j0 = blockIdx.y * 64;
+    const bool staged = !K.aos && K.ndim <= kStageDim;
+    if (t < 64) {
+        const int i = min(i0 + t, tw.m - 1);
+        ri[t] = K.row_piv[tw.row0 + i];
+    } else if (t < 128) {
+        const int j = min(j0 + t - 64, tw.n - 1);
+        ci[t - 64] = K.col_piv[tw.col0 + j];
+    }
+    __syncthreads();
+    if (staged) {
+        for (int q = t; q < 64 * K.ndim; q += 256) {
+            const int d = q / 64, e = q % 64;
+            rc[d][e] = K.row_pt[d * K.row_count + ri[e]];
+            cc[d][e] = K.col_pt[d * K.col_count + ci[e]];
+        }
+    }
+    __syncthreads();
+    const int ii = t & 63, i = i0 + ii;
     double *D = ws.D(tw.slot);
     const int ld = ws.ldD();
-    if (i >= tw.m) return;
-    for (int c = 0; c < 16; ++c) {
-        const int j = jb + 4 * c;
-        if (j < tw.n) D[(size_t)j * ld + i] = block_entry(K, tw.row0, tw.col0, i, j);
+    double ss = 0.0;
+    if (i < tw.m) {
+        for (int c = 0; c < 16; ++c) {
+            const int jj = (t >> 6) + 4 * c, j = j0 + jj;
+            if (j >= tw.n) break;
+            double v;
+            if (staged) {
+                double dist = 0.0;
+                for (int d = 0; d < K.ndim; ++d) {
+                    const double q = __dsub_rn(rc[d][ii], cc[d][jj]);
+                    dist = __dadd_rn(dist, __dmul_rn(q, q));
+                }
+                v = entry_from_dist(K, dist, ri[ii], ci[jj]);
+            } else {
+                v = entry_from_dist(K, sq_dist(K, ri[ii], ci[jj]), ri[ii], ci[jj]);
+            }
+            D[(size_t)j * ld + i] = v;
+            ss += v * v;
+        }
+    }
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) ss += __shfl_down_sync(0xffffffffu, ss, o);
+    if ((t & 31) == 0) red[t >> 5] = ss;
+    __syncthreads();
+    if (t == 0) {
+        double a = 0.0;
+        for (int w = 0; w < 8; ++w) a += red[w];
+        ws.Nrm(tw.slot)[blockIdx.x * ((ws.n_max + 63) / 64) + blockIdx.y] = a;
     }
 }
 
@@ -257,6 +312,93 @@ __global__ void k_make_desc(GemmStep step, const TileWork *__restrict__ tiles,
         d.C = ws.C(s); d.ldc = ldk;
         d.M = tw.k2; d.N = tw.n; d.K = tw.k1;
         break;
+    case STEP_A_SKETCH: // NN: Y = D Omega[:, c:c+b]
+        if (tw.bcur <= 0) break;
+        d.A = ws.D(s); d.lda = ws.ldD();
+        d.B = omega + (size_t)tw.cols_done * ld_omega; d.ldb = ld_omega;
+        d.C = ws.Y(s); d.ldc = ldm;
+        d.M = tw.m; d.N = tw.bcur; d.K = tw.n;
+        break;
+    case STEP_A_RES_Z:  // TN: S = Q^T Y
+        if (tw.bcur <= 0 || tw.k1 <= 0) break;
+        d.A = ws.Q(s); d.lda = ldm;
+        d.B = ws.Y(s); d.ldb = ldm;
+        d.C = ws.S(s); d.ldc = ldk;
+        d.M = tw.k1; d.N = tw.bcur; d.K = tw.m;
+        break;
+    case STEP_A_RES_Y:  // NN: Y -= Q S
+        if (tw.bcur <= 0 || tw.k1 <= 0) break;
+        d.A = ws.Q(s); d.lda = ldm;
+        d.B = ws.S(s); d.ldb = ldk;
+        d.C = ws.Y(s); d.ldc = ldm;
+        d.alpha = -1.0; d.beta = 1.0;
+        d.M = tw.m; d.N = tw.bcur; d.K = tw.k1;
+        break;
+    case STEP_A_GRAM:   // TN: S = Y^T Y
+        if (tw.bcur <= 0) break;
+        d.A = ws.Y(s); d.lda = ldm;
+        d.B = ws.Y(s); d.ldb = ldm;
+        d.C = ws.S(s); d.ldc = ldk;
+        d.M = tw.bcur; d.N = tw.bcur; d.K = tw.m;
+        break;
+    case STEP_A_RES_Z2: // TN: S = Q^T Y, repeat pass on the same sample
+        if (!tw.need_pass_b || tw.bcur <= 0) break;
+        d.A = ws.Q(s); d.lda = ldm;
+        d.B = ws.Y(s); d.ldb = ldm;
+        d.C = ws.S(s); d.ldc = ldk;
+        d.M = tw.k1; d.N = tw.bcur; d.K = tw.m;
+        break;
+    case STEP_A_RES_Y2: // NN: Y -= Q S
+        if (!tw.need_pass_b || tw.bcur <= 0) break;
+        d.A = ws.Q(s); d.lda = ldm;
+        d.B = ws.S(s); d.ldb = ldk;
+        d.C = ws.Y(s); d.ldc = ldm;
+        d.alpha = -1.0; d.beta = 1.0;
+        d.M = tw.m; d.N = tw.bcur; d.K = tw.k1;
+        break;
+    case STEP_A_GRAM2:  // TN: S = Y^T Y
+        if (!tw.need_pass_b || tw.bcur <= 0) break;
+        d.A = ws.Y(s); d.lda = ldm;
+        d.B = ws.Y(s); d.ldb = ldm;
+        d.C = ws.S(s); d.ldc = ldk;
+        d.M = tw.bcur; d.N = tw.bcur; d.K = tw.m;
+        break;
+    case STEP_A_Q1B:    // NN: R = Q1buf(gathered residual columns) T
+        if (tw.kb <= 0) break;
+        d.A = ws.Q1(s); d.lda = ldm;
+        d.B = ws.T(s); d.ldb = ldk;
+        d.C = ws.R(s); d.ldc = ldm;
+        d.M = tw.m; d.N = tw.kb; d.K = tw.kb;
+        break;
+    case STEP_A_ORTH_Z: // TN: S = Q^T R
+        if (tw.kb <= 0 || tw.k1 <= 0) break;
+        d.A = ws.Q(s); d.lda = ldm;
+        d.B = ws.R(s); d.ldb = ldm;
+        d.C = ws.S(s); d.ldc = ldk;
+        d.M = tw.k1; d.N = tw.kb; d.K = tw.m;
+        break;
+    case STEP_A_ORTH_R: // NN: R -= Q S
+        if (tw.kb <= 0 || tw.k1 <= 0) break;
+        d.A = ws.Q(s); d.lda = ldm;
+        d.B = ws.S(s); d.ldb = ldk;
+        d.C = ws.R(s); d.ldc = ldm;
+        d.alpha = -1.0; d.beta = 1.0;
+        d.M = tw.m; d.N = tw.kb; d.K = tw.k1;
+        break;
+    case STEP_A_GRAM_R: // TN: S = R^T R
+        if (tw.kb <= 0) break;
+        d.A = ws.R(s); d.lda = ldm;
+        d.B = ws.R(s); d.ldb = ldm;
+        d.C = ws.S(s); d.ldc = ldk;
+        d.M = tw.kb; d.N = tw.kb; d.K = tw.m;
+        break;
+    case STEP_A_QB:     // NN: Q[:, k1:k1+kb] = R T
+        if (tw.kb <= 0) break;
+        d.A = ws.R(s); d.lda = ldm;
+        d.B = ws.T(s); d.ldb = ldk;
+        d.C = ws.Q(s) + (size_t)tw.k1 * ldm; d.ldc = ldm;
+        d.M = tw.m; d.N = tw.kb; d.K = tw.kb;
+        break;
     case STEP_OUT_U:    // NN: U = Q Wsel, Wsel in L
         if (tw.rank <= 0) break;
         d.A = ws.Q(s); d.lda = ldm;
@@ -337,7 +479,9 @@ __device__ double block_sum(double x, double *red)
 
 // ------------------------------------------------ pivoted Cholesky
 
-enum : int { PH_A = 0, PH_B = 1, PH_H = 2 };
+// Phases: A/B basis passes of the fixed-width sketch, H small SVD, R a
+// round of the adaptive sketch, R2 its repeat pass on the same sample.
+enum : int { PH_A = 0, PH_B = 1, PH_H = 2, PH_R = 3, PH_R2 = 4 };
 
 constexpr int kSmallThreads = 256;
 constexpr int kMaxK = 1024;   // largest sketch width handled by one CTA
@@ -360,9 +504,16 @@ k_pivchol(TileWork *__restrict__ tiles, Workspace ws, int phase, double tol)
 
     int nn;
     if (phase == PH_H) nn = tw.k1;
+    else if (phase == PH_R) nn = tw.bcur;
+    else if (phase == PH_R2) nn = tw.need_pass_b ? tw.bcur : 0;
     else nn = tw.k;
-    if (phase == PH_B && !tw.need_pass_b) {
-        if (threadIdx.x == 0) tw.kb = 0;
+    if ((phase == PH_B && !tw.need_pass_b) ||
+        ((phase == PH_R || phase == PH_R2) && nn <= 0)) {
+        if (threadIdx.x == 0) {
+            tw.kb = 0;
+            if (phase == PH_R) tw.kround = 0;
+            if (phase == PH_R2) tw.need_pass_b = 0;
+        }
         return;
     }
     const double *G = ws.S(s);
@@ -395,6 +546,17 @@ k_pivchol(TileWork *__restrict__ tiles, Workspace ws, int phase, double tol)
     } else if (phase == PH_B) {
         thr = fmax(1e-15 * dmax, 0.01 * tol * tol * tw.tr_g / tw.k);
         cap = tw.k - tw.k1;
+    } else if (phase == PH_R || phase == PH_R2) {
+        // residual columns r_i = (I - Q Q^T) D w_i have E||r_i||^2 =
+        // ||(I - Q Q^T) D||_F^2: keep directions above (tol/10)^2 ||D||_F^2.
+        // When the squared-noise floor of this Gram hides part of that
+        // range, the same sample is projected and searched once more.
+        const double noise = 1e-15 * dmax;
+        const double floor_ = 0.01 * tol * tol * tw.dnorm2;
+        thr = fmax(noise, floor_);
+        cap = min(nn, tw.k - tw.k1);
+        if (threadIdx.x == 0)
+            tw.need_pass_b = phase == PH_R && noise > floor_;
     } else {
         thr = 1e-18 * dmax;
         if (threadIdx.x == 0) tw.tr_h = trace;
@@ -436,8 +598,12 @@ k_pivchol(TileWork *__restrict__ tiles, Workspace ws, int phase, double tol)
     const int cnt = j;
     if (threadIdx.x == 0) {
         if (phase == PH_A) tw.k1 = cnt;
-        else if (phase == PH_B) tw.kb = cnt;
+        else if (phase == PH_B || phase == PH_R || phase == PH_R2) tw.kb = cnt;
         else tw.k2 = cnt;
+        if (phase == PH_R) {
+            tw.kround = cnt;
+            if (cnt == 0) tw.need_pass_b = 0;
+        }
     }
     if (phase == PH_H) return;
     // T = R11^{-1}, R11(a, b) = L(piv[b], a) for a <= b (upper triangular).
@@ -452,6 +618,87 @@ k_pivchol(TileWork *__restrict__ tiles, Workspace ws, int phase, double tol)
             x[a] = -acc / L[(size_t)a * ld + piv[a]];
         }
     }
+}
+
+void launch_round_pivchol(TileWork *d_tiles, int ntiles, Workspace ws,
+                          double tol, int repeat, cudaStream_t stream)
+{
+    k_pivchol<<<ntiles, kSmallThreads, 0, stream>>>(d_tiles, ws,
+                                                    repeat ? PH_R2 : PH_R, tol);
+}
+
+// ||D||_F^2 of every block from the generator's per-CTA partial sums, in a
+// fixed order.
+__global__ void k_block_norms(TileWork *__restrict__ tiles, Workspace ws)
+{
+    TileWork &tw = tiles[blockIdx.x];
+    const int gx = (tw.m + 63) / 64, gy = (tw.n + 63) / 64;
+    const int ldn = (ws.n_max + 63) / 64;
+    __shared__ double red[8];
+    double a = 0.0;
+    for (int q = threadIdx.x; q < gx * gy; q += blockDim.x)
+        a += ws.Nrm(tw.slot)[(q / gy) * ldn + q % gy];
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = a;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+        tw.dnorm2 = s;
+    }
+}
+
+void launch_block_norms(const TileWork *, TileWork *d_rw, int ntiles,
+                        Workspace ws, cudaStream_t stream)
+{
+    k_block_norms<<<ntiles, 256, 0, stream>>>(d_rw, ws);
+}
+
+// Start of a sampling round: tiles not done sample min(block, k - cols)
+// more columns; *active becomes 1 if any tile samples.
+__global__ void k_round_setup(TileWork *__restrict__ tiles, int ntiles,
+                              int block, int *active)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntiles) return;
+    TileWork &tw = tiles[t];
+    if (tw.done || tw.cols_done >= tw.k) {
+        tw.bcur = 0;
+        tw.done = 1;
+        return;
+    }
+    tw.bcur = min(block, tw.k - tw.cols_done);
+    atomicOr(active, 1);
+}
+
+void launch_round_setup(TileWork *d_tiles, int ntiles, int block,
+                        int *d_active, cudaStream_t stream)
+{
+    cudaMemsetAsync(d_active, 0, sizeof(int), stream);
+    k_round_setup<<<(ntiles + 127) / 128, 128, 0, stream>>>(d_tiles, ntiles,
+                                                            block, d_active);
+}
+
+// End of a round: the new orthonormal columns join the basis; a round that
+// found no direction above the threshold (or exhausted the k columns)
+// finishes the tile.
+__global__ void k_round_end(TileWork *__restrict__ tiles, int ntiles)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntiles) return;
+    TileWork &tw = tiles[t];
+    if (tw.bcur <= 0) return;
+    tw.cols_done += tw.bcur;
+    if (tw.kround == 0 || tw.cols_done >= tw.k) tw.done = 1;
+    tw.k1 += tw.kb;       // (kb is 0 here: each pass merged its columns)
+    tw.kb = 0;
+    tw.bcur = 0;
+}
+
+void launch_round_end(TileWork *d_tiles, int ntiles, cudaStream_t stream)
+{
+    k_round_end<<<(ntiles + 127) / 128, 128, 0, stream>>>(d_tiles, ntiles);
 }
 
 void launch_pivchol(int phase, const TileWork *, TileWork *d_tiles_rw,

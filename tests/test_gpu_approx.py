@@ -17,14 +17,14 @@ from harness import RefProblem, approximate_b200, as_ref_blrm
 
 
 def _compare(ref, lib, kind, n, nb, maxrank, tol, oversample=10, rank_slack=3,
-             err_slack=1.6, **kw):
+             err_slack=1.6, engine=sb.ENGINE_FP64, **kw):
     pr = RefProblem(ref, kind, n, nb, **kw)
     Mref = ref.approximate(pr.F, maxrank, tol, oversample=oversample)
     err_ref = ref.dfe(Mref)
     cref = oracle.blrm_contents(Mref)
     pb = RefProblem(ref, kind, n, nb, **kw)
     M = approximate_b200(lib, pb.b200_format(), maxrank, tol,
-                         oversample=oversample)
+                         oversample=oversample, engine=engine)
     Mr = as_ref_blrm(M)
     err = ref.dfe(Mr)
     c = oracle.blrm_contents(Mr)
@@ -112,3 +112,32 @@ def test_unknown_kernel_is_an_error(ref, lib):
     info = lib.starsh_b200_approximate(ctypes.byref(M), pr.b200_format(), 10,
                                        1e-5, 0, 0, 1)
     assert info == sb.WRONG_PARAMETER
+
+
+# ------------------------------------------------------------------ mixed
+# The mixed engine samples the sketch adaptively (blocks of 64 columns until
+# the FP64 residual estimate is below (tol/10)^2 ||D||_F^2, at most
+# maxrank + oversample columns); parity is judged exactly as above.
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", [
+    dict(kind="spatial", n=3600, nb=400, maxrank=100, tol=1e-5,
+         kernel_name="exp", beta=0.1),
+    dict(kind="spatial", n=4096, nb=512, maxrank=128, tol=1e-7, oversample=16,
+         kernel_name="sqexp", beta=0.1),
+    dict(kind="coulomb", n=2048, nb=256, maxrank=100, tol=1e-5, ndim=3, place=1),
+    dict(kind="sin", n=2048, nb=256, maxrank=100, tol=1e-5, ndim=3, place=1,
+         wave_k=20.0, diag=1.0),
+    dict(kind="spatial", n=3000, nb=400, maxrank=100, tol=1e-5,
+         kernel_name="exp", beta=0.1, symm=b"S"),
+])
+def test_mixed_engine_matches_reference(ref, lib, case):
+    case = dict(case)
+    kind, n, nb = case.pop("kind"), case.pop("n"), case.pop("nb")
+    maxrank, tol = case.pop("maxrank"), case.pop("tol")
+    err, err_ref, c, cref, st = _compare(ref, lib, kind, n, nb, maxrank, tol,
+                                         engine=sb.ENGINE_MIXED, **case)
+    assert err <= tol
+    # never more sketch columns than the fixed-width reference sketch
+    k = min(maxrank + case.get("oversample", 10), nb)
+    assert st.sketch_flops <= 2.0 * nb * nb * k * st.tiles

@@ -1,25 +1,31 @@
 #!/usr/bin/env python
 """Benchmark of the B200 TLR approximation path.
 
-Workload (one step): the whole TLR approximation of a 2-D square-exponential
-covariance matrix (beta = 0.1, sigma = 1, no nugget) on N = 102400 points of a
-320 x 320 jittered grid in Z-order, block size 1024 (10000 far-field tiles of
-1024 x 1024, 1.0486e10 entries), maxrank 256, oversample 16, tol 1e-7, with
-the Gaussian sketch, orthogonalisation, projection, small SVD and rank
-decision of every tile, and dense near-field blocks.  Inputs are synthetic
-(points from the library's own seeded generator).
+Default workload (one step): the whole TLR approximation of a 2-D
+square-exponential covariance matrix (beta = 0.1, sigma = 1, no nugget) on
+N = 102400 points of a 320 x 320 jittered grid in Z-order, block size 1024
+(10000 far-field tiles of 1024 x 1024, 1.0486e10 entries), maxrank 256,
+oversample 16, tol 1e-7: per tile the Gaussian sketch, orthogonalisation,
+projection, small SVD and rank decision, plus dense near-field blocks.
+Other workloads (--workload): the Matérn variant of that configuration,
+the 3-D Coulomb / sin(kr)/r configurations at tol 1e-5 with a TLR-by-dense
+product (65536 x 64 RHS), and the reference's small 2-D exponential case.
+Inputs are synthetic (the library's own seeded point generators).
 
 Metric: Mentries/s = (sum of m*n over all blocks) / step time / 1e6, counted
 only if the relative Frobenius error (FP64, every block regenerated on the
 GPU) is <= tol.
-  value  -- device time of starsh_b200_approximate with the factors left on
-            the device (points already on the host side of the call; the
-            call uploads them, 1.6 MB), CUDA events on the library's stream;
-  e2e    -- the drop-in STARS-H call starsh_blrm__drsdd_b200 with host
-            buffers: point upload and the copy of all factors and dense
-            blocks back to host memory inside the timed region.
+  value      -- the chosen engine (mixed: adaptive sketch), device time of
+                starsh_b200_approximate with the factors left on the device
+                (CUDA events on the library's stream; the call uploads the
+                points, 1.6 MB);
+  plain_fp64 -- the same for the fixed-width all-FP64 engine;
+  e2e        -- the drop-in STARS-H call (starsh_blrm__drsdd_b200_mp) with
+                host buffers: point upload and the copy of all factors and
+                dense blocks to host memory inside the timed region.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+                    [--workload NAME] [--engine mixed|fp64]
 
 With N > 1 (torchrun) every rank runs an independent replica on its own GPU
 (the path does not shard); value = all ranks' entries / max rank time.
@@ -33,41 +39,89 @@ import subprocess
 import sys
 import threading
 import time
-from ctypes import POINTER, byref, c_double, c_void_p
+from ctypes import POINTER, byref, c_void_p
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "stars-h_b200"))
 
-WORKLOAD = dict(workload="spatial-2d-sqexp-N102400-nb1024-maxrank256-os16-tol1e-7",
-                kernel="sqexp", ndim=2, N=102400, nb=1024, beta=0.1, nu=0.5,
-                maxrank=256, oversample=16, tol=1e-7, place=6)
-# CPU baseline sample: same kernel, block size, sketch width and tol on a
-# quarter of the points per side (625 tiles of the same 1024 x 1024 shape).
-CPU_SAMPLE_N = 25600
-CPU_STEP_N = 16384
+WORKLOADS = {
+    "c2-sqexp": dict(kind="spatial", kernel="sqexp", ndim=2, N=102400, nb=1024,
+                     beta=0.1, nu=0.5, maxrank=256, oversample=16, tol=1e-7,
+                     place=6, cpu_n=25600, cpu_step_n=16384),
+    "c2-matern": dict(kind="spatial", kernel="matern", ndim=2, N=102400,
+                      nb=1024, beta=0.05, nu=0.7, maxrank=256, oversample=16,
+                      tol=1e-7, place=6, cpu_n=None, cpu_step_n=None),
+    "c3-coulomb": dict(kind="coulomb", ndim=3, N=65536, nb=512, maxrank=200,
+                       oversample=10, tol=1e-5, place=1, diag=1.0,
+                       cpu_n=16384, cpu_step_n=8192, dmml_nrhs=64),
+    "c3-sin": dict(kind="sin", ndim=3, N=65536, nb=512, maxrank=200,
+                   oversample=10, tol=1e-5, place=1, wave_k=20.0, diag=1.0,
+                   cpu_n=16384, cpu_step_n=8192, dmml_nrhs=64),
+    "c1-exp": dict(kind="spatial", kernel="exp", ndim=2, N=3600, nb=400,
+                   beta=0.1, nu=0.5, maxrank=100, oversample=10, tol=1e-5,
+                   place=6, cpu_n=3600, cpu_step_n=3600),
+}
 METRIC = "TLR Mentries/s at rel-err<=tol"
+
+
+def workload_name(key, wl):
+    if wl["kind"] == "spatial":
+        head = f"spatial-{wl['ndim']}d-{wl['kernel']}"
+    elif wl["kind"] == "coulomb":
+        head = f"electrostatics-{wl['ndim']}d-coulomb-diag{wl['diag']:g}"
+    else:
+        head = f"electrodynamics-{wl['ndim']}d-sin-k{wl['wave_k']:g}"
+    return (f"{head}-N{wl['N']}-nb{wl['nb']}-maxrank{wl['maxrank']}"
+            f"-os{wl['oversample']}-tol{wl['tol']:g}")
 
 
 # ----------------------------------------------------------- problem setup
 
+_keep = []   # ctypes objects that must outlive the problems
+
+
 def make_problem(lib, wl, seed=0):
+    """The workload's problem built with the library's own host API."""
     import starsh_b200 as sb
     libc = ctypes.CDLL("libc.so.6")
     libc.srand(seed)
-    data = POINTER(sb.SSData)()
-    assert lib.starsh_ssdata_generate(byref(data), wl["N"], wl["ndim"],
-                                      wl["beta"], wl["nu"], 0.0, wl["place"],
-                                      1.0) == 0
     kern = c_void_p()
-    ktype = {"exp": 1, "sqexp": 2, "matern": 3}[wl["kernel"]]
-    assert lib.starsh_ssdata_get_kernel(byref(kern), data, ktype) == 0
+    if wl["kind"] == "spatial":
+        data = POINTER(sb.SSData)()
+        assert lib.starsh_ssdata_generate(byref(data), wl["N"], wl["ndim"],
+                                          wl["beta"], wl["nu"], 0.0,
+                                          wl["place"], 1.0) == 0
+        ktype = {"exp": 1, "sqexp": 2, "matern": 3}[wl["kernel"]]
+        assert lib.starsh_ssdata_get_kernel(byref(kern), data, ktype) == 0
+    elif wl["kind"] == "coulomb":
+        data = POINTER(sb.Particles)()
+        assert lib.starsh_particles_generate(byref(data), wl["N"], wl["ndim"],
+                                             wl["place"]) == 0
+        # 1/r with a regularised (unit) diagonal: a kernel handle registered
+        # with the device Coulomb family and its r = 0 value
+        handle = sb.KERNEL(lambda *a: None)
+        _keep.append(handle)
+        kern = c_void_p(ctypes.cast(handle, c_void_p).value)
+        assert lib.starsh_b200_kernel_register(kern, sb.FAMILY["coulomb"],
+                                               wl["diag"]) == 0
+    else:
+        data = POINTER(sb.EDData)()
+        gen = lib.starsh_eddata_generate
+        gen.restype = ctypes.c_int
+        gen.argtypes = [POINTER(POINTER(sb.EDData)), sb.STARSH_int,
+                        ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                        ctypes.c_int]
+        assert gen(byref(data), wl["N"], wl["ndim"], wl["wave_k"],
+                   wl["diag"], wl["place"]) == 0
+        assert lib.starsh_eddata_get_kernel(byref(kern), data, sb.SIN) == 0
     shape = (sb.STARSH_int * 2)(wl["N"], wl["N"])
     P = POINTER(sb.Problem)()
     assert lib.starsh_problem_new(byref(P), 2, shape, b"N", b"d", data, data,
                                   kern, b"bench") == 0
     C = POINTER(sb.Cluster)()
     assert lib.starsh_cluster_new_plain(byref(C), data, wl["N"], wl["nb"]) == 0
-    return dict(data=data, P=P, C=C, shape=shape)
+    _keep.append(shape)
+    return dict(data=data, P=P, C=C)
 
 
 def new_format(lib, prob):
@@ -103,8 +157,7 @@ class ClockSampler:
                     ["nvidia-smi", "-i", str(self.index),
                      f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits"],
                     capture_output=True, text=True, timeout=5).stdout.strip()
-                f = [x.strip() for x in out.split(",")]
-                self.samples.append(f)
+                self.samples.append([x.strip() for x in out.split(",")])
             except Exception:
                 pass
             self._stop.wait(0.2)
@@ -119,27 +172,43 @@ class ClockSampler:
         self._t.join()
 
     def summary(self):
-        sm = [float(s[1]) for s in self.samples if len(s) > 7 and s[1].replace('.', '', 1).isdigit()]
-        mx = [float(s[2]) for s in self.samples if len(s) > 7 and s[2].replace('.', '', 1).isdigit()]
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        good = [s for s in self.samples if len(s) > 7]
+        sm = [v for v in (num(s[1]) for s in good) if v is not None]
+        mx = [v for v in (num(s[2]) for s in good) if v is not None]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
                  "sw_power_cap"]
-        reasons = sorted({names[i] for s in self.samples if len(s) > 7
-                          for i in range(4) if s[4 + i].lower() == "active"})
+        reasons = sorted({names[i] for s in good for i in range(4)
+                          if s[4 + i].lower() == "active"})
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(self.samples)}
 
 
+class _Null:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        return False
+
+
 # --------------------------------------------------------- CPU baseline
 
-def cpu_reference_run(n, threads, wl):
-    """Runs the reference's OpenMP RSVD path (compiled from its sources into
-    oracle/_ref) on an N-point instance of the workload in a subprocess with
-    OMP_NUM_THREADS=threads, OPENBLAS_NUM_THREADS=1; returns its JSON."""
+def cpu_reference_run(key, n, threads):
+    """The reference's OpenMP RSVD path (compiled from its sources into
+    oracle/_ref) on an N-point instance of the workload, in a subprocess
+    with OMP_NUM_THREADS=threads and OPENBLAS_NUM_THREADS=1."""
+    wl = WORKLOADS[key]
     env = dict(os.environ, OMP_NUM_THREADS=str(threads),
                OPENBLAS_NUM_THREADS="1", STARSH_BACKEND="OPENMP",
                STARSH_LRENGINE="RSVD", STARSH_OVERSAMPLE=str(wl["oversample"]))
-    cmd = [sys.executable, os.path.abspath(__file__), "--_cpu-run", str(n)]
+    cmd = [sys.executable, os.path.abspath(__file__), "--_cpu-run", str(n),
+           "--workload", key]
     out = subprocess.run(cmd, env=env, capture_output=True, text=True,
                          timeout=900)
     for line in out.stdout.splitlines():
@@ -148,22 +217,37 @@ def cpu_reference_run(n, threads, wl):
     raise RuntimeError(f"CPU reference run failed: {out.stderr[-2000:]}")
 
 
-def _cpu_run(n):
+def _cpu_run(key, n):
     """Child process body of cpu_reference_run (reference library only)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle
     from harness import RefProblem
-    wl = WORKLOAD
+    wl = WORKLOADS[key]
     ref = oracle.Ref()
-    pr = RefProblem(ref, "spatial", n, wl["nb"], ndim=wl["ndim"],
-                    place=wl["place"], beta=wl["beta"],
-                    kernel_name=wl["kernel"])
+    if wl["kind"] == "spatial":
+        pr = RefProblem(ref, "spatial", n, wl["nb"], ndim=wl["ndim"],
+                        place=wl["place"], beta=wl["beta"], nu=wl["nu"],
+                        kernel_name=wl["kernel"])
+    elif wl["kind"] == "coulomb":
+        # the reference kernel wrapped to put 1 on the r = 0 entries
+        orc = oracle.Oracle()
+        ptr = ctypes.c_void_p.in_dll(orc.lib, "oracle_coulomb_ref_kernel")
+        ptr.value = ref.symbol(
+            f"starsh_esdata_block_coulomb_potential_kernel_{wl['ndim']}d")
+        wrap = ctypes.c_void_p(ctypes.cast(orc.lib.oracle_coulomb_unit_diag,
+                                           ctypes.c_void_p).value)
+        pr = RefProblem(ref, "custom", n, wl["nb"],
+                        data=ref.particles_data(n, wl["ndim"], wl["place"]),
+                        kernel=wrap)
+    else:
+        pr = RefProblem(ref, "sin", n, wl["nb"], ndim=wl["ndim"],
+                        place=wl["place"], wave_k=wl["wave_k"], diag=wl["diag"])
     t0 = time.perf_counter()
     M = ref.approximate(pr.F, wl["maxrank"], wl["tol"],
                         oversample=wl["oversample"])
     dt = time.perf_counter() - t0
-    err = ref.dfe(M) if n <= CPU_SAMPLE_N else None
+    err = ref.dfe(M) if n <= wl.get("cpu_n") else None
     print(json.dumps({"seconds": dt, "entries": n * n, "rel_err": err}))
 
 
@@ -190,6 +274,37 @@ def fp64_peak_tflops(torch):
 
 # ------------------------------------------------------------------ main
 
+def reference_arm(args, key, wl, threads):
+    """--impl reference: the reference's OpenMP RSVD on the host cores, one
+    bounded sample of the workload (same tiles, sketch width, tol) per
+    step."""
+    n = wl.get("cpu_step_n")
+    if not n:
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "reference kernel needs GSL, which is not installed"}))
+        return
+    times = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_reference_run(key, n, threads)
+        if i >= args.warmup:
+            times.append(r["seconds"])
+    t = statistics.mean(times)
+    v = n ** 2 / t / 1e6
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v,
+        "unit": "Mentries/s", "n_gpus": 0, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": dict(workload=workload_name(key, wl), sample_N=n,
+                       engine="starsh_blrm__drsdd_omp"),
+        "cpu_baseline": {"value": v, "unit": "Mentries/s", "cores": threads,
+                         "kind": "reference",
+                         "sample": f"N={n} ({(n // wl['nb']) ** 2} tiles of {wl['nb']}x{wl['nb']})"},
+        "e2e": {"value": v, "unit": "Mentries/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0}}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -197,50 +312,29 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--engine", default="mixed", choices=["fp64", "mixed"])
-    ap.add_argument("--n", type=int, default=WORKLOAD["N"],
+    ap.add_argument("--workload", default="c2-sqexp", choices=sorted(WORKLOADS))
+    ap.add_argument("--n", type=int, default=0,
                     help="points (a smaller N profiles the same kernels)")
     ap.add_argument("--no-cpu", action="store_true",
                     help="skip the CPU baseline leg")
     ap.add_argument("--_cpu-run", type=int, default=0, dest="cpu_run")
     args = ap.parse_args()
+    key = args.workload
     if args.cpu_run:
-        _cpu_run(args.cpu_run)
+        _cpu_run(key, args.cpu_run)
         return
 
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local = int(os.environ.get("LOCAL_RANK", 0))
-    wl = dict(WORKLOAD)
-    if args.n != wl["N"]:
+    wl = dict(WORKLOADS[key])
+    if args.n:
         wl["N"] = args.n
-        wl["workload"] = wl["workload"].replace("N102400", f"N{args.n}")
     threads = len(os.sched_getaffinity(0))
 
     if args.impl == "reference":
-        if rank != 0:
-            return
-        # Reference arm: its OpenMP RSVD on the host cores, one bounded
-        # sample of the workload (same tiles, sketch width, tol) per step.
-        times = []
-        for i in range(args.warmup + args.steps):
-            r = cpu_reference_run(CPU_STEP_N, threads, wl)
-            if i >= args.warmup:
-                times.append(r["seconds"])
-        t = statistics.mean(times)
-        v = CPU_STEP_N ** 2 / t / 1e6
-        print(json.dumps({
-            "impl": "reference", "metric": METRIC, "value": v,
-            "unit": "Mentries/s", "n_gpus": 0, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": t * 1e3,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic",
-            "config": dict(workload=wl["workload"], sample_N=CPU_STEP_N,
-                           engine="starsh_blrm__drsdd_omp"),
-            "cpu_baseline": {"value": v, "unit": "Mentries/s", "cores": threads,
-                             "kind": "reference",
-                             "sample": f"N={CPU_STEP_N} ({(CPU_STEP_N // wl['nb']) ** 2} tiles of 1024x1024)"},
-            "e2e": {"value": v, "unit": "Mentries/s", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0}}))
+        if rank == 0:
+            reference_arm(args, key, wl, threads)
         return
 
     import torch
@@ -287,16 +381,15 @@ def main():
         lib.starsh_blrm_free(M)
         lib.starsh_blrf_free(F)
 
-    def measure(engine, clocks=None):
-        """W warm-up and K timed device-resident approximations; returns the
-        mean device time, the stats of the last step, its FP64 error."""
+    def measure(engine, clocks=None, keep=False):
+        """W warm-up and K timed device-resident approximations; mean device
+        time, per-step stats, FP64 error of the last result."""
         for _ in range(args.warmup):
             M, F, *_ = step(engine, 0)
             free(M, F)
         barrier()
         times, sts = [], []
-        ctx = clocks if clocks is not None else _Null()
-        with ctx:
+        with (clocks if clocks is not None else _Null()):
             for i in range(args.steps):
                 M, F, dt, host, st = step(engine, 0)
                 times.append(dt)
@@ -305,18 +398,59 @@ def main():
                     free(M, F)
         barrier()
         err = lib.starsh_blrm__dfe_b200(M)
+        if keep:
+            return statistics.mean(times), sts, err, (M, F)
         free(M, F)
-        return statistics.mean(times), sts, err
+        return statistics.mean(times), sts, err, None
 
-    # the chosen engine (timed region sampled for clocks), then the plain
-    # FP64 form on the same GPU
     clocks = ClockSampler(local)
-    t_dev, sts, err = measure(chosen, clocks)
+    t_dev, sts, err, kept = measure(chosen, clocks, keep=bool(wl.get("dmml_nrhs")))
     last = sts[-1]
     if chosen != sb.ENGINE_FP64:
-        t_plain, sts_plain, err_plain = measure(sb.ENGINE_FP64)
+        t_plain, _, err_plain, _ = measure(sb.ENGINE_FP64)
     else:
-        t_plain, sts_plain, err_plain = t_dev, sts, err
+        t_plain, err_plain = t_dev, err
+
+    # TLR-by-dense product on the device-resident factors
+    dmml = None
+    if kept is not None:
+        M, F = kept
+        nrhs = wl["dmml_nrhs"]
+        A = torch.randn(nrhs, wl["N"], dtype=torch.float64, device="cuda")
+        B = torch.zeros(nrhs, wl["N"], dtype=torch.float64, device="cuda")
+        for _ in range(2):
+            assert lib.starsh_b200_blrm_dmml_device(M, nrhs, 1.0, A.data_ptr(),
+                                                    wl["N"], 0.0, B.data_ptr(),
+                                                    wl["N"], None) == 0
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = 5
+        s.record(stream)
+        for _ in range(reps):
+            lib.starsh_b200_blrm_dmml_device(M, nrhs, 1.0, A.data_ptr(), wl["N"],
+                                             0.0, B.data_ptr(), wl["N"], None)
+        e.record(stream)
+        e.synchronize()
+        t = s.elapsed_time(e) / 1e3 / reps
+        Mc = M.contents
+        Fc = Mc.format.contents
+        R = Fc.row_cluster.contents
+        flops = 0.0
+        byts = 2.0 * wl["N"] * nrhs * 8
+        for b in range(Fc.nblocks_far):
+            i, j = Fc.block_far[2 * b], Fc.block_far[2 * b + 1]
+            r = Mc.far_rank[b]
+            flops += 2.0 * (R.size[i] + R.size[j]) * r * nrhs
+            byts += (R.size[i] + R.size[j]) * r * 8.0
+        for b in range(Fc.nblocks_near):
+            i, j = Fc.block_near[2 * b], Fc.block_near[2 * b + 1]
+            flops += 2.0 * R.size[i] * R.size[j] * nrhs
+            byts += R.size[i] * R.size[j] * 8.0
+        dmml = {"nrhs": nrhs, "ms": t * 1e3, "gflops": flops / t / 1e9,
+                "hbm_gbs": byts / t / 1e9,
+                "bound": "fp64 tensor" if flops / byts > 5 else "hbm"}
+        free(M, F)
+
     # e2e: the drop-in call with host buffers
     entry = (lib.starsh_blrm__drsdd_b200_mp if chosen == sb.ENGINE_MIXED
              else lib.starsh_blrm__drsdd_b200)
@@ -342,7 +476,7 @@ def main():
         if world > 1:
             torch.distributed.destroy_process_group()
         return
-    # roofline of the dominant kernel: the sketch GEMM (FP64 DMMA)
+    # roofline of the sketch GEMM (FP64 DMMA)
     per_launch_ms = last.sketch_ms / max(1, last.sketch_launches)
     flops_per_launch = last.sketch_flops / max(1, last.sketch_launches)
     achieved = flops_per_launch / (per_launch_ms / 1e3) / 1e12
@@ -354,16 +488,17 @@ def main():
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": t_dev * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded jittered grid)",
-        "config": {"workload": wl["workload"],
-                   "engine": "mixed (adaptive sketch, FP64 at this tol)" if chosen == sb.ENGINE_MIXED else "fp64",
+        "data": "synthetic (seeded point generators)",
+        "config": {"workload": workload_name(key, wl),
+                   "engine": ("mixed (adaptive sketch)" if chosen == sb.ENGINE_MIXED
+                              else "fp64 (fixed sketch width)"),
                    "parallelism": f"replicas{world}" if world > 1 else "single",
                    "tiles": int(last.tiles), "false_far": int(last.false_far),
                    "entries": int(entries),
                    "l2": "flushed (256 MB write) before every step",
                    "mean_rank": last.rank_sum / max(1, last.tiles - last.false_far),
                    "max_rank": last.max_rank,
-                   "sketch_columns_per_tile": last.sketch_flops / max(1.0, 2.0 * entries)},
+                   "sketch_columns_per_tile": last.sketch_flops / max(1.0, 2.0 * last.tiles * wl["nb"] ** 2)},
         "rel_err": err, "tol": wl["tol"], "accepted": accepted,
         "plain_fp64": {"value": plain_value, "ms_per_step": t_plain * 1e3,
                        "rel_err": err_plain,
@@ -382,27 +517,26 @@ def main():
                      "traffic": None},
         "clocks": clocks.summary(),
     }
+    if dmml:
+        line["dmml"] = dmml
     if world == 1 and not args.no_cpu:
-        try:
-            r = cpu_reference_run(CPU_SAMPLE_N, threads, wl)
-            line["cpu_baseline"] = {
-                "value": r["entries"] / r["seconds"] / 1e6, "unit": "Mentries/s",
-                "cores": threads, "kind": "reference",
-                "sample": f"N={CPU_SAMPLE_N}: {(CPU_SAMPLE_N // wl['nb']) ** 2} tiles of 1024x1024, same kernel/maxrank/oversample/tol, starsh_blrm__drsdd_omp",
-                "rel_err": r["rel_err"], "seconds": r["seconds"]}
-        except Exception as exc:   # reported, not fatal
-            line["cpu_baseline"] = {"value": None, "error": str(exc)[:300]}
+        n = wl.get("cpu_n")
+        if not n:
+            line["cpu_baseline"] = {"value": None, "kind": "reference",
+                                    "unavailable": "reference kernel needs GSL, which is not installed"}
+        else:
+            try:
+                r = cpu_reference_run(key, n, threads)
+                line["cpu_baseline"] = {
+                    "value": r["entries"] / r["seconds"] / 1e6, "unit": "Mentries/s",
+                    "cores": threads, "kind": "reference",
+                    "sample": f"N={n}: {(n // wl['nb']) ** 2} tiles of {wl['nb']}x{wl['nb']}, same kernel/maxrank/oversample/tol, starsh_blrm__drsdd_omp",
+                    "rel_err": r["rel_err"], "seconds": r["seconds"]}
+            except Exception as exc:   # reported, not fatal
+                line["cpu_baseline"] = {"value": None, "error": str(exc)[:300]}
     print(json.dumps(line))
     if world > 1:
         torch.distributed.destroy_process_group()
-
-
-class _Null:
-    def __enter__(self):
-        return self
-
-    def __exit__(self, *a):
-        return False
 
 
 if __name__ == "__main__":

@@ -127,7 +127,7 @@ int starsh_b200_kernel_family(STARSH_kernel *kernel, int *ndim_hint);
  * under an allocator that owns all device memory, or on threads that must
  * not wait for the allocator's implicit synchronisation).  Same algorithm,
  * Gaussian sketch and rank rule as starsh_blrm__drsdd_b200 applied to that
- * tile; its scratch is a fixed __device__ array of about 1.9 MB that every
+ * tile; its scratch is a fixed __device__ array of about 2.1 MB that every
  * GPU loading the library keeps until the process exits.
  *   dD      nrows x ncols tile, column-major, leading dimension ldd;
  *   dU      receives nrows x rank, leading dimension nrows;

@@ -25,6 +25,8 @@ struct Context {
     DeviceBuffer descs;        // GemmDesc array of a batch
     DeviceBuffer omega;        // Gaussian sketch matrix
     DeviceBuffer flag;         // round flag of the adaptive sketch
+    void *stage[2] = {nullptr, nullptr};     // pinned D2H staging buffers
+    cudaEvent_t stage_ev[2] = {nullptr, nullptr};
     size_t omega_count = 0;
     unsigned long long omega_seed = 0;
     std::mutex lock;           // one approximation / dmml at a time

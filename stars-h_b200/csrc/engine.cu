@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <atomic>
 #include <mutex>
+#include <thread>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -434,7 +435,7 @@ static int compress_far(Context &ctx, const DevKernel &K, STARSH_blrf *F,
         cudaEventRecord(ev[3], s);
         if ((info = gemm(STEP_GRAM_B, false, true, nt, k_max, k_max, none))) break;
         launch_pivchol(2, dt, dt, nt, ws, ep.tol, s);
-        launch_jacobi(dt, nt, ws, s);
+        launch_jacobi(dt, nt, ws, ep.tol, s);
         count_launch(2);
         if ((info = gemm(STEP_ROTATE, true, false, nt, k_max, n_max, none))) break;
         launch_rank_cut(dt, nt, ws, ep.tol, ep.maxrank, s);
@@ -508,6 +509,70 @@ static int make_view(Array **A, int m, int n, double *data)
     return array_from_buffer(A, 2, shape, 'd', 'F', data);
 }
 
+// Copies device memory into pageable (malloc'd) host memory through two
+// pinned staging buffers: the DMA of one chunk overlaps the host-side copy
+// of the previous one, and that copy -- which also takes the first-touch
+// page faults of the destination -- is split over several threads.  A
+// plain cudaMemcpy into fresh malloc'd memory is limited by those faults.
+constexpr size_t kStageBytes = 64u << 20;
+
+static void parallel_memcpy(char *dst, const char *src, size_t n)
+{
+    const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    const size_t per = (n + hw - 1) / hw;
+    std::vector<std::thread> th;
+    for (unsigned t = 1; t < hw && t * per < n; ++t)
+        th.emplace_back([=] { memcpy(dst + t * per, src + t * per,
+                                     std::min(per, n - t * per)); });
+    memcpy(dst, src, std::min(per, n));
+    for (auto &x : th) x.join();
+}
+
+struct D2HCopy {
+    char *dst;
+    const char *src;
+    size_t n;
+};
+
+static int staged_d2h(Context &ctx, const std::vector<D2HCopy> &jobs,
+                      cudaStream_t s)
+{
+    if (!ctx.stage[0]) {
+        for (int i = 0; i < 2; ++i)
+            B200_CUDA(cudaMallocHost(&ctx.stage[i], kStageBytes),
+                      "cudaMallocHost(staging)");
+        for (int i = 0; i < 2; ++i)
+            B200_CUDA(cudaEventCreateWithFlags(&ctx.stage_ev[i],
+                                               cudaEventDisableTiming),
+                      "cudaEventCreate(staging)");
+    }
+    // flatten into chunks of at most kStageBytes
+    struct Chunk { char *dst; const char *src; size_t n; };
+    std::vector<Chunk> chunks;
+    for (const D2HCopy &j : jobs)
+        for (size_t o = 0; o < j.n; o += kStageBytes)
+            chunks.push_back({j.dst + o, j.src + o, std::min(kStageBytes, j.n - o)});
+    for (size_t c = 0; c < chunks.size(); ++c) {
+        const int b = (int)(c & 1);
+        B200_CUDA(cudaMemcpyAsync(ctx.stage[b], chunks[c].src, chunks[c].n,
+                                  cudaMemcpyDeviceToHost, s), "staged D2H");
+        B200_CUDA(cudaEventRecord(ctx.stage_ev[b], s), "staged D2H event");
+        if (c >= 1) {
+            const int pb = (int)((c - 1) & 1);
+            B200_CUDA(cudaEventSynchronize(ctx.stage_ev[pb]), "staged D2H wait");
+            parallel_memcpy(chunks[c - 1].dst, (const char *)ctx.stage[pb],
+                            chunks[c - 1].n);
+        }
+    }
+    if (!chunks.empty()) {
+        const size_t c = chunks.size() - 1;
+        const int b = (int)(c & 1);
+        B200_CUDA(cudaEventSynchronize(ctx.stage_ev[b]), "staged D2H wait");
+        parallel_memcpy(chunks[c].dst, (const char *)ctx.stage[b], chunks[c].n);
+    }
+    return STARSH_SUCCESS;
+}
+
 static int fill_host_mirror(STARSH_blrm *M, Record &rec, cudaStream_t s)
 {
     if (rec.host_filled) return STARSH_SUCCESS;
@@ -522,12 +587,11 @@ static int fill_host_mirror(STARSH_blrm *M, Record &rec, cudaStream_t s)
         return STARSH_MALLOC_ERROR;
     }
     // One copy per factor chunk; views follow the same order.
+    std::vector<D2HCopy> jobs;
     size_t ou = 0, ov = 0;
     for (const Record::Part &pt : rec.parts) {
-        cudaMemcpyAsync(hU + ou, pt.U, pt.nu * sizeof(double),
-                        cudaMemcpyDeviceToHost, s);
-        cudaMemcpyAsync(hV + ov, pt.V, pt.nv * sizeof(double),
-                        cudaMemcpyDeviceToHost, s);
+        jobs.push_back({(char *)(hU + ou), (const char *)pt.U, pt.nu * sizeof(double)});
+        jobs.push_back({(char *)(hV + ov), (const char *)pt.V, pt.nv * sizeof(double)});
         ou += pt.nu;
         ov += pt.nv;
     }
@@ -548,8 +612,8 @@ static int fill_host_mirror(STARSH_blrm *M, Record &rec, cudaStream_t s)
         }
         // near blocks live in one contiguous device allocation
         if (rec.d_total)
-            cudaMemcpyAsync(hD, rec.dD[0], rec.d_total * sizeof(double),
-                            cudaMemcpyDeviceToHost, s);
+            jobs.push_back({(char *)hD, (const char *)rec.dD[0],
+                            rec.d_total * sizeof(double)});
         size_t od = 0;
         for (STARSH_int b = 0; b < F->nblocks_near; ++b) {
             M->near_D[b]->data = hD + od;
@@ -557,11 +621,13 @@ static int fill_host_mirror(STARSH_blrm *M, Record &rec, cudaStream_t s)
         }
     }
     cudaError_t e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) {
+    int info = e == cudaSuccess ? staged_d2h(*context(), jobs, s)
+                                : cuda_fail(e, "host mirror copy");
+    if (info) {
         free(hU);
         free(hV);
         free(hD);
-        return cuda_fail(e, "host mirror copy");
+        return info;
     }
     st.d2h_bytes += (long long)(rec.u_total + rec.v_total + rec.d_total) * 8;
     M->alloc_U = hU;

@@ -28,6 +28,7 @@ struct TileWork {
     int need_pass_b;        // residual pass required by tol
     double tr_g;            // trace of the sketch Gram Y^T Y
     double tr_h;            // ||B||_F^2 = trace of B B^T
+    double tail_h;          // energy left out of the Gram factor of B B^T
     // adaptive sketch (mixed engine)
     double dnorm2;          // ||D||_F^2 of the block, exact (FP64)
     int cols_done;          // sketch columns consumed so far
@@ -124,7 +125,7 @@ void launch_gather_cols(int phase, const TileWork *d_tiles, int ntiles,
                         Workspace ws, cudaStream_t stream);
 void launch_chol_inv(int phase, TileWork *d_tiles, int ntiles, Workspace ws,
                      cudaStream_t stream);
-void launch_jacobi(TileWork *d_tiles, int ntiles, Workspace ws,
+void launch_jacobi(TileWork *d_tiles, int ntiles, Workspace ws, double tol,
                    cudaStream_t stream);
 void launch_rank_cut(TileWork *d_tiles, int ntiles, Workspace ws,
                      double tol, int maxrank, cudaStream_t stream);

@@ -12,7 +12,7 @@
 //
 // Limits: nrows, ncols <= 256 and min(maxrank + oversample, nrows, ncols)
 // <= 96; larger sizes are rejected with STARSH_WRONG_PARAMETER.  The scratch
-// array (about 1.9 MB) exists on every GPU that loads the library and stays
+// array (about 2.1 MB) exists on every GPU that loads the library and stays
 // allocated until the process exits.  All calls share it and it keeps the
 // previous call's contents: the pipeline overwrites every field it reads,
 // and two calls that overlap on the GPU (different streams, or different
@@ -36,7 +36,8 @@ constexpr size_t round32(size_t n) { return (n + 31) & ~(size_t)31; }
 constexpr size_t slot_doubles(size_t m, size_t n, size_t k)
 {
     return round32(m * n) + 3 * round32(m * k) + 3 * round32(k * k) +
-           2 * round32(k * n) + 2 * round32(k) + 2 * round32((k + 1) / 2);
+           2 * round32(k * n) + 2 * round32(k) + 2 * round32((k + 1) / 2) +
+           round32(((m + 63) / 64) * ((n + 63) / 64)) + round32(m * k);
 }
 constexpr size_t kSlotDoubles =
     slot_doubles(kNoAllocMaxDim, kNoAllocMaxDim, kNoAllocMaxK);
@@ -171,7 +172,7 @@ extern "C" int starsh_b200_dense_rsvd_noalloc(const double *dD, int nrows,
     if ((info = gemm(STEP_PROJECT, true, false, k, n, none))) return info;
     if ((info = gemm(STEP_GRAM_B, false, true, k, k, none))) return info;
     launch_pivchol(2, dt, dt, 1, ws, tol, s);
-    launch_jacobi(dt, 1, ws, s);
+    launch_jacobi(dt, 1, ws, tol, s);
     if ((info = gemm(STEP_ROTATE, true, false, k, n, none))) return info;
     launch_rank_cut(dt, 1, ws, tol, maxrank, s);
     // One tile: its factors start at offset 0 of the caller's buffers, so

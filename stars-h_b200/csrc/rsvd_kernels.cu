@@ -19,7 +19,10 @@
 //     decides the rank is exact to FP64 rounding even where the Gram's
 //     eigenvalues are not.
 #include <cfloat>
+#include <cooperative_groups.h>
 #include "engine.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace b200 {
 
@@ -605,7 +608,15 @@ k_pivchol(TileWork *__restrict__ tiles, Workspace ws, int phase, double tol)
             if (cnt == 0) tw.need_pass_b = 0;
         }
     }
-    if (phase == PH_H) return;
+    if (phase == PH_H) {
+        // energy of B outside the span of the factor's columns
+        double rest = 0.0;
+        for (int i = threadIdx.x; i < nn; i += blockDim.x)
+            if (!used[i]) rest += fmax(0.0, dg[i]);
+        rest = block_sum(rest, redd);
+        if (threadIdx.x == 0) tw.tail_h = cnt > 0 ? rest : trace;
+        return;
+    }
     // T = R11^{-1}, R11(a, b) = L(piv[b], a) for a <= b (upper triangular).
     double *T = ws.T(s);
     for (int c = threadIdx.x; c < cnt; c += blockDim.x) {
@@ -804,9 +815,103 @@ void launch_chol_inv(int phase, TileWork *d_tiles, int ntiles, Workspace ws,
 // dynamic shared memory is rotated there; a larger one in place in global
 // memory (L2-resident).
 constexpr size_t kJacobiSmem = 200 * 1024;
+constexpr int kJacobiThreads = 1024;
+constexpr int kJacobiRegRows = 9;   // rows per lane kept in registers (<= 288)
 
-__global__ void __launch_bounds__(kSmallThreads)
-k_jacobi(TileWork *__restrict__ tiles, Workspace ws)
+// One rotation of the column pair (a, b) by one warp.  With REG the pair is
+// loaded into registers once (independent loads in flight, one round trip),
+// otherwise streamed.  Returns true if the pair was rotated.
+template <bool REG>
+__device__ __forceinline__ bool jacobi_pair(double *ca, double *cb, int rows,
+                                            int lane, double eps)
+{
+    double xa[REG ? kJacobiRegRows : 1], xb[REG ? kJacobiRegRows : 1];
+    double al = 0.0, be = 0.0, ga = 0.0;
+    if (REG) {
+        #pragma unroll
+        for (int q = 0; q < kJacobiRegRows; ++q) {
+            const int i = lane + 32 * q;
+            xa[q] = i < rows ? ca[i] : 0.0;
+            xb[q] = i < rows ? cb[i] : 0.0;
+        }
+        #pragma unroll
+        for (int q = 0; q < kJacobiRegRows; ++q) {
+            al += xa[q] * xa[q];
+            be += xb[q] * xb[q];
+            ga += xa[q] * xb[q];
+        }
+    } else {
+        for (int i = lane; i < rows; i += 32) {
+            const double x = ca[i], y = cb[i];
+            al += x * x;
+            be += y * y;
+            ga += x * y;
+        }
+    }
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        al += __shfl_xor_sync(0xffffffffu, al, o);
+        be += __shfl_xor_sync(0xffffffffu, be, o);
+        ga += __shfl_xor_sync(0xffffffffu, ga, o);
+    }
+    if (!(fabs(ga) > eps * sqrt(al * be)) || al == 0.0 || be == 0.0)
+        return false;
+    const double zeta = (be - al) / (2.0 * ga);
+    const double t = (zeta >= 0.0 ? 1.0 : -1.0) /
+                     (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+    const double c = 1.0 / sqrt(1.0 + t * t);
+    const double sn = c * t;
+    if (REG) {
+        #pragma unroll
+        for (int q = 0; q < kJacobiRegRows; ++q) {
+            const int i = lane + 32 * q;
+            if (i < rows) {
+                ca[i] = c * xa[q] - sn * xb[q];
+                cb[i] = sn * xa[q] + c * xb[q];
+            }
+        }
+    } else {
+        for (int i = lane; i < rows; i += 32) {
+            const double x = ca[i], y = cb[i];
+            ca[i] = c * x - sn * y;
+            cb[i] = sn * x + c * y;
+        }
+    }
+    return true;
+}
+
+// One-sided Jacobi (Hestenes) on the columns of A = L(slot) (k1 x k2):
+// column pairs are rotated until mutually orthogonal; then the columns of
+// A V are the eigenvectors of L L^T scaled by the singular values.  L comes
+// from a pivoted Cholesky of B B^T (the transpose of a column-pivoted QR
+// factor of B^T), the preconditioning under which one-sided Jacobi needs
+// few sweeps (Z. Drmac, K. Veselic, SIAM J. Matrix Anal. Appl. 29 (2008)).
+// Pairs follow the round-robin tournament ordering, k2/2 disjoint pairs per
+// step, one warp per pair, 32 warps.  A tile whose columns fit in the
+// dynamic shared memory is rotated there, a larger one in place in global
+// memory (L2-resident), where each pair makes a single load round trip.
+// W (normalised columns) goes to T(slot), squared norms to Sig(slot).
+constexpr int kJacobiCluster = 4;
+constexpr size_t kJacobiSmemSmall = 48 * 1024;
+constexpr int kJacobiThreadsSmall = 256;
+
+// Where the Jacobi of a k1 x k2 factor runs: 3 a small CTA (256 threads,
+// 48 KB) with the columns in shared memory, 0 a full CTA (1024 threads,
+// 200 KB) likewise, 1 a cluster of kJacobiCluster CTAs sharing them through
+// distributed shared memory, 2 one CTA on global memory.
+__host__ __device__ inline int jacobi_route(int rows, int cols)
+{
+    const size_t lds = (size_t)(rows | 1);
+    if (lds * cols * sizeof(double) <= kJacobiSmemSmall) return 3;
+    if (lds * cols * sizeof(double) <= kJacobiSmem) return 0;
+    const size_t cpb = (cols + kJacobiCluster - 1) / kJacobiCluster;
+    if (lds * cpb * sizeof(double) <= kJacobiSmem) return 1;
+    return 2;
+}
+
+template <int THREADS, bool SMALL>
+__global__ void __launch_bounds__(THREADS)
+k_jacobi(TileWork *__restrict__ tiles, Workspace ws, double eps)
 {
     extern __shared__ double sm[];
     __shared__ int rotated;
@@ -814,9 +919,11 @@ k_jacobi(TileWork *__restrict__ tiles, Workspace ws)
     const int s = tw.slot;
     const int rows = tw.k1, cols = tw.k2;
     if (cols <= 0) return;
+    const int route = jacobi_route(rows, cols);
+    if (SMALL ? route != 3 : (route != 0 && route != 2)) return;
     const int ldg = ws.ldK();
     const int lds = rows | 1;   // odd stride: fewer bank conflicts
-    const bool in_smem = (size_t)lds * cols * sizeof(double) <= kJacobiSmem;
+    const bool in_smem = route != 2;
     double *A = in_smem ? sm : ws.L(s);
     const int lda = in_smem ? lds : ldg;
     if (in_smem) {
@@ -830,47 +937,26 @@ k_jacobi(TileWork *__restrict__ tiles, Workspace ws)
     const int nwarps = blockDim.x >> 5;
     const int nc = cols + (cols & 1);      // players, with a bye if odd
     const int npairs = nc / 2;
+    const bool reg = rows <= 32 * kJacobiRegRows;
     int sweep = 0;
     for (; sweep < 40; ++sweep) {
         if (threadIdx.x == 0) rotated = 0;
         __syncthreads();
+        bool any = false;
         for (int step = 0; step < nc - 1; ++step) {
             for (int p = warp; p < npairs; p += nwarps) {
                 const int a = p == 0 ? 0 : 1 + (p - 1 + step) % (nc - 1);
                 const int b = 1 + (nc - 2 - p + step) % (nc - 1);
                 if (a >= cols || b >= cols) continue;
                 double *ca = A + (size_t)a * lda, *cb = A + (size_t)b * lda;
-                double al = 0.0, be = 0.0, ga = 0.0;
-                for (int i = lane; i < rows; i += 32) {
-                    const double x = ca[i], y = cb[i];
-                    al += x * x;
-                    be += y * y;
-                    ga += x * y;
-                }
-                #pragma unroll
-                for (int o = 16; o > 0; o >>= 1) {
-                    al += __shfl_xor_sync(0xffffffffu, al, o);
-                    be += __shfl_xor_sync(0xffffffffu, be, o);
-                    ga += __shfl_xor_sync(0xffffffffu, ga, o);
-                }
-                if (!(fabs(ga) > 1e-15 * sqrt(al * be)) || al == 0.0 || be == 0.0)
-                    continue;
-                const double zeta = (be - al) / (2.0 * ga);
-                const double t = (zeta >= 0.0 ? 1.0 : -1.0) /
-                                 (fabs(zeta) + sqrt(1.0 + zeta * zeta));
-                const double c = 1.0 / sqrt(1.0 + t * t);
-                const double sn = c * t;
-                for (int i = lane; i < rows; i += 32) {
-                    const double x = ca[i], y = cb[i];
-                    ca[i] = c * x - sn * y;
-                    cb[i] = sn * x + c * y;
-                }
-                if (lane == 0) rotated = 1;
+                any |= reg ? jacobi_pair<true>(ca, cb, rows, lane, eps)
+                           : jacobi_pair<false>(ca, cb, rows, lane, eps);
             }
             __syncthreads();
         }
-        if (!rotated) break;
+        if (any && lane == 0) rotated = 1;
         __syncthreads();
+        if (!rotated) break;
     }
     // Normalise into W = T(slot); squared norms into Sig.
     double *W = ws.T(s);
@@ -888,16 +974,113 @@ k_jacobi(TileWork *__restrict__ tiles, Workspace ws)
     if (threadIdx.x == 0 && sweep >= 40) tw.status |= TILE_JACOBI_SLOW;
 }
 
-void launch_jacobi(TileWork *d_tiles, int ntiles, Workspace ws,
+
+// The same one-sided Jacobi for factors too large for one CTA's shared
+// memory: a cluster of kJacobiCluster CTAs holds the columns, CTA r owning
+// columns [r cpb, (r+1) cpb).  A pair is rotated by one warp of any CTA
+// through distributed shared memory (generic pointers from
+// cluster.map_shared_rank), so every column load and store stays on chip;
+// the cluster synchronises after each round-robin step.
+__global__ void __cluster_dims__(kJacobiCluster, 1, 1)
+__launch_bounds__(kJacobiThreads)
+k_jacobi_cluster(TileWork *__restrict__ tiles, Workspace ws, double eps)
+{
+    extern __shared__ double sm[];
+    __shared__ int rotated;
+    cg::cluster_group cluster = cg::this_cluster();
+    const int crank = (int)cluster.block_rank();
+    TileWork &tw = tiles[blockIdx.x / kJacobiCluster];
+    const int s = tw.slot;
+    const int rows = tw.k1, cols = tw.k2;
+    if (cols <= 0 || jacobi_route(rows, cols) != 1) return;   // uniform
+    const int ldg = ws.ldK();
+    const int lds = rows | 1;
+    const int cpb = (cols + kJacobiCluster - 1) / kJacobiCluster;
+    const int c0 = crank * cpb, c1 = min(cols, c0 + cpb);
+    const double *Lg = ws.L(s);
+    for (int c = c0; c < c1; ++c)
+        for (int i = threadIdx.x; i < rows; i += blockDim.x)
+            sm[(size_t)(c - c0) * lds + i] = Lg[(size_t)c * ldg + i];
+    if (threadIdx.x == 0) rotated = 0;
+    cluster.sync();
+    auto col = [&](int c) -> double * {
+        double *base = cluster.map_shared_rank(sm, c / cpb);
+        return base + (size_t)(c % cpb) * lds;
+    };
+    const int lane = threadIdx.x & 31;
+    const int gwarp = crank * (kJacobiThreads / 32) + (threadIdx.x >> 5);
+    const int nwarps = kJacobiCluster * (kJacobiThreads / 32);
+    const int nc = cols + (cols & 1);
+    const int npairs = nc / 2;
+    const bool reg = rows <= 32 * kJacobiRegRows;
+    int sweep = 0;
+    for (; sweep < 40; ++sweep) {
+        bool any = false;
+        for (int step = 0; step < nc - 1; ++step) {
+            for (int p = gwarp; p < npairs; p += nwarps) {
+                const int a = p == 0 ? 0 : 1 + (p - 1 + step) % (nc - 1);
+                const int b = 1 + (nc - 2 - p + step) % (nc - 1);
+                if (a >= cols || b >= cols) continue;
+                any |= reg ? jacobi_pair<true>(col(a), col(b), rows, lane, eps)
+                           : jacobi_pair<false>(col(a), col(b), rows, lane, eps);
+            }
+            cluster.sync();
+        }
+        if (any && lane == 0) atomicOr(cluster.map_shared_rank(&rotated, 0), 1);
+        cluster.sync();
+        const int r = *cluster.map_shared_rank(&rotated, 0);
+        cluster.sync();
+        if (crank == 0 && threadIdx.x == 0) rotated = 0;
+        cluster.sync();
+        if (!r) break;
+    }
+    double *W = ws.T(s);
+    double *sig = ws.Sig(s);
+    const int warp = threadIdx.x >> 5;
+    for (int c = c0 + warp; c < c1; c += kJacobiThreads / 32) {
+        const double *ca = sm + (size_t)(c - c0) * lds;
+        double nrm = 0.0;
+        for (int i = lane; i < rows; i += 32) nrm += ca[i] * ca[i];
+        #pragma unroll
+        for (int o = 16; o > 0; o >>= 1) nrm += __shfl_xor_sync(0xffffffffu, nrm, o);
+        const double inv = nrm > 0.0 ? 1.0 / sqrt(nrm) : 0.0;
+        for (int i = lane; i < rows; i += 32) W[(size_t)c * ldg + i] = ca[i] * inv;
+        if (lane == 0) sig[c] = nrm;
+    }
+    if (crank == 0 && threadIdx.x == 0 && sweep >= 40)
+        tw.status |= TILE_JACOBI_SLOW;
+    cluster.sync();   // no CTA leaves while others may read its columns
+}
+
+void launch_jacobi(TileWork *d_tiles, int ntiles, Workspace ws, double tol,
                    cudaStream_t stream)
 {
     static bool attr_set = false;
     if (!attr_set) {
-        cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(k_jacobi<kJacobiThreads, false>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kJacobiSmem);
+        cudaFuncSetAttribute(k_jacobi<kJacobiThreadsSmall, true>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kJacobiSmemSmall);
+        cudaFuncSetAttribute(k_jacobi_cluster,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)kJacobiSmem);
         attr_set = true;
     }
-    k_jacobi<<<ntiles, kSmallThreads, kJacobiSmem, stream>>>(d_tiles, ws);
+    // Relative orthogonality the rotations stop at: the rank cut needs the
+    // left singular vectors orthonormal to well below tol (their overlap
+    // enters the tail energies squared and the projector linearly).
+    const double eps = fmax(1e-15, fmin(1e-8, 0.01 * tol));
+    k_jacobi<kJacobiThreadsSmall, true>
+        <<<ntiles, kJacobiThreadsSmall, kJacobiSmemSmall, stream>>>(d_tiles, ws, eps);
+    const int worst = jacobi_route(ws.k_max, ws.k_max);
+    if (worst != 3)
+        k_jacobi<kJacobiThreads, false>
+            <<<ntiles, kJacobiThreads, kJacobiSmem, stream>>>(d_tiles, ws, eps);
+    if (worst == 1 || worst == 2)
+        k_jacobi_cluster<<<ntiles * kJacobiCluster, kJacobiThreads,
+                           kJacobiSmem, stream>>>(d_tiles, ws, eps);
 }
 
 // Appends the residual-pass columns to the basis: k1 += kb.
@@ -969,7 +1152,8 @@ k_rank_cut(TileWork *__restrict__ tiles, Workspace ws, double tol,
             r = 0;
         } else {
             const double budget = tol * tol * energy;
-            const double missing = fmax(0.0, energy - total);
+            // energy outside span(W): what the Gram factor left out
+            const double missing = fmax(0.0, tw.tail_h);
             // tail(r) for r = k2 down to 1; keep the smallest r that fits
             double tail = missing;
             r = -1;

@@ -15,11 +15,14 @@ import oracle
 import starsh_b200 as sb
 from harness import RefProblem, approximate_b200, as_ref_blrm
 
-N, MAXRANK, OVERSAMPLE, TOL = 200, 64, 16, 1e-6
+TOL = 1e-6
 
 
 @pytest.mark.gpu
-def test_noalloc_matches_engine_twice(ref, lib):
+@pytest.mark.parametrize("N,MAXRANK,OVERSAMPLE", [(200, 64, 16), (256, 80, 16)])
+def test_noalloc_matches_engine_twice(ref, lib, N, MAXRANK, OVERSAMPLE):
+    # the second case uses the largest tile and sketch width the fixed
+    # scratch accepts (256 x 256, 96 columns)
     import torch
     # one 200 x 200 tile: a smooth 2-D kernel whose rank is below maxrank
     pr = RefProblem(ref, "spatial", N, N, kernel_name="sqexp", beta=0.3)

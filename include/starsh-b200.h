@@ -176,6 +176,10 @@ typedef struct starsh_b200_stats
     long long d2h_bytes;      /* device to host bytes                   */
     long long batches;        /* tile batches (launches of each GEMM step) */
     long long sketch_launches;/* sketch GEMM launches (timed by sketch_ms) */
+    double gen_ms;            /* device time generating far tiles       */
+    double basis_ms;          /* sketch and orthogonalisation, in all   */
+    double svd_ms;            /* Gram of B, its factor, Jacobi, rank cut */
+    double output_ms;         /* U = Q W and V written to the arena     */
 } starsh_b200_stats;
 int starsh_b200_get_stats(starsh_b200_stats *stats);
 

@@ -20,6 +20,7 @@ struct DeviceBuffer {
 struct Context {
     int device = -1;
     cudaStream_t stream = nullptr;
+    cudaStream_t side = nullptr;   // second stream for overlapping launches
     DeviceBuffer workspace;    // per-slot scratch of the engine
     DeviceBuffer tiles;        // TileWork array of a batch
     DeviceBuffer descs;        // GemmDesc array of a batch

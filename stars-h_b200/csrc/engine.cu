@@ -76,6 +76,8 @@ Context *context()
         }
         g_ctx.device = dev;
         if (cudaStreamCreateWithFlags(&g_ctx.stream, cudaStreamNonBlocking)
+                != cudaSuccess ||
+            cudaStreamCreateWithFlags(&g_ctx.side, cudaStreamNonBlocking)
                 != cudaSuccess) {
             cudaGetLastError();
             set_error("cudaStreamCreate failed");
@@ -231,6 +233,7 @@ struct EngineParams {
     int engine;
     int block;      // adaptive sketch: columns of the first round
     int block_next; // ... and of every later round
+    int verify;     // unselected sample columns that finish a tile
 };
 
 // Runs the device pipeline over all far blocks of F.  Fills ranks (host)
@@ -303,8 +306,16 @@ static int compress_far(Context &ctx, const DevKernel &K, STARSH_blrf *F,
     TileWork *dt = (TileWork *)ctx.tiles.ptr;
     GemmDesc *dd = (GemmDesc *)ctx.descs.ptr;
 
-    cudaEvent_t ev[4];
+    // ev[0..1] sketch GEMM, ev[2..3] projection GEMM, ev[4] generation
+    // start, ev[5] basis start, ev[6] SVD end, ev[7..8] output
+    cudaEvent_t ev[9];
     for (auto &e : ev) cudaEventCreate(&e);
+    bool output_pending = false;
+    auto phase_ms = [&](int a, int b) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ev[a], ev[b]);
+        return (double)ms;
+    };
     OutArena none{nullptr, nullptr};
     int info = STARSH_SUCCESS;
 
@@ -322,8 +333,10 @@ static int compress_far(Context &ctx, const DevKernel &K, STARSH_blrf *F,
         for (int t = 0; t < nt; ++t) all[b0 + t].slot = t;
         cudaMemcpyAsync(dt, &all[b0], nt * sizeof(TileWork),
                         cudaMemcpyHostToDevice, s);
+        cudaEventRecord(ev[4], s);
         launch_gen_tiles(K, dt, nt, ws, s);
         count_launch();
+        cudaEventRecord(ev[5], s);
         if (ep.engine == STARSH_B200_FP64) {
         cudaEventRecord(ev[0], s);
         if ((info = gemm(STEP_SKETCH, false, false, nt, m_max, k_max, none))) break;
@@ -362,9 +375,10 @@ static int compress_far(Context &ctx, const DevKernel &K, STARSH_blrf *F,
         } else {
         // Adaptive sketch: sample Omega in blocks; each round projects the
         // new sample off the basis, keeps the residual directions above
-        // (tol/10)^2 ||D||_F^2 and stops a tile when a round adds none
-        // (the residual estimate of N. Halko, P.-G. Martinsson, J. A. Tropp,
-        // SIAM Review 53 (2011) sec. 4.3) or after k columns.
+        // (tol/10)^2 ||D||_F^2 and stops a tile once `verify` columns of a
+        // round stayed below that threshold (the residual estimate of
+        // N. Halko, P.-G. Martinsson, J. A. Tropp, SIAM Review 53 (2011)
+        // sec. 4.3), when a round adds none, or after k columns.
         launch_block_norms(dt, dt, nt, ws, s);
         count_launch();
         int *d_active = (int *)ctx.flag.ptr;
@@ -419,7 +433,7 @@ static int compress_far(Context &ctx, const DevKernel &K, STARSH_blrf *F,
                 count_launch();
                 if ((info = append(bmax))) break;
             }
-            launch_round_end(dt, nt, s);
+            launch_round_end(dt, nt, ep.verify, s);
             count_launch();
             float ms = 0.f;
             cudaEventSynchronize(ev[1]);
@@ -435,18 +449,22 @@ static int compress_far(Context &ctx, const DevKernel &K, STARSH_blrf *F,
         cudaEventRecord(ev[3], s);
         if ((info = gemm(STEP_GRAM_B, false, true, nt, k_max, k_max, none))) break;
         launch_pivchol(2, dt, dt, nt, ws, ep.tol, s);
-        launch_jacobi(dt, nt, ws, ep.tol, s);
+        launch_jacobi(dt, nt, ws, ep.tol, s, ctx.side);
         count_launch(2);
         if ((info = gemm(STEP_ROTATE, true, false, nt, k_max, n_max, none))) break;
         launch_rank_cut(dt, nt, ws, ep.tol, ep.maxrank, s);
         count_launch();
+        cudaEventRecord(ev[6], s);
         B200_CUDA(cudaMemcpyAsync(&all[b0], dt, nt * sizeof(TileWork),
                                   cudaMemcpyDeviceToHost, s),
                   "cudaMemcpyAsync(tiles)");
         B200_CUDA(cudaStreamSynchronize(s), "compression pipeline");
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, ev[2], ev[3]);
-        st.project_ms += ms;
+        st.project_ms += phase_ms(2, 3);
+        st.gen_ms += phase_ms(4, 5);
+        st.basis_ms += phase_ms(5, 2);
+        st.svd_ms += phase_ms(3, 6);
+        if (output_pending) st.output_ms += phase_ms(7, 8);
+        output_pending = false;
         // Output placement of this batch: one device chunk for U and V.
         size_t nu = 0, nv = 0;
         for (int t = 0; t < nt; ++t) {
@@ -487,18 +505,35 @@ static int compress_far(Context &ctx, const DevKernel &K, STARSH_blrf *F,
         if (nu + nv > 0) {
             cudaMemcpyAsync(dt, &all[b0], nt * sizeof(TileWork),
                             cudaMemcpyHostToDevice, s);
+            cudaEventRecord(ev[7], s);
             launch_select_w(dt, nt, ws, s);
             count_launch();
             if ((info = gemm(STEP_OUT_U, false, false, nt, m_max, k_max, out))) break;
             launch_write_v(dt, nt, ws, out, s);
             count_launch();
+            cudaEventRecord(ev[8], s);
+            output_pending = true;
+        }
+        if (const char *path = getenv("STARSH_B200_TILE_LOG")) {
+            // diagnostics: one line per tile of the shape, basis and factor
+            // sizes, Jacobi sweeps and rank
+            if (FILE *f = fopen(path, b0 == 0 ? "w" : "a")) {
+                for (int t = 0; t < nt; ++t) {
+                    const TileWork &w = all[b0 + t];
+                    fprintf(f, "%d %d %d %d %d %d %d %d\n", w.m, w.n, w.cols_done,
+                            w.k1, w.k2, w.sweeps, w.rank, w.status);
+                }
+                fclose(f);
+            }
         }
         st.tiles += nt;
         st.batches += 1;
     }
-    for (auto &e : ev) cudaEventDestroy(e);
-    if (info == STARSH_SUCCESS)
+    if (info == STARSH_SUCCESS) {
         B200_CUDA(cudaStreamSynchronize(s), "factor output");
+        if (output_pending) st.output_ms += phase_ms(7, 8);
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
     return info;
 }
 
@@ -676,13 +711,15 @@ static int approximate(STARSH_blrm **matrix, STARSH_blrf *F, int maxrank,
     auto *rec = new Record();
     rec->points = points;
     std::vector<int> rank;
-    int block = 64, block_next = 32;
+    int block = 64, block_next = 32, verify = 10;
     if (const char *e = getenv("STARSH_B200_SKETCH_BLOCK"))
         block = std::max(8, std::min(1024, atoi(e)));
     if (const char *e = getenv("STARSH_B200_SKETCH_STEP"))
         block_next = std::max(8, std::min(1024, atoi(e)));
+    if (const char *e = getenv("STARSH_B200_SKETCH_VERIFY"))
+        verify = std::max(1, std::min(1024, atoi(e)));
     EngineParams ep{maxrank, tol, b200_oversample(), engine, block,
-                    block_next};
+                    block_next, verify};
     info = compress_far(*ctx, points->K, F, ep, rank, *rec);
     if (info) {
         delete rec;

@@ -35,6 +35,8 @@ struct TileWork {
     int bcur;               // columns of the current round (0: inactive)
     int done;               // sampling finished (converged or capped)
     int kround;             // directions the current round's sample added
+    int k1_round;           // basis columns when the current round began
+    int sweeps;             // Jacobi sweeps the small SVD took
     long long off_u, off_v; // output offsets (doubles)
 };
 
@@ -126,7 +128,7 @@ void launch_gather_cols(int phase, const TileWork *d_tiles, int ntiles,
 void launch_chol_inv(int phase, TileWork *d_tiles, int ntiles, Workspace ws,
                      cudaStream_t stream);
 void launch_jacobi(TileWork *d_tiles, int ntiles, Workspace ws, double tol,
-                   cudaStream_t stream);
+                   cudaStream_t stream, cudaStream_t side);
 void launch_rank_cut(TileWork *d_tiles, int ntiles, Workspace ws,
                      double tol, int maxrank, cudaStream_t stream);
 void launch_merge_basis(TileWork *d_tiles, int ntiles, cudaStream_t stream);
@@ -137,7 +139,8 @@ void launch_block_norms(const TileWork *d_tiles, TileWork *d_rw, int ntiles,
                         Workspace ws, cudaStream_t stream);
 void launch_round_setup(TileWork *d_tiles, int ntiles, int block,
                         int *d_active, cudaStream_t stream);
-void launch_round_end(TileWork *d_tiles, int ntiles, cudaStream_t stream);
+void launch_round_end(TileWork *d_tiles, int ntiles, int verify,
+                      cudaStream_t stream);
 void launch_round_pivchol(TileWork *d_tiles, int ntiles, Workspace ws,
                           double tol, int repeat, cudaStream_t stream);
 void launch_select_w(const TileWork *d_tiles, int ntiles, Workspace ws,

@@ -172,7 +172,7 @@ extern "C" int starsh_b200_dense_rsvd_noalloc(const double *dD, int nrows,
     if ((info = gemm(STEP_PROJECT, true, false, k, n, none))) return info;
     if ((info = gemm(STEP_GRAM_B, false, true, k, k, none))) return info;
     launch_pivchol(2, dt, dt, 1, ws, tol, s);
-    launch_jacobi(dt, 1, ws, tol, s);
+    launch_jacobi(dt, 1, ws, tol, s, nullptr);
     if ((info = gemm(STEP_ROTATE, true, false, k, n, none))) return info;
     launch_rank_cut(dt, 1, ws, tol, maxrank, s);
     // One tile: its factors start at offset 0 of the caller's buffers, so

@@ -19,10 +19,7 @@
 //     decides the rank is exact to FP64 rounding even where the Gram's
 //     eigenvalues are not.
 #include <cfloat>
-#include <cooperative_groups.h>
 #include "engine.cuh"
-
-namespace cg = cooperative_groups;
 
 namespace b200 {
 
@@ -680,6 +677,7 @@ __global__ void k_round_setup(TileWork *__restrict__ tiles, int ntiles,
         return;
     }
     tw.bcur = min(block, tw.k - tw.cols_done);
+    tw.k1_round = tw.k1;
     atomicOr(active, 1);
 }
 
@@ -691,25 +689,32 @@ void launch_round_setup(TileWork *d_tiles, int ntiles, int block,
                                                             block, d_active);
 }
 
-// End of a round: the new orthonormal columns join the basis; a round that
-// found no direction above the threshold (or exhausted the k columns)
-// finishes the tile.
-__global__ void k_round_end(TileWork *__restrict__ tiles, int ntiles)
+// End of a round: the new orthonormal columns join the basis.  The tile is
+// finished when the round's sample left at least `verify` columns whose
+// residuals against the grown basis all fell below the threshold (so the
+// residual estimate rests on that many independent Gaussian samples), when
+// it found no direction at all, or when the k columns are exhausted.
+__global__ void k_round_end(TileWork *__restrict__ tiles, int ntiles,
+                            int verify)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= ntiles) return;
     TileWork &tw = tiles[t];
     if (tw.bcur <= 0) return;
     tw.cols_done += tw.bcur;
-    if (tw.kround == 0 || tw.cols_done >= tw.k) tw.done = 1;
+    const int added = tw.k1 + tw.kb - tw.k1_round;
+    if (tw.kround == 0 || tw.cols_done >= tw.k || tw.bcur - added >= verify)
+        tw.done = 1;
     tw.k1 += tw.kb;       // (kb is 0 here: each pass merged its columns)
     tw.kb = 0;
     tw.bcur = 0;
 }
 
-void launch_round_end(TileWork *d_tiles, int ntiles, cudaStream_t stream)
+void launch_round_end(TileWork *d_tiles, int ntiles, int verify,
+                      cudaStream_t stream)
 {
-    k_round_end<<<(ntiles + 127) / 128, 128, 0, stream>>>(d_tiles, ntiles);
+    k_round_end<<<(ntiles + 127) / 128, 128, 0, stream>>>(d_tiles, ntiles,
+                                                          verify);
 }
 
 void launch_pivchol(int phase, const TileWork *, TileWork *d_tiles_rw,
@@ -807,45 +812,110 @@ void launch_chol_inv(int phase, TileWork *d_tiles, int ntiles, Workspace ws,
 // -------------------------------------------------- one-sided Jacobi
 
 // One-sided Jacobi (Hestenes) on the columns of A = L(slot) (k1 x k2):
-// column pairs are rotated until mutually orthogonal; then the columns
-// of A V are the eigenvectors of L L^T scaled by the singular values.
-// Pairs follow the round-robin tournament ordering, k2/2 disjoint pairs per
-// step, one warp per pair.  W (normalised columns) goes to T(slot), the
-// squared column norms to Sig(slot).  A tile whose columns fit in the
-// dynamic shared memory is rotated there; a larger one in place in global
-// memory (L2-resident).
-constexpr size_t kJacobiSmem = 200 * 1024;
-constexpr int kJacobiThreads = 1024;
-constexpr int kJacobiRegRows = 9;   // rows per lane kept in registers (<= 288)
+// column pairs are rotated until mutually orthogonal; then the columns of
+// A V are the eigenvectors of L L^T scaled by the singular values.  L comes
+// from a pivoted Cholesky of B B^T (the transpose of a column-pivoted QR
+// factor of B^T), the preconditioning under which one-sided Jacobi needs
+// few sweeps (Z. Drmac, K. Veselic, SIAM J. Matrix Anal. Appl. 29 (2008)).
+// Pairs follow the round-robin tournament ordering: k2/2 disjoint pairs per
+// step, all rotated at once, a block barrier between steps.
+//
+// The cost is the chain of dependent steps (k2 - 1 per sweep), each issue
+// bound on its SM for large tiles, so a pair is rotated by a group of G
+// lanes holding E rows each in registers (G E >= k1): the group sizes its
+// dot-product reduction to the column length, and a warp rotates 32 / G
+// pairs at once, sharing the instructions of the rotation angle among
+// them.  The kernel is instantiated per size
+// class; tiles of one class share a launch, every other tile's CTA returns
+// at once.  Columns live in shared memory when they fit, otherwise in
+// global memory (L2-resident for the tiles of one launch).  W (normalised
+// columns) goes to T(slot), squared norms to Sig(slot).
+constexpr size_t kJacobiSmemMax = 220 * 1024;
 
-// One rotation of the column pair (a, b) by one warp.  With REG the pair is
-// loaded into registers once (independent loads in flight, one round trip),
-// otherwise streamed.  Returns true if the pair was rotated.
-template <bool REG>
-__device__ __forceinline__ bool jacobi_pair(double *ca, double *cb, int rows,
-                                            int lane, double eps)
+struct JacobiClass {
+    int groups;     // G: lanes per pair
+    int per_lane;   // E: rows per lane
+    int threads;
+    bool smem;
+};
+
+// Size classes, by rows (k1); shared-memory classes first.  The last class
+// streams rows through registers for k1 > 512.
+__host__ __device__ inline int jacobi_class(int rows, int cols)
 {
-    double xa[REG ? kJacobiRegRows : 1], xb[REG ? kJacobiRegRows : 1];
+    const size_t bytes = (size_t)(rows | 1) * cols * sizeof(double);
+    const bool fits = bytes <= kJacobiSmemMax;
+    if (rows <= 32) return 0;                     // G 4,  E 8,  64 threads
+    if (rows <= 64) return 1;                     // G 4,  E 16, 128 threads
+    if (rows <= 128) return 2;                    // G 8,  E 16, 512 threads
+    if (rows <= 256) return fits ? 3 : 4;         // G 16, E 16, 512 threads
+    if (rows <= 512) return 5;                    // G 32, E 16, 512, global
+    return 6;                                     // streamed, global
+}
+
+// Rotation of the column pair (ca, cb) by the G lanes of one group (gl =
+// lane within the group).  Every lane of the warp calls this (inactive
+// groups with valid = false) because the reductions shuffle across the
+// whole warp.  Returns true if the pair was rotated.
+template <int G, int E>
+__device__ __forceinline__ bool jacobi_rotate(double *ca, double *cb, int rows,
+                                              int gl, bool valid, double eps2)
+{
+    double xa[E], xb[E];
     double al = 0.0, be = 0.0, ga = 0.0;
-    if (REG) {
-        #pragma unroll
-        for (int q = 0; q < kJacobiRegRows; ++q) {
-            const int i = lane + 32 * q;
-            xa[q] = i < rows ? ca[i] : 0.0;
-            xb[q] = i < rows ? cb[i] : 0.0;
+    #pragma unroll
+    for (int q = 0; q < E; ++q) {
+        const int i = gl + G * q;
+        const bool in = valid && i < rows;
+        xa[q] = in ? ca[i] : 0.0;
+        xb[q] = in ? cb[i] : 0.0;
+    }
+    #pragma unroll
+    for (int q = 0; q < E; ++q) {
+        al = fma(xa[q], xa[q], al);
+        be = fma(xb[q], xb[q], be);
+        ga = fma(xa[q], xb[q], ga);
+    }
+    #pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) {
+        al += __shfl_xor_sync(0xffffffffu, al, o);
+        be += __shfl_xor_sync(0xffffffffu, be, o);
+        ga += __shfl_xor_sync(0xffffffffu, ga, o);
+    }
+    // |gamma| > eps sqrt(alpha beta), compared in squares
+    if (!(ga * ga > eps2 * al * be) || !(al > 0.0) || !(be > 0.0))
+        return false;
+    // t = sign(zeta) / (|zeta| + sqrt(1 + zeta^2)), zeta = (beta - alpha) /
+    // (2 gamma), rewritten with one division: t = sign(d) g / (|d| + h),
+    // d = beta - alpha, g = 2 gamma, h = sqrt(d^2 + g^2).
+    const double d = be - al, g = 2.0 * ga;
+    const double h = sqrt(fma(d, d, g * g));
+    const double t = (d >= 0.0 ? g : -g) / (fabs(d) + h);
+    const double c = rsqrt(fma(t, t, 1.0));
+    const double sn = c * t;
+    #pragma unroll
+    for (int q = 0; q < E; ++q) {
+        const int i = gl + G * q;
+        if (i < rows) {
+            ca[i] = c * xa[q] - sn * xb[q];
+            cb[i] = sn * xa[q] + c * xb[q];
         }
-        #pragma unroll
-        for (int q = 0; q < kJacobiRegRows; ++q) {
-            al += xa[q] * xa[q];
-            be += xb[q] * xb[q];
-            ga += xa[q] * xb[q];
-        }
-    } else {
+    }
+    return true;
+}
+
+// The same for long columns: rows streamed in chunks of 32 per lane (one
+// warp per pair), loaded twice (dot products, then rotation).
+__device__ bool jacobi_rotate_stream(double *ca, double *cb, int rows,
+                                     int lane, bool valid, double eps2)
+{
+    double al = 0.0, be = 0.0, ga = 0.0;
+    if (valid) {
         for (int i = lane; i < rows; i += 32) {
             const double x = ca[i], y = cb[i];
-            al += x * x;
-            be += y * y;
-            ga += x * y;
+            al = fma(x, x, al);
+            be = fma(y, y, be);
+            ga = fma(x, y, ga);
         }
     }
     #pragma unroll
@@ -854,233 +924,166 @@ __device__ __forceinline__ bool jacobi_pair(double *ca, double *cb, int rows,
         be += __shfl_xor_sync(0xffffffffu, be, o);
         ga += __shfl_xor_sync(0xffffffffu, ga, o);
     }
-    if (!(fabs(ga) > eps * sqrt(al * be)) || al == 0.0 || be == 0.0)
+    if (!(ga * ga > eps2 * al * be) || !(al > 0.0) || !(be > 0.0))
         return false;
-    const double zeta = (be - al) / (2.0 * ga);
-    const double t = (zeta >= 0.0 ? 1.0 : -1.0) /
-                     (fabs(zeta) + sqrt(1.0 + zeta * zeta));
-    const double c = 1.0 / sqrt(1.0 + t * t);
+    const double d = be - al, g = 2.0 * ga;
+    const double h = sqrt(fma(d, d, g * g));
+    const double t = (d >= 0.0 ? g : -g) / (fabs(d) + h);
+    const double c = rsqrt(fma(t, t, 1.0));
     const double sn = c * t;
-    if (REG) {
-        #pragma unroll
-        for (int q = 0; q < kJacobiRegRows; ++q) {
-            const int i = lane + 32 * q;
-            if (i < rows) {
-                ca[i] = c * xa[q] - sn * xb[q];
-                cb[i] = sn * xa[q] + c * xb[q];
-            }
-        }
-    } else {
-        for (int i = lane; i < rows; i += 32) {
-            const double x = ca[i], y = cb[i];
-            ca[i] = c * x - sn * y;
-            cb[i] = sn * x + c * y;
-        }
+    for (int i = lane; i < rows; i += 32) {
+        const double x = ca[i], y = cb[i];
+        ca[i] = c * x - sn * y;
+        cb[i] = sn * x + c * y;
     }
     return true;
 }
 
-// One-sided Jacobi (Hestenes) on the columns of A = L(slot) (k1 x k2):
-// column pairs are rotated until mutually orthogonal; then the columns of
-// A V are the eigenvectors of L L^T scaled by the singular values.  L comes
-// from a pivoted Cholesky of B B^T (the transpose of a column-pivoted QR
-// factor of B^T), the preconditioning under which one-sided Jacobi needs
-// few sweeps (Z. Drmac, K. Veselic, SIAM J. Matrix Anal. Appl. 29 (2008)).
-// Pairs follow the round-robin tournament ordering, k2/2 disjoint pairs per
-// step, one warp per pair, 32 warps.  A tile whose columns fit in the
-// dynamic shared memory is rotated there, a larger one in place in global
-// memory (L2-resident), where each pair makes a single load round trip.
-// W (normalised columns) goes to T(slot), squared norms to Sig(slot).
-constexpr int kJacobiCluster = 4;
-constexpr size_t kJacobiSmemSmall = 48 * 1024;
-constexpr int kJacobiThreadsSmall = 256;
-
-// Where the Jacobi of a k1 x k2 factor runs: 3 a small CTA (256 threads,
-// 48 KB) with the columns in shared memory, 0 a full CTA (1024 threads,
-// 200 KB) likewise, 1 a cluster of kJacobiCluster CTAs sharing them through
-// distributed shared memory, 2 one CTA on global memory.
-__host__ __device__ inline int jacobi_route(int rows, int cols)
-{
-    const size_t lds = (size_t)(rows | 1);
-    if (lds * cols * sizeof(double) <= kJacobiSmemSmall) return 3;
-    if (lds * cols * sizeof(double) <= kJacobiSmem) return 0;
-    const size_t cpb = (cols + kJacobiCluster - 1) / kJacobiCluster;
-    if (lds * cpb * sizeof(double) <= kJacobiSmem) return 1;
-    return 2;
-}
-
-template <int THREADS, bool SMALL>
-__global__ void __launch_bounds__(THREADS)
-k_jacobi(TileWork *__restrict__ tiles, Workspace ws, double eps)
+template <int CLASS, int G, int E, int THREADS, bool SMEM>
+__global__ void __launch_bounds__(THREADS, THREADS <= 128 ? 512 / THREADS : 1)
+k_jacobi(TileWork *__restrict__ tiles, Workspace ws, double eps2)
 {
     extern __shared__ double sm[];
-    __shared__ int rotated;
+    __shared__ int rotated[2];
     TileWork &tw = tiles[blockIdx.x];
     const int s = tw.slot;
     const int rows = tw.k1, cols = tw.k2;
-    if (cols <= 0) return;
-    const int route = jacobi_route(rows, cols);
-    if (SMALL ? route != 3 : (route != 0 && route != 2)) return;
+    if (cols <= 0 || jacobi_class(rows, cols) != CLASS) return;   // uniform
     const int ldg = ws.ldK();
     const int lds = rows | 1;   // odd stride: fewer bank conflicts
-    const bool in_smem = route != 2;
-    double *A = in_smem ? sm : ws.L(s);
-    const int lda = in_smem ? lds : ldg;
-    if (in_smem) {
+    double *A = SMEM ? sm : ws.L(s);
+    const int lda = SMEM ? lds : ldg;
+    if (SMEM) {
         const double *Lg = ws.L(s);
-        for (int c = 0; c < cols; ++c)
-            for (int i = threadIdx.x; i < rows; i += blockDim.x)
-                A[(size_t)c * lda + i] = Lg[(size_t)c * ldg + i];
-        __syncthreads();
+        for (int e = threadIdx.x; e < rows * cols; e += THREADS) {
+            const int c = e / rows, i = e - c * rows;
+            A[(size_t)c * lda + i] = Lg[(size_t)c * ldg + i];
+        }
     }
+    if (threadIdx.x == 0) rotated[0] = rotated[1] = 0;
+    __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int nwarps = blockDim.x >> 5;
+    constexpr int kGroupsPerWarp = 32 / G;
+    constexpr int kWarps = THREADS / 32;
+    const int gw = lane / G, gl = lane % G;
     const int nc = cols + (cols & 1);      // players, with a bye if odd
     const int npairs = nc / 2;
-    const bool reg = rows <= 32 * kJacobiRegRows;
     int sweep = 0;
     for (; sweep < 40; ++sweep) {
-        if (threadIdx.x == 0) rotated = 0;
-        __syncthreads();
         bool any = false;
         for (int step = 0; step < nc - 1; ++step) {
-            for (int p = warp; p < npairs; p += nwarps) {
-                const int a = p == 0 ? 0 : 1 + (p - 1 + step) % (nc - 1);
-                const int b = 1 + (nc - 2 - p + step) % (nc - 1);
-                if (a >= cols || b >= cols) continue;
+            for (int base = warp * kGroupsPerWarp; base < npairs;
+                 base += kWarps * kGroupsPerWarp) {
+                const int p = base + gw;
+                int a = 0, b = 0;
+                if (p < npairs) {
+                    // a = 1 + (p - 1 + step) mod (nc - 1) for p > 0,
+                    // b = 1 + (nc - 2 - p + step) mod (nc - 1); both
+                    // arguments lie in [0, 2 (nc - 1))
+                    int x = p - 1 + step, y = nc - 2 - p + step;
+                    if (x >= nc - 1) x -= nc - 1;
+                    if (y >= nc - 1) y -= nc - 1;
+                    a = p == 0 ? 0 : 1 + x;
+                    b = 1 + y;
+                }
+                const bool valid = p < npairs && a < cols && b < cols;
                 double *ca = A + (size_t)a * lda, *cb = A + (size_t)b * lda;
-                any |= reg ? jacobi_pair<true>(ca, cb, rows, lane, eps)
-                           : jacobi_pair<false>(ca, cb, rows, lane, eps);
+                if constexpr (E > 0)
+                    any |= jacobi_rotate<G, E>(ca, cb, rows, gl, valid, eps2);
+                else
+                    any |= jacobi_rotate_stream(ca, cb, rows, lane, valid, eps2);
             }
             __syncthreads();
         }
-        if (any && lane == 0) rotated = 1;
+        // double-buffered flag: cleared one sweep ahead, read after a barrier
+        if (any) rotated[sweep & 1] = 1;
+        if (threadIdx.x == 0) rotated[(sweep + 1) & 1] = 0;
         __syncthreads();
-        if (!rotated) break;
+        if (!rotated[sweep & 1]) break;
     }
     // Normalise into W = T(slot); squared norms into Sig.
     double *W = ws.T(s);
     double *sig = ws.Sig(s);
-    for (int c = warp; c < cols; c += nwarps) {
+    for (int c = warp; c < cols; c += kWarps) {
         const double *ca = A + (size_t)c * lda;
         double nrm = 0.0;
-        for (int i = lane; i < rows; i += 32) nrm += ca[i] * ca[i];
+        for (int i = lane; i < rows; i += 32) nrm = fma(ca[i], ca[i], nrm);
         #pragma unroll
         for (int o = 16; o > 0; o >>= 1) nrm += __shfl_xor_sync(0xffffffffu, nrm, o);
         const double inv = nrm > 0.0 ? 1.0 / sqrt(nrm) : 0.0;
         for (int i = lane; i < rows; i += 32) W[(size_t)c * ldg + i] = ca[i] * inv;
         if (lane == 0) sig[c] = nrm;
     }
-    if (threadIdx.x == 0 && sweep >= 40) tw.status |= TILE_JACOBI_SLOW;
+    if (threadIdx.x == 0) {
+        tw.sweeps = sweep;
+        if (sweep >= 40) tw.status |= TILE_JACOBI_SLOW;
+    }
 }
 
-
-// The same one-sided Jacobi for factors too large for one CTA's shared
-// memory: a cluster of kJacobiCluster CTAs holds the columns, CTA r owning
-// columns [r cpb, (r+1) cpb).  A pair is rotated by one warp of any CTA
-// through distributed shared memory (generic pointers from
-// cluster.map_shared_rank), so every column load and store stays on chip;
-// the cluster synchronises after each round-robin step.
-__global__ void __cluster_dims__(kJacobiCluster, 1, 1)
-__launch_bounds__(kJacobiThreads)
-k_jacobi_cluster(TileWork *__restrict__ tiles, Workspace ws, double eps)
+template <int CLASS, int G, int E, int THREADS, bool SMEM>
+static void jacobi_class_launch(TileWork *d_tiles, int ntiles, Workspace ws,
+                                double eps2, size_t smem, cudaStream_t stream)
 {
-    extern __shared__ double sm[];
-    __shared__ int rotated;
-    cg::cluster_group cluster = cg::this_cluster();
-    const int crank = (int)cluster.block_rank();
-    TileWork &tw = tiles[blockIdx.x / kJacobiCluster];
-    const int s = tw.slot;
-    const int rows = tw.k1, cols = tw.k2;
-    if (cols <= 0 || jacobi_route(rows, cols) != 1) return;   // uniform
-    const int ldg = ws.ldK();
-    const int lds = rows | 1;
-    const int cpb = (cols + kJacobiCluster - 1) / kJacobiCluster;
-    const int c0 = crank * cpb, c1 = min(cols, c0 + cpb);
-    const double *Lg = ws.L(s);
-    for (int c = c0; c < c1; ++c)
-        for (int i = threadIdx.x; i < rows; i += blockDim.x)
-            sm[(size_t)(c - c0) * lds + i] = Lg[(size_t)c * ldg + i];
-    if (threadIdx.x == 0) rotated = 0;
-    cluster.sync();
-    auto col = [&](int c) -> double * {
-        double *base = cluster.map_shared_rank(sm, c / cpb);
-        return base + (size_t)(c % cpb) * lds;
-    };
-    const int lane = threadIdx.x & 31;
-    const int gwarp = crank * (kJacobiThreads / 32) + (threadIdx.x >> 5);
-    const int nwarps = kJacobiCluster * (kJacobiThreads / 32);
-    const int nc = cols + (cols & 1);
-    const int npairs = nc / 2;
-    const bool reg = rows <= 32 * kJacobiRegRows;
-    int sweep = 0;
-    for (; sweep < 40; ++sweep) {
-        bool any = false;
-        for (int step = 0; step < nc - 1; ++step) {
-            for (int p = gwarp; p < npairs; p += nwarps) {
-                const int a = p == 0 ? 0 : 1 + (p - 1 + step) % (nc - 1);
-                const int b = 1 + (nc - 2 - p + step) % (nc - 1);
-                if (a >= cols || b >= cols) continue;
-                any |= reg ? jacobi_pair<true>(col(a), col(b), rows, lane, eps)
-                           : jacobi_pair<false>(col(a), col(b), rows, lane, eps);
-            }
-            cluster.sync();
-        }
-        if (any && lane == 0) atomicOr(cluster.map_shared_rank(&rotated, 0), 1);
-        cluster.sync();
-        const int r = *cluster.map_shared_rank(&rotated, 0);
-        cluster.sync();
-        if (crank == 0 && threadIdx.x == 0) rotated = 0;
-        cluster.sync();
-        if (!r) break;
-    }
-    double *W = ws.T(s);
-    double *sig = ws.Sig(s);
-    const int warp = threadIdx.x >> 5;
-    for (int c = c0 + warp; c < c1; c += kJacobiThreads / 32) {
-        const double *ca = sm + (size_t)(c - c0) * lds;
-        double nrm = 0.0;
-        for (int i = lane; i < rows; i += 32) nrm += ca[i] * ca[i];
-        #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) nrm += __shfl_xor_sync(0xffffffffu, nrm, o);
-        const double inv = nrm > 0.0 ? 1.0 / sqrt(nrm) : 0.0;
-        for (int i = lane; i < rows; i += 32) W[(size_t)c * ldg + i] = ca[i] * inv;
-        if (lane == 0) sig[c] = nrm;
-    }
-    if (crank == 0 && threadIdx.x == 0 && sweep >= 40)
-        tw.status |= TILE_JACOBI_SLOW;
-    cluster.sync();   // no CTA leaves while others may read its columns
+    auto *fn = k_jacobi<CLASS, G, E, THREADS, SMEM>;
+    if (SMEM && smem > 48 * 1024)
+        cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+    fn<<<ntiles, THREADS, SMEM ? smem : 0, stream>>>(d_tiles, ws, eps2);
 }
 
 void launch_jacobi(TileWork *d_tiles, int ntiles, Workspace ws, double tol,
-                   cudaStream_t stream)
+                   cudaStream_t stream, cudaStream_t side)
 {
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaFuncSetAttribute(k_jacobi<kJacobiThreads, false>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)kJacobiSmem);
-        cudaFuncSetAttribute(k_jacobi<kJacobiThreadsSmall, true>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)kJacobiSmemSmall);
-        cudaFuncSetAttribute(k_jacobi_cluster,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)kJacobiSmem);
-        attr_set = true;
-    }
     // Relative orthogonality the rotations stop at: the rank cut needs the
     // left singular vectors orthonormal to well below tol (their overlap
     // enters the tail energies squared and the projector linearly).
     const double eps = fmax(1e-15, fmin(1e-8, 0.01 * tol));
-    k_jacobi<kJacobiThreadsSmall, true>
-        <<<ntiles, kJacobiThreadsSmall, kJacobiSmemSmall, stream>>>(d_tiles, ws, eps);
-    const int worst = jacobi_route(ws.k_max, ws.k_max);
-    if (worst != 3)
-        k_jacobi<kJacobiThreads, false>
-            <<<ntiles, kJacobiThreads, kJacobiSmem, stream>>>(d_tiles, ws, eps);
-    if (worst == 1 || worst == 2)
-        k_jacobi_cluster<<<ntiles * kJacobiCluster, kJacobiThreads,
-                           kJacobiSmem, stream>>>(d_tiles, ws, eps);
+    const double eps2 = eps * eps;
+    // Classes a batch can reach, from the largest factor it may hold
+    // (k1, k2 <= k_max).  Shared memory is sized for the class's largest
+    // tile that fits.
+    const int kmax = ws.k_max;
+    auto smem_for = [&](int rows) {
+        const int r = std::min(rows, kmax);
+        const size_t full = (size_t)(r | 1) * std::min(r, kmax) * sizeof(double);
+        return std::min(full, kJacobiSmemMax);
+    };
+    // The classes that hold many CTAs per SM run on `stream`; the large
+    // classes (one CTA per SM, long-running) on `side`, overlapping them.
+    cudaStream_t big = side ? side : stream;
+    cudaEvent_t fork = nullptr, join = nullptr;
+    if (side && kmax > 64) {
+        cudaEventCreateWithFlags(&fork, cudaEventDisableTiming);
+        cudaEventCreateWithFlags(&join, cudaEventDisableTiming);
+        cudaEventRecord(fork, stream);
+        cudaStreamWaitEvent(side, fork, 0);
+    }
+    if (kmax > 128) {
+        jacobi_class_launch<4, 16, 16, 512, false>(d_tiles, ntiles, ws, eps2, 0,
+                                                   big);
+        jacobi_class_launch<3, 16, 16, 512, true>(d_tiles, ntiles, ws, eps2,
+                                                  smem_for(256), big);
+    }
+    if (kmax > 64)
+        jacobi_class_launch<2, 8, 16, 512, true>(d_tiles, ntiles, ws, eps2,
+                                                 smem_for(128), big);
+    if (kmax > 256)
+        jacobi_class_launch<5, 32, 16, 512, false>(d_tiles, ntiles, ws, eps2, 0,
+                                                   big);
+    if (kmax > 512)
+        jacobi_class_launch<6, 32, 0, 1024, false>(d_tiles, ntiles, ws, eps2, 0,
+                                                   big);
+    jacobi_class_launch<0, 4, 8, 64, true>(d_tiles, ntiles, ws, eps2,
+                                           smem_for(32), stream);
+    if (kmax > 32)
+        jacobi_class_launch<1, 4, 16, 128, true>(d_tiles, ntiles, ws, eps2,
+                                                 smem_for(64), stream);
+    if (fork) {
+        cudaEventRecord(join, side);
+        cudaStreamWaitEvent(stream, join, 0);
+        cudaEventDestroy(fork);
+        cudaEventDestroy(join);
+    }
 }
 
 // Appends the residual-pass columns to the basis: k1 += kb.

@@ -125,7 +125,9 @@ class Stats(Structure):
                 ("entries", c_longlong), ("kernel_launches", c_longlong),
                 ("rank_sum", c_longlong), ("max_rank", c_int),
                 ("h2d_bytes", c_longlong), ("d2h_bytes", c_longlong),
-                ("batches", c_longlong), ("sketch_launches", c_longlong)]
+                ("batches", c_longlong), ("sketch_launches", c_longlong),
+                ("gen_ms", c_double), ("basis_ms", c_double),
+                ("svd_ms", c_double), ("output_ms", c_double)]
 
 
 def _proto(lib):

@@ -32,11 +32,15 @@ extern "C" {
 int starsh_blrm__drsdd_b200(STARSH_blrm **matrix, STARSH_blrf *format,
         int maxrank, double tol, int onfly);
 
-/* Same contract; the Gaussian sketch Y = D*Omega runs on the tcgen05 tensor
- * cores in split BF16 (hi/lo parts, three products, FP32 accumulation per
- * K-chunk, FP64 sum of chunks) with D generated in shared memory.
- * Orthogonalisation, projection, small SVD and the rank decision are FP64.
- * Selected by STARSH_LRENGINE=RSVD_MP on the B200 backend. */
+/* Same contract with an adaptive sketch width: Gaussian columns are drawn
+ * in blocks (64, then 32), each block is projected off the basis built so
+ * far and only directions above (tol/10)^2 ||D||_F^2 are kept; a tile stops
+ * once a block leaves 10 columns below that threshold (a posterior
+ * residual estimate) or its k = min(maxrank + oversample, m, n) columns are
+ * used.  Low-rank tiles therefore pay for a few dozen sketch columns
+ * instead of k.  Projection, small SVD and the rank decision are as in
+ * starsh_blrm__drsdd_b200, all in FP64.  Selected by STARSH_LRENGINE=
+ * RSVD_MP on the B200 backend. */
 int starsh_blrm__drsdd_b200_mp(STARSH_blrm **matrix, STARSH_blrf *format,
         int maxrank, double tol, int onfly);
 

@@ -38,10 +38,10 @@ enum STARSH_LRENGINE
     /* On the B200 backend: randomized SVD with every step in FP64. */
     STARSH_LRENGINE_RSVD = 3,
     STARSH_LRENGINE_CROSS = 4,
-    /* On the B200 backend: randomized SVD whose sketch runs on the tensor
-     * cores in split BF16 (three BF16 products per FP64 pair, FP32
-     * accumulation); orthogonalisation, projection, small SVD and the
-     * tolerance test stay FP64. */
+    /* On the B200 backend: randomized SVD with an adaptive sketch width
+     * (Gaussian columns in blocks until a posterior residual estimate
+     * falls below tol); projection, small SVD and the tolerance test are
+     * FP64 as in RSVD. */
     STARSH_LRENGINE_RSVD_MP = 5,
 };
 

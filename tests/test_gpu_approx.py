@@ -145,10 +145,11 @@ def test_mixed_engine_matches_reference(ref, lib, case):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("engine", [sb.ENGINE_FP64, sb.ENGINE_MIXED])
-def test_high_rank_tiles_cluster_jacobi(ref, lib, engine):
+def test_high_rank_tiles_large_jacobi_classes(ref, lib, engine):
     # 512-point 3-D Coulomb tiles with maxrank 200: the diagonal and
     # neighbouring blocks keep k1 ~ 200 basis columns, whose small SVD runs
-    # on a 4-CTA cluster through distributed shared memory
+    # in the large Jacobi classes (shared memory up to 220 KB, then global
+    # memory), the far blocks in the small ones
     err, err_ref, c, cref, st = _compare(ref, lib, "coulomb", 2048, 512, 200,
                                          1e-5, ndim=3, place=1, engine=engine)
     assert err <= 1e-5

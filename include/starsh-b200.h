@@ -83,6 +83,17 @@ enum STARSH_B200_FLAGS
 int starsh_b200_approximate(STARSH_blrm **matrix, STARSH_blrf *format,
         int maxrank, double tol, int onfly, int engine, int flags);
 
+/* Approximates nprob independent problems in shared batches: the tiles of
+ * all problems (any kernels, tile sizes, maxrank and tol) go through the
+ * same launches, so many small problems fill the GPU like one large one.
+ * matrices[p] receives the approximation of formats[p] under maxrank[p],
+ * tol[p] and onfly[p] (onfly may be NULL: all 0); each result equals what
+ * starsh_b200_approximate() returns for that problem alone.  The formats
+ * must be distinct.  On error no matrix is returned. */
+int starsh_b200_approximate_batch(int nprob, STARSH_blrm **matrices,
+        STARSH_blrf **formats, const int *maxrank, const double *tol,
+        const int *onfly, int engine, int flags);
+
 /* Fills the host mirror of a device-resident matrix (no-op if present). */
 int starsh_b200_blrm_download(STARSH_blrm *matrix);
 
@@ -147,6 +158,64 @@ int starsh_b200_kernel_family(STARSH_kernel *kernel, int *ndim_hint);
 int starsh_b200_dense_rsvd_noalloc(const double *dD, int nrows, int ncols,
         int ldd, int maxrank, int oversample, double tol, double *dU,
         double *dV, int *d_rank, void *stream);
+
+/* ------------------------------------------------------------ serving */
+
+/* A serving loop: approximation requests are admitted by an HBM budget and
+ * run in shared batches (continuous batching: requests that arrive while a
+ * group is on the GPU join the next group as memory allows), then each
+ * request's TLR-by-dense product runs on the resident factors.  All calls
+ * are thread-safe; one worker thread per server drives the GPU. */
+typedef struct starsh_b200_server starsh_b200_server;
+
+typedef struct starsh_b200_server_stats
+{
+    long long submitted, completed, failed;
+    long long groups;             /* batched approximation calls           */
+    long long entries;            /* sum of m*n over approximated blocks   */
+    double busy_ms;               /* worker time inside groups             */
+    double resident_bytes;        /* results kept and not yet released     */
+    double peak_resident_bytes;
+} starsh_b200_server_stats;
+
+/* hbm_budget_bytes bounds the device memory of admitted and kept results
+ * (admission uses an upper bound: factors at maxrank, dense near blocks);
+ * engine is STARSH_B200_FP64 or STARSH_B200_MIXED; max_group caps the
+ * requests of one group (<= 0: no cap). */
+int starsh_b200_server_new(starsh_b200_server **server,
+        double hbm_budget_bytes, int engine, int max_group);
+
+/* Queues the approximation of `format` (updated in place on demotion, as
+ * by starsh_blrm_approximate) followed, if nrhs > 0, by B = M A with host
+ * A (N x nrhs, lda) and B (N x nrhs, ldb).  format, A and B must stay valid
+ * until the request completes.  With keep = 0 the matrix is freed after
+ * the product; with keep = 1 it stays resident (counted in the budget)
+ * until starsh_b200_server_release().  *ticket identifies the request. */
+int starsh_b200_server_submit(starsh_b200_server *server,
+        STARSH_blrf *format, int maxrank, double tol, int nrhs,
+        const double *A, int lda, double *B, int ldb, int keep,
+        long long *ticket);
+
+/* Blocks until the request completes; returns its status
+ * (STARSH_MALLOC_ERROR if it can never fit the budget), the kept matrix
+ * (device-resident, NULL if keep = 0) and the latency from submit to
+ * completion in milliseconds.  Each ticket is waited for once. */
+int starsh_b200_server_wait(starsh_b200_server *server, long long ticket,
+        STARSH_blrm **matrix, double *latency_ms);
+
+/* Frees a kept matrix and returns its memory to the budget. */
+int starsh_b200_server_release(starsh_b200_server *server,
+        STARSH_blrm *matrix);
+
+/* paused = 1 holds admission (queued requests wait, running groups
+ * finish); paused = 0 resumes. */
+int starsh_b200_server_pause(starsh_b200_server *server, int paused);
+
+int starsh_b200_server_get_stats(starsh_b200_server *server,
+        starsh_b200_server_stats *stats);
+
+/* Finishes the queued requests and stops the worker. */
+int starsh_b200_server_free(starsh_b200_server *server);
 
 /* ------------------------------------------------------------ device */
 

@@ -28,8 +28,8 @@ struct Context {
     DeviceBuffer flag;         // round flag of the adaptive sketch
     void *stage[2] = {nullptr, nullptr};     // pinned D2H staging buffers
     cudaEvent_t stage_ev[2] = {nullptr, nullptr};
-    size_t omega_count = 0;
-    unsigned long long omega_seed = 0;
+    DeviceBuffer kernels;      // DevKernel table of a batch's problems
+    int omega_rows = 0, omega_cols = 0;   // shape Omega was generated for
     std::mutex lock;           // one approximation / dmml at a time
 };
 

@@ -85,7 +85,12 @@ Context *context()
         }
         g_ctx_ok = true;
     });
-    return g_ctx_ok ? &g_ctx : nullptr;
+    if (!g_ctx_ok) return nullptr;
+    // every host thread that calls in works on the library's device
+    int cur = -1;
+    if (cudaGetDevice(&cur) != cudaSuccess || cur != g_ctx.device)
+        cudaSetDevice(g_ctx.device);
+    return &g_ctx;
 }
 
 void set_error(const std::string &msg)
@@ -227,8 +232,6 @@ Record *find_record(const STARSH_blrm *M)
 static const unsigned long long kOmegaSeed = 0x5354415253480001ull;
 
 struct EngineParams {
-    int maxrank;
-    double tol;
     int oversample;
     int engine;
     int block;      // adaptive sketch: columns of the first round
@@ -236,52 +239,86 @@ struct EngineParams {
     int verify;     // unselected sample columns that finish a tile
 };
 
-// Runs the device pipeline over all far blocks of F.  Fills ranks (host)
-// and per-block device pointers of U and V inside `rec`.
-static int compress_far(Context &ctx, const DevKernel &K, STARSH_blrf *F,
-                        const EngineParams &ep, std::vector<int> &rank,
-                        Record &rec)
+// One problem of a batched approximation call.
+struct ProblemJob {
+    STARSH_blrf *F;
+    int maxrank;
+    double tol;
+    int onfly;
+    Record *rec;              // owns the problem's points and factors
+    std::vector<int> rank;    // per far block of F (filled by compress)
+};
+
+// Runs the device pipeline over the far blocks of every problem of `jobs`
+// in shared batches: tiles of different problems (kernels, sizes, tol,
+// maxrank) share every launch.  Fills each job's ranks and the per-block
+// device pointers of U and V in its record.  A tile's result does not
+// depend on the other tiles of its batch: every kernel works per tile, and
+// Omega(j, c) depends on (j, c) only.
+static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
+                          const EngineParams &ep)
 {
     cudaStream_t s = ctx.stream;
-    STARSH_cluster *R = F->row_cluster, *C = F->col_cluster;
-    const STARSH_int nfar = F->nblocks_far;
-    rank.assign(nfar, 0);
-    rec.dU.assign(nfar, nullptr);
-    rec.dV.assign(nfar, nullptr);
-    if (nfar == 0) return STARSH_SUCCESS;
     starsh_b200_stats &st = thread_stats();
-
-    std::vector<TileWork> all(nfar);
+    std::vector<TileWork> all;
+    std::vector<std::pair<int, STARSH_int>> owner;   // (job, far block)
     int m_max = 0, n_max = 0, k_max = 0;
-    for (STARSH_int b = 0; b < nfar; ++b) {
-        const STARSH_int i = F->block_far[2 * b], j = F->block_far[2 * b + 1];
-        TileWork &t = all[b];
-        memset(&t, 0, sizeof(t));
-        t.row0 = R->start[i];
-        t.col0 = C->start[j];
-        t.m = (int)R->size[i];
-        t.n = (int)C->size[j];
-        t.k = std::min(ep.maxrank + ep.oversample, std::min(t.m, t.n));
-        m_max = std::max(m_max, t.m);
-        n_max = std::max(n_max, t.n);
-        k_max = std::max(k_max, t.k);
-        st.entries += (long long)t.m * t.n;
+    bool may_repeat = false;
+    std::vector<DevKernel> kernels;
+    for (size_t p = 0; p < jobs.size(); ++p) {
+        ProblemJob &jb = jobs[p];
+        STARSH_blrf *F = jb.F;
+        STARSH_cluster *R = F->row_cluster, *C = F->col_cluster;
+        const STARSH_int nfar = F->nblocks_far;
+        jb.rank.assign(nfar, 0);
+        jb.rec->dU.assign(nfar, nullptr);
+        jb.rec->dV.assign(nfar, nullptr);
+        kernels.push_back(jb.rec->points->K);
+        // a repeat pass can only be needed when (tol/10)^2 lies below the
+        // squared-noise floor of a Gram
+        if (nfar > 0 && 0.01 * jb.tol * jb.tol < 1e-15) may_repeat = true;
+        for (STARSH_int b = 0; b < nfar; ++b) {
+            const STARSH_int i = F->block_far[2 * b], j = F->block_far[2 * b + 1];
+            TileWork t;
+            memset(&t, 0, sizeof(t));
+            t.row0 = R->start[i];
+            t.col0 = C->start[j];
+            t.m = (int)R->size[i];
+            t.n = (int)C->size[j];
+            t.k = std::min(jb.maxrank + ep.oversample, std::min(t.m, t.n));
+            t.prob = (int)p;
+            t.maxrank = jb.maxrank;
+            t.tol = jb.tol;
+            m_max = std::max(m_max, t.m);
+            n_max = std::max(n_max, t.n);
+            k_max = std::max(k_max, t.k);
+            st.entries += (long long)t.m * t.n;
+            all.push_back(t);
+            owner.emplace_back((int)p, b);
+        }
     }
+    const long long ntot = (long long)all.size();
+    if (ntot == 0) return STARSH_SUCCESS;
     if (k_max > 1024) {
         set_error("maxrank + oversample above 1024 is not supported");
         return STARSH_WRONG_PARAMETER;
     }
+    if (!ctx.kernels.reserve(kernels.size() * sizeof(DevKernel)))
+        return cuda_fail(cudaErrorMemoryAllocation, "kernel table");
+    B200_CUDA(cudaMemcpyAsync(ctx.kernels.ptr, kernels.data(),
+                              kernels.size() * sizeof(DevKernel),
+                              cudaMemcpyHostToDevice, s), "kernel table");
+    const DevKernel *d_kernels = (const DevKernel *)ctx.kernels.ptr;
     // Gaussian sketch, shared by every tile (as the reference reuses the
     // same iseed for every block): n_max x k_max, ld n_max.
-    const size_t om_count = (size_t)n_max * k_max;
-    if (ctx.omega_count != om_count || ctx.omega_seed != kOmegaSeed) {
-        if (!ctx.omega.reserve(om_count * sizeof(double)))
+    if (ctx.omega_rows != n_max || ctx.omega_cols != k_max) {
+        if (!ctx.omega.reserve((size_t)n_max * k_max * sizeof(double)))
             return cuda_fail(cudaErrorMemoryAllocation, "omega");
-        launch_gaussian((double *)ctx.omega.ptr, (long long)om_count,
+        launch_gaussian((double *)ctx.omega.ptr, n_max, k_max, n_max,
                         kOmegaSeed, s);
         count_launch();
-        ctx.omega_count = om_count;
-        ctx.omega_seed = kOmegaSeed;
+        ctx.omega_rows = n_max;
+        ctx.omega_cols = k_max;
     }
     const double *omega = (const double *)ctx.omega.ptr;
 
@@ -293,7 +330,7 @@ static int compress_far(Context &ctx, const DevKernel &K, STARSH_blrf *F,
     if (const char *e = getenv("STARSH_B200_WORKSPACE_MB"))
         budget = std::min<size_t>(budget, (size_t)atoll(e) << 20);
     long long slots = (long long)(budget / (stride * sizeof(double)));
-    slots = std::max<long long>(1, std::min<long long>(slots, nfar));
+    slots = std::max<long long>(1, std::min<long long>(slots, ntot));
     slots = std::min<long long>(slots, 4096);
     if (!ctx.workspace.reserve((size_t)slots * stride * sizeof(double)))
         return cuda_fail(cudaErrorMemoryAllocation, "workspace");
@@ -328,13 +365,13 @@ static int compress_far(Context &ctx, const DevKernel &K, STARSH_blrf *F,
                    : cuda_fail(cudaGetLastError(), "gemm_f64_batched");
     };
 
-    for (STARSH_int b0 = 0; b0 < nfar && info == STARSH_SUCCESS; b0 += slots) {
-        const int nt = (int)std::min<STARSH_int>(slots, nfar - b0);
+    for (long long b0 = 0; b0 < ntot && info == STARSH_SUCCESS; b0 += slots) {
+        const int nt = (int)std::min<long long>(slots, ntot - b0);
         for (int t = 0; t < nt; ++t) all[b0 + t].slot = t;
         cudaMemcpyAsync(dt, &all[b0], nt * sizeof(TileWork),
                         cudaMemcpyHostToDevice, s);
         cudaEventRecord(ev[4], s);
-        launch_gen_tiles(K, dt, nt, ws, s);
+        launch_gen_tiles(d_kernels, dt, nt, ws, s);
         count_launch();
         cudaEventRecord(ev[5], s);
         if (ep.engine == STARSH_B200_FP64) {
@@ -343,7 +380,7 @@ static int compress_far(Context &ctx, const DevKernel &K, STARSH_blrf *F,
         cudaEventRecord(ev[1], s);
         // basis: pass A
         if ((info = gemm(STEP_GRAM_Y, true, false, nt, k_max, k_max, none))) break;
-        launch_pivchol(0, dt, dt, nt, ws, ep.tol, s);
+        launch_pivchol(0, dt, dt, nt, ws, s);
         launch_gather_cols(0, dt, nt, ws, s);
         count_launch(2);
         if ((info = gemm(STEP_Q1, false, false, nt, m_max, k_max, none))) break;
@@ -355,7 +392,7 @@ static int compress_far(Context &ctx, const DevKernel &K, STARSH_blrf *F,
         if ((info = gemm(STEP_RES_Z, true, false, nt, k_max, k_max, none))) break;
         if ((info = gemm(STEP_RES_Y, false, false, nt, m_max, k_max, none))) break;
         if ((info = gemm(STEP_GRAM_YR, true, false, nt, k_max, k_max, none))) break;
-        launch_pivchol(1, dt, dt, nt, ws, ep.tol, s);
+        launch_pivchol(1, dt, dt, nt, ws, s);
         launch_gather_cols(1, dt, nt, ws, s);
         count_launch(2);
         if ((info = gemm(STEP_Q1B, false, false, nt, m_max, k_max, none))) break;
@@ -382,9 +419,6 @@ static int compress_far(Context &ctx, const DevKernel &K, STARSH_blrf *F,
         launch_block_norms(dt, dt, nt, ws, s);
         count_launch();
         int *d_active = (int *)ctx.flag.ptr;
-        // a repeat pass can only be needed when (tol/10)^2 lies below the
-        // squared-noise floor of a Gram
-        const bool may_repeat = 0.01 * ep.tol * ep.tol < 1e-15;
         auto append = [&](int bmax) -> int {
             // orthonormalise the selected residual columns (kb of them)
             // against the basis and append them: CholQR of R_J, one more
@@ -421,7 +455,7 @@ static int compress_far(Context &ctx, const DevKernel &K, STARSH_blrf *F,
                 if ((info = gemm(STEP_A_RES_Y, false, false, nt, m_max, bmax, none))) break;
             }
             if ((info = gemm(STEP_A_GRAM, true, false, nt, bmax, bmax, none))) break;
-            launch_round_pivchol(dt, nt, ws, ep.tol, 0, s);
+            launch_round_pivchol(dt, nt, ws, 0, s);
             count_launch();
             if ((info = append(bmax))) break;
             if (may_repeat) {
@@ -429,7 +463,7 @@ static int compress_far(Context &ctx, const DevKernel &K, STARSH_blrf *F,
                 if ((info = gemm(STEP_A_RES_Z2, true, false, nt, k_max, bmax, none))) break;
                 if ((info = gemm(STEP_A_RES_Y2, false, false, nt, m_max, bmax, none))) break;
                 if ((info = gemm(STEP_A_GRAM2, true, false, nt, bmax, bmax, none))) break;
-                launch_round_pivchol(dt, nt, ws, ep.tol, 1, s);
+                launch_round_pivchol(dt, nt, ws, 1, s);
                 count_launch();
                 if ((info = append(bmax))) break;
             }
@@ -448,11 +482,11 @@ static int compress_far(Context &ctx, const DevKernel &K, STARSH_blrf *F,
         if ((info = gemm(STEP_PROJECT, true, false, nt, k_max, n_max, none))) break;
         cudaEventRecord(ev[3], s);
         if ((info = gemm(STEP_GRAM_B, false, true, nt, k_max, k_max, none))) break;
-        launch_pivchol(2, dt, dt, nt, ws, ep.tol, s);
-        launch_jacobi(dt, nt, ws, ep.tol, s, ctx.side);
+        launch_pivchol(2, dt, dt, nt, ws, s);
+        launch_jacobi(dt, nt, ws, s, ctx.side);
         count_launch(2);
         if ((info = gemm(STEP_ROTATE, true, false, nt, k_max, n_max, none))) break;
-        launch_rank_cut(dt, nt, ws, ep.tol, ep.maxrank, s);
+        launch_rank_cut(dt, nt, ws, s);
         count_launch();
         cudaEventRecord(ev[6], s);
         B200_CUDA(cudaMemcpyAsync(&all[b0], dt, nt * sizeof(TileWork),
@@ -465,8 +499,11 @@ static int compress_far(Context &ctx, const DevKernel &K, STARSH_blrf *F,
         st.svd_ms += phase_ms(3, 6);
         if (output_pending) st.output_ms += phase_ms(7, 8);
         output_pending = false;
-        // Output placement of this batch: one device chunk for U and V.
-        size_t nu = 0, nv = 0;
+        // Output placement of this batch: one device chunk, the U then V
+        // factors of each problem contiguous (so every problem's host
+        // mirror is a concatenation of its parts), shared by the records
+        // of the problems with tiles here.
+        std::vector<size_t> nu(jobs.size(), 0), nv(jobs.size(), 0);
         for (int t = 0; t < nt; ++t) {
             TileWork &w = all[b0 + t];
             st.sketch_flops += 2.0 * w.m * w.n *
@@ -476,33 +513,50 @@ static int compress_far(Context &ctx, const DevKernel &K, STARSH_blrf *F,
                 set_error("re-orthogonalisation failed on a tile");
                 info = STARSH_UNKNOWN_ERROR;
             }
-            rank[b0 + t] = w.rank;
+            jobs[w.prob].rank[owner[b0 + t].second] = w.rank;
             if (w.rank > 0) {
-                w.off_u = (long long)nu;
-                w.off_v = (long long)nv;
-                nu += (size_t)w.m * w.rank;
-                nv += (size_t)w.n * w.rank;
+                nu[w.prob] += (size_t)w.m * w.rank;
+                nv[w.prob] += (size_t)w.n * w.rank;
             }
         }
         if (info) break;
-        double *chunk = nullptr;
-        if (nu + nv > 0) {
-            B200_CUDA(cudaMalloc(&chunk, (nu + nv) * sizeof(double)),
+        std::vector<size_t> u0(jobs.size()), v0(jobs.size());
+        size_t total = 0;
+        for (size_t p = 0; p < jobs.size(); ++p) {
+            u0[p] = total;
+            v0[p] = total + nu[p];
+            total += nu[p] + nv[p];
+        }
+        std::shared_ptr<void> chunk;
+        if (total > 0) {
+            void *raw = nullptr;
+            B200_CUDA(cudaMalloc(&raw, total * sizeof(double)),
                       "cudaMalloc(factors)");
-            rec.chunks.push_back(chunk);
+            chunk = std::shared_ptr<void>(raw, [](void *q) { cudaFree(q); });
         }
-        OutArena out{chunk, chunk ? chunk + nu : nullptr};
-        if (chunk) rec.parts.push_back({out.U, nu, out.V, nv});
+        double *base = (double *)chunk.get();
+        std::vector<size_t> cu(u0), cv(v0);
         for (int t = 0; t < nt; ++t) {
-            const TileWork &w = all[b0 + t];
-            if (w.rank > 0) {
-                rec.dU[b0 + t] = out.U + w.off_u;
-                rec.dV[b0 + t] = out.V + w.off_v;
-            }
+            TileWork &w = all[b0 + t];
+            if (w.rank <= 0) continue;
+            w.off_u = (long long)cu[w.prob];
+            w.off_v = (long long)cv[w.prob];
+            cu[w.prob] += (size_t)w.m * w.rank;
+            cv[w.prob] += (size_t)w.n * w.rank;
+            Record *rec = jobs[w.prob].rec;
+            rec->dU[owner[b0 + t].second] = base + w.off_u;
+            rec->dV[owner[b0 + t].second] = base + w.off_v;
         }
-        rec.u_total += nu;
-        rec.v_total += nv;
-        if (nu + nv > 0) {
+        for (size_t p = 0; p < jobs.size(); ++p) {
+            if (nu[p] + nv[p] == 0) continue;
+            Record *rec = jobs[p].rec;
+            rec->shared.push_back(chunk);
+            rec->parts.push_back({base + u0[p], nu[p], base + v0[p], nv[p]});
+            rec->u_total += nu[p];
+            rec->v_total += nv[p];
+        }
+        if (total > 0) {
+            OutArena out{base, base};
             cudaMemcpyAsync(dt, &all[b0], nt * sizeof(TileWork),
                             cudaMemcpyHostToDevice, s);
             cudaEventRecord(ev[7], s);
@@ -535,6 +589,16 @@ static int compress_far(Context &ctx, const DevKernel &K, STARSH_blrf *F,
     }
     for (auto &e : ev) cudaEventDestroy(e);
     return info;
+}
+
+// Device bytes held by a matrix of this library: factors, dense near-field
+// blocks and the problem's points (0 if M has no device record).
+size_t matrix_device_bytes(const STARSH_blrm *M)
+{
+    Record *rec = find_record(M);
+    if (rec == nullptr) return 0;
+    return (rec->u_total + rec->v_total + rec->d_total) * sizeof(double) +
+           (rec->points ? rec->points->h2d : 0);
 }
 
 // Host Array view helper (shape m x n, column-major).
@@ -672,67 +736,28 @@ static int fill_host_mirror(STARSH_blrm *M, Record &rec, cudaStream_t s)
     return STARSH_SUCCESS;
 }
 
-static int approximate(STARSH_blrm **matrix, STARSH_blrf *F, int maxrank,
-                       double tol, int onfly, int engine, int flags)
+// Turns the compressed far blocks of one problem into its STARSH_blrm:
+// demotes false far-field blocks, generates the near-field blocks and builds
+// the host structure (with its host mirror if requested).  On success the
+// job's record belongs to the record table.
+static int finish_problem(ProblemJob &jb, int flags, cudaStream_t s,
+                          STARSH_blrm **matrix)
 {
-    auto t_start = std::chrono::steady_clock::now();
     starsh_b200_stats &st = thread_stats();
-    memset(&st, 0, sizeof(st));
-    const long long launches0 = launch_count();
-    if (matrix == nullptr || F == nullptr || maxrank < 0 || !(tol >= 0.0) ||
-        (onfly != 0 && onfly != 1)) {
-        set_error("invalid argument");
-        return STARSH_WRONG_PARAMETER;
-    }
-    if (engine != STARSH_B200_FP64 && engine != STARSH_B200_MIXED) {
-        set_error("unknown engine");
-        return STARSH_WRONG_PARAMETER;
-    }
-    Context *ctx = context();
-    if (!ctx) return STARSH_UNKNOWN_ERROR;
-    std::lock_guard<std::mutex> guard(ctx->lock);
-    cudaSetDevice(ctx->device);
-    cudaStream_t s = ctx->stream;
+    STARSH_blrf *F = jb.F;
     STARSH_problem *P = F->problem;
     STARSH_cluster *R = F->row_cluster, *C = F->col_cluster;
-    if (P == nullptr || R == nullptr || C == nullptr || P->ndim != 2 ||
-        P->dtype != 'd') {
-        set_error("only scalar double-precision problems are supported");
-        return STARSH_WRONG_PARAMETER;
-    }
-
-    auto *points = new DevicePoints();
-    int info = upload_problem(*points, P, R, C, s);
-    if (info) {
-        delete points;
-        return info;
-    }
-    st.h2d_bytes += points->h2d;
-    auto *rec = new Record();
-    rec->points = points;
-    std::vector<int> rank;
-    int block = 64, block_next = 32, verify = 10;
-    if (const char *e = getenv("STARSH_B200_SKETCH_BLOCK"))
-        block = std::max(8, std::min(1024, atoi(e)));
-    if (const char *e = getenv("STARSH_B200_SKETCH_STEP"))
-        block_next = std::max(8, std::min(1024, atoi(e)));
-    if (const char *e = getenv("STARSH_B200_SKETCH_VERIFY"))
-        verify = std::max(1, std::min(1024, atoi(e)));
-    EngineParams ep{maxrank, tol, b200_oversample(), engine, block,
-                    block_next, verify};
-    info = compress_far(*ctx, points->K, F, ep, rank, *rec);
-    if (info) {
-        delete rec;
-        return info;
-    }
-
+    Record *rec = jb.rec;
+    const std::vector<int> &rank = jb.rank;
+    const int onfly = jb.onfly;
+    int info = STARSH_SUCCESS;
     // False far-field blocks (rank -1) become near-field; the format is
     // rebuilt and swapped into *F, the old lists freed.
     const STARSH_int nfar = F->nblocks_far, nnear = F->nblocks_near;
     std::vector<STARSH_int> keep, demote;
     for (STARSH_int b = 0; b < nfar; ++b)
         (rank[b] < 0 ? demote : keep).push_back(b);
-    st.false_far = (long long)demote.size();
+    st.false_far += (long long)demote.size();
     std::vector<double *> dU, dV;
     std::vector<int> far_rank;
     for (STARSH_int b : keep) {
@@ -751,7 +776,6 @@ static int approximate(STARSH_blrm **matrix, STARSH_blrf *F, int maxrank,
         if (!bn || (new_far > 0 && !bf)) {
             free(bn);
             free(bf);
-            delete rec;
             return STARSH_MALLOC_ERROR;
         }
         for (STARSH_int b = 0; b < 2 * nnear; ++b) bn[b] = F->block_near[b];
@@ -769,7 +793,6 @@ static int approximate(STARSH_blrm **matrix, STARSH_blrf *F, int maxrank,
         if (info) {
             free(bn);
             free(bf);
-            delete rec;
             return info;
         }
         STARSH_blrf tmp = *F;
@@ -791,7 +814,6 @@ static int approximate(STARSH_blrm **matrix, STARSH_blrf *F, int maxrank,
         double *dD = nullptr;
         cudaError_t e = cudaMalloc(&dD, total * sizeof(double));
         if (e != cudaSuccess) {
-            delete rec;
             return cuda_fail(e, "cudaMalloc(near blocks)");
         }
         rec->chunks.push_back(dD);
@@ -800,15 +822,14 @@ static int approximate(STARSH_blrm **matrix, STARSH_blrf *F, int maxrank,
         size_t off = 0;
         for (STARSH_int b = 0; b < near; ++b) {
             const STARSH_int i = F->block_near[2 * b], j = F->block_near[2 * b + 1];
-            BlockJob jb{R->start[i], C->start[j], (int)R->size[i],
+            BlockJob bj{R->start[i], C->start[j], (int)R->size[i],
                         (int)C->size[j], dD + off};
             rec->dD[b] = dD + off;
-            jobs.push_back(jb);
-            off += (size_t)jb.m * jb.n;
-            st.entries += (long long)jb.m * jb.n;
+            jobs.push_back(bj);
+            off += (size_t)bj.m * bj.n;
+            st.entries += (long long)bj.m * bj.n;
         }
-        if ((info = gen_blocks(points->K, jobs, s))) {
-            delete rec;
+        if ((info = gen_blocks(rec->points->K, jobs, s))) {
             return info;
         }
     } else {
@@ -839,23 +860,140 @@ static int approximate(STARSH_blrm **matrix, STARSH_blrf *F, int maxrank,
     STARSH_blrm *M = nullptr;
     info = starsh_blrm_new(&M, F, fr, fU, fV, onfly, nD, nullptr, nullptr,
                            nullptr, '1');
-    if (info) {
-        delete rec;
-        return info;
-    }
+    if (info) return info;
     add_record(M, rec);
+    jb.rec = nullptr;   // owned by the record table now
     if (flags & STARSH_B200_HOST_MIRROR) {
         info = fill_host_mirror(M, *rec, s);
-        if (info) return info;
     } else {
-        B200_CUDA(cudaStreamSynchronize(s), "near blocks");
+        const cudaError_t e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) info = cuda_fail(e, "near blocks");
+    }
+    if (info) {
+        starsh_blrm_free(M);   // releases the record as well
+        return info;
     }
     *matrix = M;
+    return STARSH_SUCCESS;
+}
+
+static void read_engine_env(EngineParams &ep)
+{
+    ep.block = 64;
+    ep.block_next = 32;
+    ep.verify = 10;
+    if (const char *e = getenv("STARSH_B200_SKETCH_BLOCK"))
+        ep.block = std::max(8, std::min(1024, atoi(e)));
+    if (const char *e = getenv("STARSH_B200_SKETCH_STEP"))
+        ep.block_next = std::max(8, std::min(1024, atoi(e)));
+    if (const char *e = getenv("STARSH_B200_SKETCH_VERIFY"))
+        ep.verify = std::max(1, std::min(1024, atoi(e)));
+}
+
+// Approximates `np` problems in shared batches (every launch carries tiles
+// of all of them).  matrices[p] receives the result of formats[p]; each
+// format is updated in place on demotion as by the single-problem call.
+static int approximate_batch(int np, STARSH_blrm **matrices,
+                             STARSH_blrf **formats, const int *maxranks,
+                             const double *tols, const int *onflys,
+                             int engine, int flags)
+{
+    auto t_start = std::chrono::steady_clock::now();
+    starsh_b200_stats &st = thread_stats();
+    memset(&st, 0, sizeof(st));
+    const long long launches0 = launch_count();
+    if (np <= 0 || matrices == nullptr || formats == nullptr ||
+        maxranks == nullptr || tols == nullptr) {
+        set_error("invalid argument");
+        return STARSH_WRONG_PARAMETER;
+    }
+    for (int p = 0; p < np; ++p) {
+        const int onfly = onflys ? onflys[p] : 0;
+        if (formats[p] == nullptr ||
+            maxranks[p] < 0 || !(tols[p] >= 0.0) ||
+            (onfly != 0 && onfly != 1)) {
+            set_error("invalid argument");
+            return STARSH_WRONG_PARAMETER;
+        }
+        for (int q = 0; q < p; ++q)
+            if (formats[q] == formats[p]) {
+                set_error("the same format appears twice in one batch");
+                return STARSH_WRONG_PARAMETER;
+            }
+        STARSH_blrf *F = formats[p];
+        STARSH_problem *P = F->problem;
+        if (P == nullptr || F->row_cluster == nullptr ||
+            F->col_cluster == nullptr || P->ndim != 2 || P->dtype != 'd') {
+            set_error("only scalar double-precision problems are supported");
+            return STARSH_WRONG_PARAMETER;
+        }
+    }
+    if (engine != STARSH_B200_FP64 && engine != STARSH_B200_MIXED) {
+        set_error("unknown engine");
+        return STARSH_WRONG_PARAMETER;
+    }
+    Context *ctx = context();
+    if (!ctx) return STARSH_UNKNOWN_ERROR;
+    std::lock_guard<std::mutex> guard(ctx->lock);
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+
+    std::vector<ProblemJob> jobs(np);
+    auto cleanup = [&]() {
+        for (ProblemJob &jb : jobs) {
+            delete jb.rec;
+            jb.rec = nullptr;
+        }
+    };
+    for (int p = 0; p < np; ++p) {
+        ProblemJob &jb = jobs[p];
+        jb.F = formats[p];
+        jb.maxrank = maxranks[p];
+        jb.tol = tols[p];
+        jb.onfly = onflys ? onflys[p] : 0;
+        jb.rec = new Record();
+        jb.rec->points = new DevicePoints();
+        int info = upload_problem(*jb.rec->points, jb.F->problem,
+                                  jb.F->row_cluster, jb.F->col_cluster, s);
+        if (info) {
+            cleanup();
+            return info;
+        }
+        st.h2d_bytes += jb.rec->points->h2d;
+    }
+    EngineParams ep{};
+    ep.oversample = b200_oversample();
+    ep.engine = engine;
+    read_engine_env(ep);
+    int info = compress_multi(*ctx, jobs, ep);
+    int done = 0;
+    for (; done < np && info == STARSH_SUCCESS; ++done)
+        info = finish_problem(jobs[done], flags, s, &matrices[done]);
+    if (info) {
+        // the problems finished before the failure are released too
+        for (int q = 0; q + 1 < done; ++q) {
+            starsh_blrm_free(matrices[q]);
+            matrices[q] = nullptr;
+        }
+        cleanup();
+        return info;
+    }
     st.kernel_launches = launch_count() - launches0;
     st.device_ms = st.sketch_ms + st.project_ms;
     st.total_ms = std::chrono::duration<double, std::milli>(
                       std::chrono::steady_clock::now() - t_start).count();
     return STARSH_SUCCESS;
+}
+
+static int approximate(STARSH_blrm **matrix, STARSH_blrf *F, int maxrank,
+                       double tol, int onfly, int engine, int flags)
+{
+    if (matrix == nullptr || F == nullptr) {
+        set_error("invalid argument");
+        return STARSH_WRONG_PARAMETER;
+    }
+    return approximate_batch(1, matrix, &F, &maxrank, &tol, &onfly, engine,
+                             flags);
 }
 
 }  // namespace b200
@@ -870,6 +1008,17 @@ extern "C" int starsh_b200_approximate(STARSH_blrm **matrix,
                                        int flags)
 {
     return approximate(matrix, format, maxrank, tol, onfly, engine, flags);
+}
+
+extern "C" int starsh_b200_approximate_batch(int nprob, STARSH_blrm **matrices,
+                                             STARSH_blrf **formats,
+                                             const int *maxrank,
+                                             const double *tol,
+                                             const int *onfly, int engine,
+                                             int flags)
+{
+    return approximate_batch(nprob, matrices, formats, maxrank, tol, onfly,
+                             engine, flags);
 }
 
 extern "C" int starsh_blrm__drsdd_b200(STARSH_blrm **matrix,

@@ -37,6 +37,9 @@ struct TileWork {
     int kround;             // directions the current round's sample added
     int k1_round;           // basis columns when the current round began
     int sweeps;             // Jacobi sweeps the small SVD took
+    int prob;               // problem of the batch the tile belongs to
+    int maxrank;            // the problem's maxrank and tol
+    double tol;
     long long off_u, off_v; // output offsets (doubles)
 };
 
@@ -119,18 +122,20 @@ void make_gemm_descs(GemmStep step, const TileWork *d_tiles, int ntiles,
                      OutArena out, GemmDesc *d_desc, cudaStream_t stream);
 
 // Per-tile kernels (one CTA per tile).
-void launch_gen_tiles(const DevKernel &K, const TileWork *d_tiles,
+// Thresholds come from each tile's tol and maxrank; the generator reads
+// the tile's kernel from d_kernels[tile.prob].
+void launch_gen_tiles(const DevKernel *d_kernels, const TileWork *d_tiles,
                       int ntiles, Workspace ws, cudaStream_t stream);
 void launch_pivchol(int phase, const TileWork *d_tiles, TileWork *d_tiles_rw,
-                    int ntiles, Workspace ws, double tol, cudaStream_t s);
+                    int ntiles, Workspace ws, cudaStream_t s);
 void launch_gather_cols(int phase, const TileWork *d_tiles, int ntiles,
                         Workspace ws, cudaStream_t stream);
 void launch_chol_inv(int phase, TileWork *d_tiles, int ntiles, Workspace ws,
                      cudaStream_t stream);
-void launch_jacobi(TileWork *d_tiles, int ntiles, Workspace ws, double tol,
+void launch_jacobi(TileWork *d_tiles, int ntiles, Workspace ws,
                    cudaStream_t stream, cudaStream_t side);
 void launch_rank_cut(TileWork *d_tiles, int ntiles, Workspace ws,
-                     double tol, int maxrank, cudaStream_t stream);
+                     cudaStream_t stream);
 void launch_merge_basis(TileWork *d_tiles, int ntiles, cudaStream_t stream);
 // Adaptive sketch: squared Frobenius norms of the generated blocks, round
 // set-up (returns through d_active whether any tile still samples) and the
@@ -142,12 +147,15 @@ void launch_round_setup(TileWork *d_tiles, int ntiles, int block,
 void launch_round_end(TileWork *d_tiles, int ntiles, int verify,
                       cudaStream_t stream);
 void launch_round_pivchol(TileWork *d_tiles, int ntiles, Workspace ws,
-                          double tol, int repeat, cudaStream_t stream);
+                          int repeat, cudaStream_t stream);
 void launch_select_w(const TileWork *d_tiles, int ntiles, Workspace ws,
                      cudaStream_t stream);
 void launch_write_v(const TileWork *d_tiles, int ntiles, Workspace ws,
                     OutArena out, cudaStream_t stream);
-void launch_gaussian(double *d_omega, long long count, unsigned long long seed,
-                     cudaStream_t stream);
+// Omega(j, c) for j < rows, c < cols into column-major storage with leading
+// dimension ld; entry (j, c) depends only on (j, c) and the seed, not on
+// the storage shape.
+void launch_gaussian(double *d_omega, int rows, int cols, int ld,
+                     unsigned long long seed, cudaStream_t stream);
 
 }  // namespace b200

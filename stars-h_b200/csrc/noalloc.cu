@@ -130,6 +130,8 @@ extern "C" int starsh_b200_dense_rsvd_noalloc(const double *dD, int nrows,
     tw.n = ncols;
     tw.k = k;
     tw.slot = 0;
+    tw.maxrank = maxrank;
+    tw.tol = tol;
     B200_CUDA(cudaMemcpyAsync(dt, &tw, sizeof(tw), cudaMemcpyHostToDevice, s),
               "no-alloc tile record");
     B200_CUDA(cudaMemcpy2DAsync(ws.D(0), (size_t)ws.ldD() * sizeof(double), dD,
@@ -137,7 +139,7 @@ extern "C" int starsh_b200_dense_rsvd_noalloc(const double *dD, int nrows,
                                 (size_t)nrows * sizeof(double), ncols,
                                 cudaMemcpyDeviceToDevice, s),
               "no-alloc tile copy");
-    launch_gaussian(omega, (long long)ncols * k, kNoAllocOmegaSeed, s);
+    launch_gaussian(omega, ncols, k, ncols, kNoAllocOmegaSeed, s);
 
     const OutArena none{nullptr, nullptr};
     const OutArena out{dU, dV};
@@ -151,7 +153,7 @@ extern "C" int starsh_b200_dense_rsvd_noalloc(const double *dD, int nrows,
     const int m = nrows, n = ncols;
     if ((info = gemm(STEP_SKETCH, false, false, m, k, none))) return info;
     if ((info = gemm(STEP_GRAM_Y, true, false, k, k, none))) return info;
-    launch_pivchol(0, dt, dt, 1, ws, tol, s);
+    launch_pivchol(0, dt, dt, 1, ws, s);
     launch_gather_cols(0, dt, 1, ws, s);
     if ((info = gemm(STEP_Q1, false, false, m, k, none))) return info;
     if ((info = gemm(STEP_GRAM_Q1, true, false, k, k, none))) return info;
@@ -160,7 +162,7 @@ extern "C" int starsh_b200_dense_rsvd_noalloc(const double *dD, int nrows,
     if ((info = gemm(STEP_RES_Z, true, false, k, k, none))) return info;
     if ((info = gemm(STEP_RES_Y, false, false, m, k, none))) return info;
     if ((info = gemm(STEP_GRAM_YR, true, false, k, k, none))) return info;
-    launch_pivchol(1, dt, dt, 1, ws, tol, s);
+    launch_pivchol(1, dt, dt, 1, ws, s);
     launch_gather_cols(1, dt, 1, ws, s);
     if ((info = gemm(STEP_Q1B, false, false, m, k, none))) return info;
     if ((info = gemm(STEP_RES_Z2, true, false, k, k, none))) return info;
@@ -171,10 +173,10 @@ extern "C" int starsh_b200_dense_rsvd_noalloc(const double *dD, int nrows,
     launch_merge_basis(dt, 1, s);
     if ((info = gemm(STEP_PROJECT, true, false, k, n, none))) return info;
     if ((info = gemm(STEP_GRAM_B, false, true, k, k, none))) return info;
-    launch_pivchol(2, dt, dt, 1, ws, tol, s);
-    launch_jacobi(dt, 1, ws, tol, s, nullptr);
+    launch_pivchol(2, dt, dt, 1, ws, s);
+    launch_jacobi(dt, 1, ws, s, nullptr);
     if ((info = gemm(STEP_ROTATE, true, false, k, n, none))) return info;
-    launch_rank_cut(dt, 1, ws, tol, maxrank, s);
+    launch_rank_cut(dt, 1, ws, s);
     // One tile: its factors start at offset 0 of the caller's buffers, so
     // the output kernels run without a host round trip (rank <= 0 skips).
     launch_select_w(dt, 1, ws, s);

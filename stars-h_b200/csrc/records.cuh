@@ -3,6 +3,7 @@
 // device-resident record kept per STARSH_blrm.
 #pragma once
 #include <cuda_runtime.h>
+#include <memory>
 #include <vector>
 #include "device_ctx.cuh"
 #include "kernel_entry.cuh"
@@ -43,6 +44,8 @@ struct BlockJob {
 // Device-resident factors of one STARSH_blrm.
 struct Record {
     std::vector<void *> chunks;        // device allocations
+    // factor chunks shared with other problems of the same batched call
+    std::vector<std::shared_ptr<void>> shared;
     std::vector<double *> dU, dV;      // per far block (device)
     std::vector<double *> dD;          // per near block (device, or null)
     // Factor chunks in far-block order: the host mirror of U (V) is the

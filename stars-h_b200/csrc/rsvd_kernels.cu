@@ -69,14 +69,19 @@ size_t workspace_layout(Workspace &w, int m_max, int n_max, int k_max,
 constexpr int kStageDim = 4;
 
 __global__ void __launch_bounds__(256)
-k_gen_tiles(DevKernel K, const TileWork *__restrict__ tiles, Workspace ws)
+k_gen_tiles(const DevKernel *__restrict__ kernels,
+            const TileWork *__restrict__ tiles, Workspace ws)
 {
     const TileWork tw = tiles[blockIdx.z];
     if (blockIdx.x * 64 >= tw.m || blockIdx.y * 64 >= tw.n) return;
     __shared__ double rc[kStageDim][64], cc[kStageDim][64];
     __shared__ long long ri[64], ci[64];
     __shared__ double red[8];
+    __shared__ DevKernel Ks;
     const int t = threadIdx.x;
+    if (t == 0) Ks = kernels[tw.prob];
+    __syncthreads();
+    const DevKernel &K = Ks;
     const int i0 = blockIdx.x * 64, j0 = blockIdx.y * 64;
     const bool staged = !K.aos && K.ndim <= kStageDim;
     if (t < 64) {
@@ -129,11 +134,11 @@ k_gen_tiles(DevKernel K, const TileWork *__restrict__ tiles, Workspace ws)
     }
 }
 
-void launch_gen_tiles(const DevKernel &K, const TileWork *d_tiles,
+void launch_gen_tiles(const DevKernel *d_kernels, const TileWork *d_tiles,
                       int ntiles, Workspace ws, cudaStream_t stream)
 {
     dim3 grid((ws.m_max + 63) / 64, (ws.n_max + 63) / 64, ntiles);
-    k_gen_tiles<<<grid, 256, 0, stream>>>(K, d_tiles, ws);
+    k_gen_tiles<<<grid, 256, 0, stream>>>(d_kernels, d_tiles, ws);
 }
 
 // ---------------------------------------------------- Gaussian sketch
@@ -159,12 +164,15 @@ __device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k)
 // Omega entries N(0,1): one Philox block -> two 53-bit uniforms in (0,1]
 // -> one Box-Muller pair (G. E. P. Box, M. E. Muller, Ann. Math. Stat. 29
 // (1958) 610-611).
-__global__ void k_gaussian(double *out, long long count,
+// Entries (2q, c) and (2q + 1, c) come from the Philox block with counter
+// (q, c, 0, 0).
+__global__ void k_gaussian(double *out, int rows, int cols, int ld,
                            unsigned long long seed)
 {
-    const long long pair = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (2 * pair >= count) return;
-    const uint4 c = make_uint4((unsigned)pair, (unsigned)(pair >> 32), 0u, 0u);
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    const int col = blockIdx.y;
+    if (2 * q >= rows || col >= cols) return;
+    const uint4 c = make_uint4((unsigned)q, (unsigned)col, 0u, 0u);
     const uint4 r = philox4x32_10(c, make_uint2((unsigned)seed,
                                                 (unsigned)(seed >> 32)));
     const unsigned long long b1 = ((unsigned long long)r.x << 32) | r.y;
@@ -174,16 +182,18 @@ __global__ void k_gaussian(double *out, long long count,
     const double rad = sqrt(-2.0 * log(u1));
     double s, co;
     sincospi(2.0 * u2, &s, &co);
-    out[2 * pair] = rad * co;
-    if (2 * pair + 1 < count) out[2 * pair + 1] = rad * s;
+    double *o = out + (size_t)col * ld;
+    o[2 * q] = rad * co;
+    if (2 * q + 1 < rows) o[2 * q + 1] = rad * s;
 }
 
-void launch_gaussian(double *d_omega, long long count,
+void launch_gaussian(double *d_omega, int rows, int cols, int ld,
                      unsigned long long seed, cudaStream_t stream)
 {
-    const long long pairs = (count + 1) / 2;
-    k_gaussian<<<(unsigned)((pairs + 255) / 256), 256, 0, stream>>>(
-        d_omega, count, seed);
+    if (rows <= 0 || cols <= 0) return;
+    const int pairs = (rows + 1) / 2;
+    dim3 grid((pairs + 255) / 256, cols);
+    k_gaussian<<<grid, 256, 0, stream>>>(d_omega, rows, cols, ld, seed);
 }
 
 // ------------------------------------------------- GEMM descriptors
@@ -492,10 +502,11 @@ constexpr int kMaxK = 1024;   // largest sketch width handled by one CTA
 // remaining diagonal entry is <= thr.  For the basis phases (A, B) the
 // pivot block R11 = L[piv, :]^T is inverted into T(slot).
 __global__ void __launch_bounds__(kSmallThreads)
-k_pivchol(TileWork *__restrict__ tiles, Workspace ws, int phase, double tol)
+k_pivchol(TileWork *__restrict__ tiles, Workspace ws, int phase)
 {
     TileWork &tw = tiles[blockIdx.x];
     const int s = tw.slot;
+    const double tol = tw.tol;
     __shared__ double dg[kMaxK];
     __shared__ double lp[kMaxK];
     __shared__ unsigned char used[kMaxK];
@@ -629,10 +640,10 @@ k_pivchol(TileWork *__restrict__ tiles, Workspace ws, int phase, double tol)
 }
 
 void launch_round_pivchol(TileWork *d_tiles, int ntiles, Workspace ws,
-                          double tol, int repeat, cudaStream_t stream)
+                          int repeat, cudaStream_t stream)
 {
     k_pivchol<<<ntiles, kSmallThreads, 0, stream>>>(d_tiles, ws,
-                                                    repeat ? PH_R2 : PH_R, tol);
+                                                    repeat ? PH_R2 : PH_R);
 }
 
 // ||D||_F^2 of every block from the generator's per-CTA partial sums, in a
@@ -718,9 +729,9 @@ void launch_round_end(TileWork *d_tiles, int ntiles, int verify,
 }
 
 void launch_pivchol(int phase, const TileWork *, TileWork *d_tiles_rw,
-                    int ntiles, Workspace ws, double tol, cudaStream_t s)
+                    int ntiles, Workspace ws, cudaStream_t s)
 {
-    k_pivchol<<<ntiles, kSmallThreads, 0, s>>>(d_tiles_rw, ws, phase, tol);
+    k_pivchol<<<ntiles, kSmallThreads, 0, s>>>(d_tiles_rw, ws, phase);
 }
 
 // Gathers the pivot columns of Y into the Q buffer (phase A) or the Q1
@@ -941,7 +952,7 @@ __device__ bool jacobi_rotate_stream(double *ca, double *cb, int rows,
 
 template <int CLASS, int G, int E, int THREADS, bool SMEM>
 __global__ void __launch_bounds__(THREADS, THREADS <= 128 ? 512 / THREADS : 1)
-k_jacobi(TileWork *__restrict__ tiles, Workspace ws, double eps2)
+k_jacobi(TileWork *__restrict__ tiles, Workspace ws)
 {
     extern __shared__ double sm[];
     __shared__ int rotated[2];
@@ -949,6 +960,11 @@ k_jacobi(TileWork *__restrict__ tiles, Workspace ws, double eps2)
     const int s = tw.slot;
     const int rows = tw.k1, cols = tw.k2;
     if (cols <= 0 || jacobi_class(rows, cols) != CLASS) return;   // uniform
+    // Relative orthogonality the rotations stop at: the rank cut needs the
+    // left singular vectors orthonormal to well below tol (their overlap
+    // enters the tail energies squared and the projector linearly).
+    const double eps = fmax(1e-15, fmin(1e-8, 0.01 * tw.tol));
+    const double eps2 = eps * eps;
     const int ldg = ws.ldK();
     const int lds = rows | 1;   // odd stride: fewer bank conflicts
     double *A = SMEM ? sm : ws.L(s);
@@ -1022,23 +1038,18 @@ k_jacobi(TileWork *__restrict__ tiles, Workspace ws, double eps2)
 
 template <int CLASS, int G, int E, int THREADS, bool SMEM>
 static void jacobi_class_launch(TileWork *d_tiles, int ntiles, Workspace ws,
-                                double eps2, size_t smem, cudaStream_t stream)
+                                size_t smem, cudaStream_t stream)
 {
     auto *fn = k_jacobi<CLASS, G, E, THREADS, SMEM>;
     if (SMEM && smem > 48 * 1024)
         cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem);
-    fn<<<ntiles, THREADS, SMEM ? smem : 0, stream>>>(d_tiles, ws, eps2);
+    fn<<<ntiles, THREADS, SMEM ? smem : 0, stream>>>(d_tiles, ws);
 }
 
-void launch_jacobi(TileWork *d_tiles, int ntiles, Workspace ws, double tol,
+void launch_jacobi(TileWork *d_tiles, int ntiles, Workspace ws,
                    cudaStream_t stream, cudaStream_t side)
 {
-    // Relative orthogonality the rotations stop at: the rank cut needs the
-    // left singular vectors orthonormal to well below tol (their overlap
-    // enters the tail energies squared and the projector linearly).
-    const double eps = fmax(1e-15, fmin(1e-8, 0.01 * tol));
-    const double eps2 = eps * eps;
     // Classes a batch can reach, from the largest factor it may hold
     // (k1, k2 <= k_max).  Shared memory is sized for the class's largest
     // tile that fits.
@@ -1059,24 +1070,24 @@ void launch_jacobi(TileWork *d_tiles, int ntiles, Workspace ws, double tol,
         cudaStreamWaitEvent(side, fork, 0);
     }
     if (kmax > 128) {
-        jacobi_class_launch<4, 16, 16, 512, false>(d_tiles, ntiles, ws, eps2, 0,
+        jacobi_class_launch<4, 16, 16, 512, false>(d_tiles, ntiles, ws, 0,
                                                    big);
-        jacobi_class_launch<3, 16, 16, 512, true>(d_tiles, ntiles, ws, eps2,
+        jacobi_class_launch<3, 16, 16, 512, true>(d_tiles, ntiles, ws,
                                                   smem_for(256), big);
     }
     if (kmax > 64)
-        jacobi_class_launch<2, 8, 16, 512, true>(d_tiles, ntiles, ws, eps2,
+        jacobi_class_launch<2, 8, 16, 512, true>(d_tiles, ntiles, ws,
                                                  smem_for(128), big);
     if (kmax > 256)
-        jacobi_class_launch<5, 32, 16, 512, false>(d_tiles, ntiles, ws, eps2, 0,
+        jacobi_class_launch<5, 32, 16, 512, false>(d_tiles, ntiles, ws, 0,
                                                    big);
     if (kmax > 512)
-        jacobi_class_launch<6, 32, 0, 1024, false>(d_tiles, ntiles, ws, eps2, 0,
+        jacobi_class_launch<6, 32, 0, 1024, false>(d_tiles, ntiles, ws, 0,
                                                    big);
-    jacobi_class_launch<0, 4, 8, 64, true>(d_tiles, ntiles, ws, eps2,
+    jacobi_class_launch<0, 4, 8, 64, true>(d_tiles, ntiles, ws,
                                            smem_for(32), stream);
     if (kmax > 32)
-        jacobi_class_launch<1, 4, 16, 128, true>(d_tiles, ntiles, ws, eps2,
+        jacobi_class_launch<1, 4, 16, 128, true>(d_tiles, ntiles, ws,
                                                  smem_for(64), stream);
     if (fork) {
         cudaEventRecord(join, side);
@@ -1109,12 +1120,13 @@ void launch_merge_basis(TileWork *d_tiles, int ntiles, cudaStream_t stream)
 // i.e. starsh_dense_dsvfr applied to the exact energies (0 if B = 0).
 // rank = r if r <= maxrank, else -1.
 __global__ void __launch_bounds__(kSmallThreads)
-k_rank_cut(TileWork *__restrict__ tiles, Workspace ws, double tol,
-           int maxrank)
+k_rank_cut(TileWork *__restrict__ tiles, Workspace ws)
 {
     TileWork &tw = tiles[blockIdx.x];
     const int s = tw.slot;
     const int k2 = tw.k2;
+    const double tol = tw.tol;
+    const int maxrank = tw.maxrank;
     __shared__ double e[kMaxK];
     __shared__ int ord[kMaxK];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -1172,10 +1184,10 @@ k_rank_cut(TileWork *__restrict__ tiles, Workspace ws, double tol,
     }
 }
 
-void launch_rank_cut(TileWork *d_tiles, int ntiles, Workspace ws, double tol,
-                     int maxrank, cudaStream_t stream)
+void launch_rank_cut(TileWork *d_tiles, int ntiles, Workspace ws,
+                     cudaStream_t stream)
 {
-    k_rank_cut<<<ntiles, kSmallThreads, 0, stream>>>(d_tiles, ws, tol, maxrank);
+    k_rank_cut<<<ntiles, kSmallThreads, 0, stream>>>(d_tiles, ws);
 }
 
 // Wsel(:, c) = W(:, ord[c]) for c < rank, into L(slot).

@@ -130,6 +130,14 @@ class Stats(Structure):
                 ("svd_ms", c_double), ("output_ms", c_double)]
 
 
+class ServerStats(Structure):
+    _fields_ = [("submitted", c_longlong), ("completed", c_longlong),
+                ("failed", c_longlong), ("groups", c_longlong),
+                ("entries", c_longlong), ("busy_ms", c_double),
+                ("resident_bytes", c_double),
+                ("peak_resident_bytes", c_double)]
+
+
 def _proto(lib):
     P = POINTER
     sig = {
@@ -159,6 +167,22 @@ def _proto(lib):
                                                c_double, c_int]),
         "starsh_b200_approximate": (c_int, [P(P(Blrm)), P(Blrf), c_int,
                                             c_double, c_int, c_int, c_int]),
+        "starsh_b200_approximate_batch": (c_int, [c_int, P(P(Blrm)),
+                                                  P(P(Blrf)), P(c_int),
+                                                  P(c_double), P(c_int),
+                                                  c_int, c_int]),
+        "starsh_b200_server_new": (c_int, [P(c_void_p), c_double, c_int,
+                                           c_int]),
+        "starsh_b200_server_submit": (c_int, [c_void_p, P(Blrf), c_int,
+                                              c_double, c_int, c_void_p, c_int,
+                                              c_void_p, c_int, c_int,
+                                              P(c_longlong)]),
+        "starsh_b200_server_wait": (c_int, [c_void_p, c_longlong, P(P(Blrm)),
+                                            P(c_double)]),
+        "starsh_b200_server_release": (c_int, [c_void_p, P(Blrm)]),
+        "starsh_b200_server_pause": (c_int, [c_void_p, c_int]),
+        "starsh_b200_server_get_stats": (c_int, [c_void_p, P(ServerStats)]),
+        "starsh_b200_server_free": (c_int, [c_void_p]),
         "starsh_b200_blrm_download": (c_int, [P(Blrm)]),
         "starsh_b200_blrm_release": (None, [P(Blrm)]),
         "starsh_b200_blrm_dmml_device": (c_int, [P(Blrm), c_int, c_double,

@@ -132,6 +132,426 @@ def new_format(lib, prob):
     return F
 
 
+# ------------------------------------------- many-problem workloads (C4/C5)
+
+C4 = dict(problems=512, nmin=1024, nmax=16384, tols=(1e-3, 1e-5, 1e-7),
+          kernels=("exp", "sqexp", "matern", "coulomb", "rbf"), oversample=10)
+C5 = dict(rate=200.0, seconds=10.0, median=8192, sigma_log=0.5, nmin=2048,
+          nmax=65536, tols=(1e-4, 1e-6), nrhs=32, budget=120e9, oversample=10)
+
+
+def tile_size(n):
+    """Block size for an N-point problem (from {256, 512, 1024}): at least
+    about 16 x 16 tiles for small problems, 1024 above 8192 points."""
+    return 256 if n <= 2048 else 512 if n <= 8192 else 1024
+
+
+def _malloc_doubles(values):
+    """A libc-malloc'd copy (the library frees point arrays it owns)."""
+    libc = ctypes.CDLL("libc.so.6")
+    libc.malloc.restype = c_void_p
+    ptr = libc.malloc(ctypes.c_size_t(8 * len(values)))
+    arr = (ctypes.c_double * len(values)).from_address(ptr)
+    arr[:] = list(map(float, values))
+    return ctypes.cast(ptr, POINTER(ctypes.c_double))
+
+
+def sphere_points(rng, n):
+    """n points uniform on the surfaces of 1-8 spheres (radius U[0.05, 0.2],
+    centres uniform in the unit cube)."""
+    import numpy as np
+    ns = int(rng.integers(1, 9))
+    centres = rng.uniform(0.0, 1.0, (ns, 3))
+    radii = rng.uniform(0.05, 0.2, ns)
+    which = np.sort(rng.integers(0, ns, n))
+    v = rng.standard_normal((n, 3))
+    v /= np.linalg.norm(v, axis=1)[:, None]
+    return centres[which] + radii[which, None] * v
+
+
+def mixed_problem(lib, seed, n, kernel, ndim, coulomb_handle):
+    """One problem of the many-problem workloads, built with the library's
+    own host API: spatial kernels on a jittered grid (N rounded to a
+    square / cube), 1/r (unit diagonal) on jittered particles, Gaussian RBF
+    (radius 0.1) on points on spheres, all Z-sorted."""
+    import numpy as np
+    import starsh_b200 as sb
+    libc = ctypes.CDLL("libc.so.6")
+    libc.srand(seed)
+    kern = c_void_p()
+    if kernel in ("exp", "sqexp", "matern"):
+        side = max(2, int(round(n ** (1.0 / ndim))))
+        n = side ** ndim
+        data = POINTER(sb.SSData)()
+        nu = 1.5 if kernel == "matern" else 0.5
+        assert lib.starsh_ssdata_generate(byref(data), n, ndim, 0.1, nu, 0.0,
+                                          6, 1.0) == 0
+        ktype = {"exp": 1, "sqexp": 2, "matern": 3}[kernel]
+        assert lib.starsh_ssdata_get_kernel(byref(kern), data, ktype) == 0
+    elif kernel == "coulomb":
+        side = max(2, int(round(n ** (1.0 / ndim))))
+        n = side ** ndim
+        data = POINTER(sb.Particles)()
+        assert lib.starsh_particles_generate(byref(data), n, ndim, 6) == 0
+        kern = c_void_p(ctypes.cast(coulomb_handle, c_void_p).value)
+    else:
+        rng = np.random.default_rng(seed)
+        pts = sphere_points(rng, n)
+        part = POINTER(sb.Particles)()
+        assert lib.starsh_particles_init(byref(part), n, 3,
+                                         _malloc_doubles(pts.T.ravel())) == 0
+        assert lib.starsh_particles_zsort_inplace(part) == 0
+        soa = np.ctypeslib.as_array(part.contents.point, shape=(3 * n,))
+        mesh = soa.reshape(3, n).T.ravel()          # point-major
+        data = POINTER(sb.MDData)()
+        assert lib.starsh_mddata_init(byref(data), n, _malloc_doubles(mesh),
+                                      0, 1, 0, 0.0, 0.1, 0.0) == 0
+        kern = c_void_p(sb.kernel_symbol(lib, "starsh_generate_3d_virus"))
+        _keep.append(part)
+    nb = tile_size(n)
+    shape = (sb.STARSH_int * 2)(n, n)
+    P = POINTER(sb.Problem)()
+    assert lib.starsh_problem_new(byref(P), 2, shape, b"N", b"d", data, data,
+                                  kern, b"mixed") == 0
+    C = POINTER(sb.Cluster)()
+    assert lib.starsh_cluster_new_plain(byref(C), data, n, nb) == 0
+    _keep.append(shape)
+    return dict(data=data, P=P, C=C, n=n, nb=nb, maxrank=min(nb // 2, 256),
+                kernel=kernel, ndim=ndim)
+
+
+def c4_specs():
+    """The 512 problems: N log-uniform in [1024, 16384], kernel and tol
+    uniform over their sets, seed = problem index."""
+    import numpy as np
+    out = []
+    for p in range(C4["problems"]):
+        rng = np.random.default_rng(p)
+        n = int(round(np.exp(rng.uniform(np.log(C4["nmin"]), np.log(C4["nmax"])))))
+        kernel = C4["kernels"][int(rng.integers(len(C4["kernels"])))]
+        tol = C4["tols"][int(rng.integers(len(C4["tols"])))]
+        ndim = 3 if kernel in ("coulomb", "rbf") else 2
+        out.append(dict(seed=p, n=n, kernel=kernel, tol=tol, ndim=ndim, t=0.0))
+    return out
+
+
+def c5_specs(seconds, rate, seed=12345):
+    """Poisson arrivals: N lognormal (median 8192, sigma_log 0.5) clipped to
+    [2048, 65536], 2-D or 3-D, kernel from the C4 set, tol in {1e-4, 1e-6}."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    out, t = [], 0.0
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t > seconds:
+            break
+        n = int(np.clip(np.exp(rng.normal(np.log(C5["median"]), C5["sigma_log"])),
+                        C5["nmin"], C5["nmax"]))
+        kernel = C4["kernels"][int(rng.integers(len(C4["kernels"])))]
+        ndim = 3 if kernel == "rbf" else int(rng.integers(2, 4))
+        tol = C5["tols"][int(rng.integers(len(C5["tols"])))]
+        out.append(dict(seed=len(out), n=n, kernel=kernel, tol=tol, ndim=ndim,
+                        t=t))
+    return out
+
+
+def build_mixed(lib, specs, coulomb_handle):
+    out = []
+    for sp in specs:
+        pr = mixed_problem(lib, sp["seed"], sp["n"], sp["kernel"], sp["ndim"],
+                           coulomb_handle)
+        pr["tol"] = sp["tol"]
+        pr["t"] = sp["t"]
+        out.append(pr)
+    return out
+
+
+def reference_arm_mixed(args, key, threads):
+    """--impl reference for c4-batch / c5-serve: the reference's OpenMP RSVD
+    (plus its dmml with 32 right-hand sides for c5) one problem at a time on
+    the host cores, over the first exp/sqexp problems of the workload (the
+    reference has no Matern without GSL; its other kernels need wrappers
+    this sample leaves out)."""
+    specs = c4_specs() if key == "c4-batch" else c5_specs(C5["seconds"], C5["rate"])
+    sample = [sp for sp in specs if sp["kernel"] in ("exp", "sqexp")][:6]
+    for sp in sample:
+        side = max(2, int(round(sp["n"] ** (1.0 / sp["ndim"]))))
+        sp["n"] = side ** sp["ndim"]
+        sp["nb"] = tile_size(sp["n"])
+        sp["maxrank"] = min(sp["nb"] // 2, 256)
+        sp["nrhs"] = C5["nrhs"] if key == "c5-serve" else 0
+    times, entries, lat = [], 0, []
+    for i in range(args.warmup + args.steps):
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads),
+                   OPENBLAS_NUM_THREADS="1", STARSH_MIXED_SPECS=json.dumps(sample))
+        out = subprocess.run([sys.executable, os.path.abspath(__file__),
+                              "--_cpu-run", "1", "--workload", key], env=env,
+                             capture_output=True, text=True, timeout=900)
+        r = next(json.loads(x) for x in out.stdout.splitlines() if x.startswith("{"))
+        if i >= args.warmup:
+            times.append(r["seconds"])
+            lat += r["latency_ms"]
+        entries = r["entries"]
+    t = statistics.mean(times)
+    v = entries / t / 1e6
+    import numpy as np
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "Mentries/s",
+        "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": dict(workload=key, engine="starsh_blrm__drsdd_omp",
+                       sample=[(sp["n"], sp["kernel"], sp["tol"]) for sp in sample]),
+        "cpu_baseline": {"value": v, "unit": "Mentries/s", "cores": threads,
+                         "kind": "reference",
+                         "sample": f"{len(sample)} exp/sqexp problems of the workload, one at a time"},
+        "e2e": {"value": v, "unit": "Mentries/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0}}
+    if key == "c5-serve":
+        line["latency_ms"] = {"p50": float(np.percentile(lat, 50)),
+                              "p99": float(np.percentile(lat, 99)),
+                              "note": "service time of one request alone, no queueing"}
+    print(json.dumps(line))
+
+
+def _cpu_run_mixed():
+    """Child process body of reference_arm_mixed (reference library only)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import numpy as np
+    import oracle
+    from harness import RefProblem
+    ref = oracle.Ref()
+    specs = json.loads(os.environ["STARSH_MIXED_SPECS"])
+    total, entries, lat = 0.0, 0, []
+    for sp in specs:
+        pr = RefProblem(ref, "spatial", sp["n"], sp["nb"], ndim=sp["ndim"],
+                        place=6, beta=0.1, nu=0.5, kernel_name=sp["kernel"],
+                        seed=sp["seed"])
+        A = np.random.default_rng(1).standard_normal((sp["n"], max(1, sp["nrhs"])))
+        t0 = time.perf_counter()
+        M = ref.approximate(pr.F, sp["maxrank"], sp["tol"], oversample=10)
+        if sp["nrhs"]:
+            ref.dmml(M, A)
+        dt = time.perf_counter() - t0
+        total += dt
+        lat.append(dt * 1e3)
+        entries += sp["n"] ** 2
+    print(json.dumps({"seconds": total, "entries": entries, "latency_ms": lat}))
+
+
+def run_c4(args, lib, stream, clocks, torch):
+    """512 independent problems in one batched call (the mixed engine),
+    against the FP64 engine one problem at a time."""
+    import starsh_b200 as sb
+    handle = sb.KERNEL(lambda *a: None)
+    _keep.append(handle)
+    assert lib.starsh_b200_kernel_register(
+        c_void_p(ctypes.cast(handle, c_void_p).value), sb.FAMILY["coulomb"],
+        1.0) == 0
+    lib.starsh_set_oversample(str(C4["oversample"]).encode())
+    t_build = time.perf_counter()
+    probs = build_mixed(lib, c4_specs(), handle)
+    t_build = time.perf_counter() - t_build
+    n = len(probs)
+    ranks = (ctypes.c_int * n)(*[p["maxrank"] for p in probs])
+    tols = (ctypes.c_double * n)(*[p["tol"] for p in probs])
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def batched(engine):
+        Fs = (POINTER(sb.Blrf) * n)(*[new_format(lib, p) for p in probs])
+        Ms = (POINTER(sb.Blrm) * n)()
+        flush.zero_()
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        info = lib.starsh_b200_approximate_batch(n, Ms, Fs, ranks, tols, None,
+                                                 engine, 0)
+        e.record(stream)
+        e.synchronize()
+        assert info == 0, lib.starsh_b200_last_error()
+        return Ms, Fs, s.elapsed_time(e) / 1e3, sb.stats(lib)
+
+    def sequential(engine):
+        total = 0.0
+        for p in probs:
+            F = new_format(lib, p)
+            M = POINTER(sb.Blrm)()
+            flush.zero_()
+            torch.cuda.synchronize()
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            assert lib.starsh_b200_approximate(byref(M), F, p["maxrank"],
+                                               p["tol"], 0, engine, 0) == 0
+            e.record(stream)
+            e.synchronize()
+            total += s.elapsed_time(e) / 1e3
+            lib.starsh_blrm_free(M)
+            lib.starsh_blrf_free(F)
+        return total
+
+    def free_all(Ms, Fs):
+        for i in range(n):
+            lib.starsh_blrm_free(Ms[i])
+            lib.starsh_blrf_free(Fs[i])
+
+    for _ in range(args.warmup):
+        free_all(*batched(sb.ENGINE_MIXED)[:2])
+    times, st = [], None
+    with clocks:
+        for i in range(args.steps):
+            Ms, Fs, t, st = batched(sb.ENGINE_MIXED)
+            times.append(t)
+            if i + 1 < args.steps:
+                free_all(Ms, Fs)
+    worst = 0.0
+    ok = True
+    for i in range(n):
+        err = lib.starsh_blrm__dfe_b200(Ms[i])
+        ok &= 0 <= err <= probs[i]["tol"]
+        worst = max(worst, err / probs[i]["tol"])
+    free_all(Ms, Fs)
+    t_dev = statistics.mean(times)
+    Ms, Fs, t_fp64_batched, _ = batched(sb.ENGINE_FP64)
+    free_all(Ms, Fs)
+    t_seq_fp64 = sequential(sb.ENGINE_FP64)
+    t_seq_mixed = sequential(sb.ENGINE_MIXED)
+    entries = st.entries
+    kinds = {k: sum(1 for p in probs if p["kernel"] == k) for k in C4["kernels"]}
+    line = {
+        "metric": METRIC, "value": entries / t_dev / 1e6 if ok else None,
+        "unit": "Mentries/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_dev * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded point generators)",
+        "config": {"workload": "uneven-batch-512-problems-N1024-16384",
+                   "engine": "mixed (adaptive sketch), one batched call",
+                   "problems": n, "kernels": kinds,
+                   "tols": list(C4["tols"]), "tile_sizes": [256, 512, 1024],
+                   "entries": int(entries), "tiles": int(st.tiles),
+                   "false_far": int(st.false_far), "batches": int(st.batches),
+                   "l2": "flushed (256 MB write) before every step",
+                   "host_build_s": t_build},
+        "accepted": bool(ok), "worst_err_over_tol": worst,
+        "fp64_batched": {"value": entries / t_fp64_batched / 1e6,
+                         "ms": t_fp64_batched * 1e3},
+        "plain_fp64": {"value": entries / t_seq_fp64 / 1e6,
+                       "ms_per_step": t_seq_fp64 * 1e3,
+                       "what": "FP64 engine, one problem at a time",
+                       "chosen_over_plain": t_seq_fp64 / t_dev},
+        "mixed_one_at_a_time": {"value": entries / t_seq_mixed / 1e6,
+                                "ms": t_seq_mixed * 1e3},
+        "phases_ms": {"gen": st.gen_ms, "basis": st.basis_ms,
+                      "project": st.project_ms, "svd": st.svd_ms,
+                      "output": st.output_ms},
+        "gpu_launches": int(st.kernel_launches),
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line))
+
+
+def serve(lib, reqs, engine, max_group, A):
+    """Replays the arrivals against a server; returns latencies (ms),
+    entries and the wall time from the first submit to the last
+    completion."""
+    import numpy as np
+    import starsh_b200 as sb
+    srv = c_void_p()
+    assert lib.starsh_b200_server_new(byref(srv), C5["budget"], engine,
+                                      max_group) == 0
+    fmts = [new_format(lib, r) for r in reqs]
+    outs = [None] * len(reqs)
+    tickets = [None] * len(reqs)
+    nrhs = C5["nrhs"]
+    lda = A.shape[0]
+
+    def submitter():
+        t0 = time.perf_counter()
+        for i, r in enumerate(reqs):
+            dt = r["t"] - (time.perf_counter() - t0)
+            if dt > 0:
+                time.sleep(dt)
+            outs[i] = np.empty((r["n"], nrhs), order="F")
+            t = ctypes.c_longlong()
+            assert lib.starsh_b200_server_submit(
+                srv, fmts[i], r["maxrank"], r["tol"], nrhs, A.ctypes.data, lda,
+                outs[i].ctypes.data, r["n"], 0, byref(t)) == 0
+            tickets[i] = t.value
+
+    t_start = time.perf_counter()
+    th = threading.Thread(target=submitter)
+    th.start()
+    lat, status = [], []
+    for i in range(len(reqs)):
+        while tickets[i] is None:
+            time.sleep(0.0005)
+        L = ctypes.c_double()
+        status.append(lib.starsh_b200_server_wait(srv, tickets[i], None,
+                                                  byref(L)))
+        lat.append(L.value)
+        outs[i] = None
+    th.join()
+    wall = time.perf_counter() - t_start
+    st = sb.ServerStats()
+    lib.starsh_b200_server_get_stats(srv, byref(st))
+    lib.starsh_b200_server_free(srv)
+    for F in fmts:
+        lib.starsh_blrf_free(F)
+    return np.array(lat), status, st, wall
+
+
+def run_c5(args, lib, clocks):
+    """Poisson arrivals replayed against the serving loop (mixed engine,
+    continuous batching), then against the FP64 engine one request at a
+    time."""
+    import numpy as np
+    import starsh_b200 as sb
+    handle = sb.KERNEL(lambda *a: None)
+    _keep.append(handle)
+    assert lib.starsh_b200_kernel_register(
+        c_void_p(ctypes.cast(handle, c_void_p).value), sb.FAMILY["coulomb"],
+        1.0) == 0
+    lib.starsh_set_oversample(str(C5["oversample"]).encode())
+    seconds = args.serve_seconds
+    reqs = build_mixed(lib, c5_specs(seconds, C5["rate"]), handle)
+    A = np.asfortranarray(np.random.default_rng(1).standard_normal(
+        (C5["nmax"], C5["nrhs"])))
+    # warm-up on the first few requests
+    serve(lib, reqs[:min(8, len(reqs))], sb.ENGINE_MIXED, 0, A)
+    with clocks:
+        lat, status, st, wall = serve(lib, reqs, sb.ENGINE_MIXED, 0, A)
+    lat_p, status_p, st_p, wall_p = serve(lib, reqs, sb.ENGINE_FP64, 1, A)
+    ok = all(x == 0 for x in status)
+
+    def pct(v):
+        return {"p50": float(np.percentile(v, 50)),
+                "p99": float(np.percentile(v, 99)),
+                "mean": float(np.mean(v)), "max": float(np.max(v))}
+    big = np.array([r["n"] for r in reqs]) >= 32768
+    line = {
+        "metric": "served Mentries/s and request latency (submit to 32 matvecs done)",
+        "value": st.entries / wall / 1e6 if ok else None, "unit": "Mentries/s",
+        "n_gpus": 1, "steps": 1, "warmup": 1, "ms_per_step": wall * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded point generators)",
+        "config": {"workload": f"serving-poisson-{C5['rate']:g}rps-{seconds:g}s",
+                   "requests": len(reqs), "offered_rate_rps": C5["rate"],
+                   "N": "lognormal median 8192, sigma_log 0.5, clipped [2048, 65536]",
+                   "tols": list(C5["tols"]), "nrhs": C5["nrhs"],
+                   "hbm_budget_bytes": C5["budget"], "engine": "mixed, continuous batching"},
+        "latency_ms": pct(lat),
+        "latency_ms_N_ge_32768": pct(lat[big]) if big.any() else None,
+        "served_rps": len(reqs) / wall, "groups": int(st.groups),
+        "failed": int(st.failed),
+        "peak_resident_bytes": st.peak_resident_bytes,
+        "plain_fp64_one_at_a_time": {
+            "value": st_p.entries / wall_p / 1e6, "latency_ms": pct(lat_p),
+            "served_rps": len(reqs) / wall_p, "wall_s": wall_p},
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line))
+
+
 # ------------------------------------------------------------- clocks
 
 class ClockSampler:
@@ -312,7 +732,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--engine", default="mixed", choices=["fp64", "mixed"])
-    ap.add_argument("--workload", default="c2-sqexp", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="c2-sqexp",
+                    choices=sorted(WORKLOADS) + ["c4-batch", "c5-serve"])
+    ap.add_argument("--serve-seconds", type=float, default=C5["seconds"],
+                    help="c5-serve: length of the arrival stream")
     ap.add_argument("--n", type=int, default=0,
                     help="points (a smaller N profiles the same kernels)")
     ap.add_argument("--no-cpu", action="store_true",
@@ -321,12 +744,32 @@ def main():
     args = ap.parse_args()
     key = args.workload
     if args.cpu_run:
-        _cpu_run(key, args.cpu_run)
+        if key in ("c4-batch", "c5-serve"):
+            _cpu_run_mixed()
+        else:
+            _cpu_run(key, args.cpu_run)
         return
 
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local = int(os.environ.get("LOCAL_RANK", 0))
+    if key in ("c4-batch", "c5-serve"):
+        if args.impl == "reference":
+            if rank == 0:
+                reference_arm_mixed(args, key, len(os.sched_getaffinity(0)))
+            return
+        import torch
+        import starsh_b200 as sb
+        lib = sb.load()
+        torch.cuda.set_device(local)
+        assert lib.starsh_b200_set_device(local) == 0
+        stream = torch.cuda.ExternalStream(lib.starsh_b200_stream())
+        clocks = ClockSampler(local)
+        if key == "c4-batch":
+            run_c4(args, lib, stream, clocks, torch)
+        else:
+            run_c5(args, lib, clocks)
+        return
     wl = dict(WORKLOADS[key])
     if args.n:
         wl["N"] = args.n

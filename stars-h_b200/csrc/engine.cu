@@ -10,6 +10,9 @@
 // are compacted (:259-282).  The per-block loop runs as batches of tiles
 // through the device pipeline of rsvd_kernels.cu.
 #include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstdint>
 #include <atomic>
 #include <mutex>
 #include <thread>
@@ -144,6 +147,10 @@ int upload_problem(DevicePoints &dp, STARSH_problem *P,
                                    &cp, &cc, P->col_data);
     if (info != STARSH_SUCCESS) return info;
     fill_kernel(dp.K, spec);
+    dp.h_row = rp;
+    dp.h_col = cp;
+    dp.h_row_count = rc;
+    dp.h_col_count = cc;
     const void *d;
     const size_t per = (size_t)spec.ndim * sizeof(double);
     if ((info = dp.upload(rp, rc * per, &d, s))) return info;
@@ -249,6 +256,32 @@ struct ProblemJob {
     std::vector<int> rank;    // per far block of F (filled by compress)
 };
 
+// Bounding boxes of the clusters of C over the given coordinates (SoA
+// x[d * count + i], or AoS x[ndim * i + d]): lo/hi per cluster and
+// dimension.
+static void cluster_boxes(const double *pts, long long count, int ndim,
+                          int aos, const STARSH_cluster *C,
+                          std::vector<double> &lo, std::vector<double> &hi)
+{
+    const STARSH_int nc = C->nblocks;
+    lo.assign((size_t)nc * ndim, 0.0);
+    hi.assign((size_t)nc * ndim, 0.0);
+    if (pts == nullptr) return;
+    for (STARSH_int c = 0; c < nc; ++c)
+        for (int d = 0; d < ndim; ++d) {
+            double a = DBL_MAX, b = -DBL_MAX;
+            for (STARSH_int q = C->start[c]; q < C->start[c] + C->size[c]; ++q) {
+                const long long i = C->pivot[q];
+                const double x = aos ? pts[(size_t)ndim * i + d]
+                                     : pts[(size_t)d * count + i];
+                a = std::min(a, x);
+                b = std::max(b, x);
+            }
+            lo[(size_t)c * ndim + d] = a;
+            hi[(size_t)c * ndim + d] = b;
+        }
+}
+
 // Runs the device pipeline over the far blocks of every problem of `jobs`
 // in shared batches: tiles of different problems (kernels, sizes, tol,
 // maxrank) share every launch.  Fills each job's ranks and the per-block
@@ -262,6 +295,7 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
     starsh_b200_stats &st = thread_stats();
     std::vector<TileWork> all;
     std::vector<std::pair<int, STARSH_int>> owner;   // (job, far block)
+    std::vector<double> sep;                          // cluster separation
     int m_max = 0, n_max = 0, k_max = 0;
     bool may_repeat = false;
     std::vector<DevKernel> kernels;
@@ -274,6 +308,12 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
         jb.rec->dU.assign(nfar, nullptr);
         jb.rec->dV.assign(nfar, nullptr);
         kernels.push_back(jb.rec->points->K);
+        // cluster boxes, for ordering tiles by separation
+        const DevicePoints &dp = *jb.rec->points;
+        const int nd = dp.K.ndim;
+        std::vector<double> rlo, rhi, clo, chi;
+        cluster_boxes(dp.h_row, dp.h_row_count, nd, dp.K.aos, R, rlo, rhi);
+        cluster_boxes(dp.h_col, dp.h_col_count, nd, dp.K.aos, C, clo, chi);
         // a repeat pass can only be needed when (tol/10)^2 lies below the
         // squared-noise floor of a Gram
         if (nfar > 0 && 0.01 * jb.tol * jb.tol < 1e-15) may_repeat = true;
@@ -293,6 +333,19 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
             n_max = std::max(n_max, t.n);
             k_max = std::max(k_max, t.k);
             st.entries += (long long)t.m * t.n;
+            // separation of the two clusters relative to the larger
+            // diameter: small for near-diagonal (high-rank) blocks
+            double gap2 = 0.0, di = 0.0, dj = 0.0;
+            for (int d = 0; d < nd; ++d) {
+                const double a0 = rlo[(size_t)i * nd + d], a1 = rhi[(size_t)i * nd + d];
+                const double b0 = clo[(size_t)j * nd + d], b1 = chi[(size_t)j * nd + d];
+                const double g = std::max(0.0, std::max(a0 - b1, b0 - a1));
+                gap2 += g * g;
+                di += (a1 - a0) * (a1 - a0);
+                dj += (b1 - b0) * (b1 - b0);
+            }
+            const double diam = std::sqrt(std::max(di, dj));
+            sep.push_back(diam > 0.0 ? std::sqrt(gap2) / diam : 0.0);
             all.push_back(t);
             owner.emplace_back((int)p, b);
         }
@@ -322,24 +375,67 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
     }
     const double *omega = (const double *)ctx.omega.ptr;
 
-    Workspace ws{};
-    const size_t stride = workspace_layout(ws, m_max, n_max, k_max, true);
+    // Processing order: larger tiles first (a batch's workspace layout is
+    // sized by its first tile), then by sketch width, then by cluster
+    // separation (near-diagonal, high-rank blocks together, so that their
+    // long small-SVD runs share batches), then the problems' block order.
+    // Results do not depend on the order.
+    {
+        std::vector<long long> ord(ntot);
+        for (long long q = 0; q < ntot; ++q) ord[q] = q;
+        std::stable_sort(ord.begin(), ord.end(), [&](long long a, long long b) {
+            const long long sa = (long long)all[a].m * all[a].n;
+            const long long sb = (long long)all[b].m * all[b].n;
+            if (sa != sb) return sa > sb;
+            if (all[a].k != all[b].k) return all[a].k > all[b].k;
+            return sep[a] < sep[b];
+        });
+        std::vector<TileWork> a2(ntot);
+        std::vector<std::pair<int, STARSH_int>> o2(ntot);
+        for (long long q = 0; q < ntot; ++q) {
+            a2[q] = all[ord[q]];
+            o2[q] = owner[ord[q]];
+        }
+        all.swap(a2);
+        owner.swap(o2);
+    }
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
     size_t budget = std::min<size_t>(free_b / 2, (size_t)24 << 30);
     if (const char *e = getenv("STARSH_B200_WORKSPACE_MB"))
         budget = std::min<size_t>(budget, (size_t)atoll(e) << 20);
-    long long slots = (long long)(budget / (stride * sizeof(double)));
-    slots = std::max<long long>(1, std::min<long long>(slots, ntot));
-    slots = std::min<long long>(slots, 4096);
-    if (!ctx.workspace.reserve((size_t)slots * stride * sizeof(double)))
+    // Batch plan: each batch takes as many tiles as fit the budget with
+    // the layout of its largest dimensions (at most 4096).
+    struct BatchPlan { long long b0; int nt; int m, n, k; size_t stride; };
+    std::vector<BatchPlan> plan;
+    size_t ws_need = 0;
+    long long max_slots = 1;
+    for (long long b0 = 0; b0 < ntot;) {
+        Workspace probe{};
+        int bm = all[b0].m, bn = all[b0].n, bk = all[b0].k;
+        size_t stride = workspace_layout(probe, bm, bn, bk, true);
+        long long cap = (long long)(budget / (stride * sizeof(double)));
+        cap = std::max<long long>(1, std::min<long long>({cap, ntot - b0, 4096}));
+        for (long long q = b0; q < b0 + cap; ++q) {
+            bm = std::max(bm, all[q].m);
+            bn = std::max(bn, all[q].n);
+            bk = std::max(bk, all[q].k);
+        }
+        stride = workspace_layout(probe, bm, bn, bk, true);
+        long long fit = (long long)(budget / (stride * sizeof(double)));
+        const int nt = (int)std::max<long long>(1, std::min(cap, fit));
+        plan.push_back({b0, nt, bm, bn, bk, stride});
+        ws_need = std::max(ws_need, (size_t)nt * stride * sizeof(double));
+        max_slots = std::max<long long>(max_slots, nt);
+        b0 += nt;
+    }
+    if (!ctx.workspace.reserve(ws_need))
         return cuda_fail(cudaErrorMemoryAllocation, "workspace");
-    ws.base = (double *)ctx.workspace.ptr;
-    ws.stride = stride;
-    if (!ctx.tiles.reserve((size_t)slots * sizeof(TileWork)) ||
-        !ctx.descs.reserve((size_t)slots * sizeof(GemmDesc)) ||
+    if (!ctx.tiles.reserve((size_t)max_slots * sizeof(TileWork)) ||
+        !ctx.descs.reserve((size_t)max_slots * sizeof(GemmDesc)) ||
         !ctx.flag.reserve(256))
         return cuda_fail(cudaErrorMemoryAllocation, "batch arrays");
+    Workspace ws{};
     TileWork *dt = (TileWork *)ctx.tiles.ptr;
     GemmDesc *dd = (GemmDesc *)ctx.descs.ptr;
 
@@ -365,8 +461,13 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
                    : cuda_fail(cudaGetLastError(), "gemm_f64_batched");
     };
 
-    for (long long b0 = 0; b0 < ntot && info == STARSH_SUCCESS; b0 += slots) {
-        const int nt = (int)std::min<long long>(slots, ntot - b0);
+    for (size_t pi = 0; pi < plan.size() && info == STARSH_SUCCESS; ++pi) {
+        const long long b0 = plan[pi].b0;
+        const int nt = plan[pi].nt;
+        const int m_max = plan[pi].m, k_max = plan[pi].k;
+        workspace_layout(ws, plan[pi].m, plan[pi].n, plan[pi].k, true);
+        ws.base = (double *)ctx.workspace.ptr;
+        ws.stride = plan[pi].stride;
         for (int t = 0; t < nt; ++t) all[b0 + t].slot = t;
         cudaMemcpyAsync(dt, &all[b0], nt * sizeof(TileWork),
                         cudaMemcpyHostToDevice, s);
@@ -374,6 +475,9 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
         launch_gen_tiles(d_kernels, dt, nt, ws, s);
         count_launch();
         cudaEventRecord(ev[5], s);
+        // exact ||D||_F^2 of every block (generator partial sums)
+        launch_block_norms(dt, dt, nt, ws, s);
+        count_launch();
         if (ep.engine == STARSH_B200_FP64) {
         cudaEventRecord(ev[0], s);
         if ((info = gemm(STEP_SKETCH, false, false, nt, m_max, k_max, none))) break;
@@ -416,8 +520,6 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
         // round stayed below that threshold (the residual estimate of
         // N. Halko, P.-G. Martinsson, J. A. Tropp, SIAM Review 53 (2011)
         // sec. 4.3), when a round adds none, or after k columns.
-        launch_block_norms(dt, dt, nt, ws, s);
-        count_launch();
         int *d_active = (int *)ctx.flag.ptr;
         auto append = [&](int bmax) -> int {
             // orthonormalise the selected residual columns (kb of them)
@@ -479,13 +581,13 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
         }
         // projection and small SVD
         cudaEventRecord(ev[2], s);
-        if ((info = gemm(STEP_PROJECT, true, false, nt, k_max, n_max, none))) break;
+        if ((info = gemm(STEP_PROJECT, true, false, nt, k_max, plan[pi].n, none))) break;
         cudaEventRecord(ev[3], s);
         if ((info = gemm(STEP_GRAM_B, false, true, nt, k_max, k_max, none))) break;
         launch_pivchol(2, dt, dt, nt, ws, s);
         launch_jacobi(dt, nt, ws, s, ctx.side);
         count_launch(2);
-        if ((info = gemm(STEP_ROTATE, true, false, nt, k_max, n_max, none))) break;
+        if ((info = gemm(STEP_ROTATE, true, false, nt, k_max, plan[pi].n, none))) break;
         launch_rank_cut(dt, nt, ws, s);
         count_launch();
         cudaEventRecord(ev[6], s);
@@ -509,10 +611,6 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
             st.sketch_flops += 2.0 * w.m * w.n *
                 (ep.engine == STARSH_B200_FP64 ? w.k : w.cols_done);
             st.project_flops += 2.0 * w.m * w.n * w.k1;
-            if (w.status & TILE_CHOL_FAIL) {
-                set_error("re-orthogonalisation failed on a tile");
-                info = STARSH_UNKNOWN_ERROR;
-            }
             jobs[w.prob].rank[owner[b0 + t].second] = w.rank;
             if (w.rank > 0) {
                 nu[w.prob] += (size_t)w.m * w.rank;
@@ -694,13 +792,44 @@ static int fill_host_mirror(STARSH_blrm *M, Record &rec, cudaStream_t s)
         ou += pt.nu;
         ov += pt.nv;
     }
+    // Each block's host position: the host offset of the part holding its
+    // device factors plus its offset inside that part (tiles of a problem
+    // may have been processed in any order).
+    struct Span { const double *dev; size_t n, host; };
+    std::vector<Span> su, sv;
     ou = ov = 0;
+    for (const Record::Part &pt : rec.parts) {
+        su.push_back({pt.U, pt.nu, ou});
+        sv.push_back({pt.V, pt.nv, ov});
+        ou += pt.nu;
+        ov += pt.nv;
+    }
+    auto by_dev = [](const Span &a, const Span &b) { return a.dev < b.dev; };
+    std::sort(su.begin(), su.end(), by_dev);
+    std::sort(sv.begin(), sv.end(), by_dev);
+    auto host_of = [](const std::vector<Span> &sp, const double *d) -> size_t {
+        auto it = std::upper_bound(sp.begin(), sp.end(), Span{d, 0, 0},
+                                   [](const Span &a, const Span &b) {
+                                       return a.dev < b.dev;
+                                   });
+        if (it == sp.begin()) return SIZE_MAX;
+        --it;
+        if (d < it->dev || d >= it->dev + it->n) return SIZE_MAX;
+        return it->host + (size_t)(d - it->dev);
+    };
     for (STARSH_int b = 0; b < F->nblocks_far; ++b) {
-        const int r = M->far_rank[b];
-        M->far_U[b]->data = hU + ou;
-        M->far_V[b]->data = hV + ov;
-        ou += (size_t)M->far_U[b]->shape[0] * r;
-        ov += (size_t)M->far_V[b]->shape[0] * r;
+        M->far_U[b]->data = hU;
+        M->far_V[b]->data = hV;
+        if (M->far_rank[b] <= 0) continue;
+        const size_t pu = host_of(su, rec.dU[b]), pv = host_of(sv, rec.dV[b]);
+        if (pu == SIZE_MAX || pv == SIZE_MAX) {
+            free(hU);
+            free(hV);
+            set_error("host mirror: factor outside its chunks");
+            return STARSH_UNKNOWN_ERROR;
+        }
+        M->far_U[b]->data = hU + pu;
+        M->far_V[b]->data = hV + pv;
     }
     if (M->onfly == 0 && F->nblocks_near > 0) {
         hD = (double *)malloc(std::max<size_t>(rec.d_total, 1) * sizeof(double));

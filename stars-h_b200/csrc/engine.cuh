@@ -10,9 +10,9 @@ namespace b200 {
 // Status bits of a tile.
 enum : int {
     TILE_OK = 0,
-    TILE_CHOL_FAIL = 1,    // Cholesky of a re-orthogonalisation Gram failed
+    TILE_CHOL_TRUNC = 1,   // a re-orthogonalisation dropped dependent columns
     TILE_JACOBI_SLOW = 2,  // Jacobi sweeps hit their cap
-    TILE_TAIL_LEFT = 4,    // deflated energy alone exceeded the tolerance
+    TILE_TAIL_LEFT = 4,    // energy outside the factors alone exceeds tol
 };
 
 // One far-field tile of a batch.
@@ -37,6 +37,7 @@ struct TileWork {
     int kround;             // directions the current round's sample added
     int k1_round;           // basis columns when the current round began
     int sweeps;             // Jacobi sweeps the small SVD took
+    int trunc_round;        // a CholQR of this round dropped columns
     int prob;               // problem of the batch the tile belongs to
     int maxrank;            // the problem's maxrank and tol
     double tol;

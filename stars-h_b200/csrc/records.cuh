@@ -16,6 +16,9 @@ struct DevicePoints {
     DevKernel K{};
     std::vector<void *> owned;
     size_t h2d = 0;
+    // host coordinates the device copy was made from (for tile ordering)
+    const double *h_row = nullptr, *h_col = nullptr;
+    long long h_row_count = 0, h_col_count = 0;
     ~DevicePoints()
     {
         for (void *p : owned) cudaFree(p);

@@ -689,6 +689,7 @@ __global__ void k_round_setup(TileWork *__restrict__ tiles, int ntiles,
     }
     tw.bcur = min(block, tw.k - tw.cols_done);
     tw.k1_round = tw.k1;
+    tw.trunc_round = 0;
     atomicOr(active, 1);
 }
 
@@ -714,7 +715,8 @@ __global__ void k_round_end(TileWork *__restrict__ tiles, int ntiles,
     if (tw.bcur <= 0) return;
     tw.cols_done += tw.bcur;
     const int added = tw.k1 + tw.kb - tw.k1_round;
-    if (tw.kround == 0 || tw.cols_done >= tw.k || tw.bcur - added >= verify)
+    if (tw.kround == 0 || tw.cols_done >= tw.k ||
+        (tw.bcur - added >= verify && !tw.trunc_round))
         tw.done = 1;
     tw.k1 += tw.kb;       // (kb is 0 here: each pass merged its columns)
     tw.kb = 0;
@@ -777,21 +779,28 @@ k_chol_inv(TileWork *__restrict__ tiles, Workspace ws, int phase)
     double *T = ws.T(s);
     const int ld = ws.ldK();
     __shared__ double diag;
-    __shared__ int fail;
-    if (threadIdx.x == 0) fail = 0;
+    __shared__ int stop;
+    if (threadIdx.x == 0) stop = 0;
     __syncthreads();
+    int nn_ok = nn;
     for (int j = 0; j < nn; ++j) {
         if (threadIdx.x == 0) {
-            double acc = G[(size_t)j * ld + j];
+            const double gjj = G[(size_t)j * ld + j];
+            double acc = gjj;
             for (int l = 0; l < j; ++l) {
                 const double r = R[(size_t)j * ld + l];
                 acc -= r * r;
             }
-            if (!(acc > 0.0)) { fail = 1; acc = 1.0; }
-            diag = sqrt(acc);
+            // a column numerically inside the span of the previous ones:
+            // the factor keeps the columns before it (they come in
+            // decreasing pivot order) and the round may not finish the
+            // tile on its verification columns
+            if (!(acc > 1e-14 * gjj)) stop = 1;
+            diag = sqrt(fmax(acc, 0.0));
             R[(size_t)j * ld + j] = diag;
         }
         __syncthreads();
+        if (stop) { nn_ok = j; break; }
         const double rjj = diag;
         for (int c = j + 1 + threadIdx.x; c < nn; c += blockDim.x) {
             double acc = G[(size_t)c * ld + j];
@@ -801,9 +810,9 @@ k_chol_inv(TileWork *__restrict__ tiles, Workspace ws, int phase)
         }
         __syncthreads();
     }
-    for (int c = threadIdx.x; c < nn; c += blockDim.x) {
+    for (int c = threadIdx.x; c < nn_ok; c += blockDim.x) {
         double *x = T + (size_t)c * ld;
-        for (int a = c + 1; a < nn; ++a) x[a] = 0.0;
+        for (int a = c + 1; a < nn_ok; ++a) x[a] = 0.0;
         x[c] = 1.0 / R[(size_t)c * ld + c];
         for (int a = c - 1; a >= 0; --a) {
             double acc = 0.0;
@@ -811,7 +820,12 @@ k_chol_inv(TileWork *__restrict__ tiles, Workspace ws, int phase)
             x[a] = -acc / R[(size_t)a * ld + a];
         }
     }
-    if (threadIdx.x == 0 && fail) tw.status |= TILE_CHOL_FAIL;
+    if (threadIdx.x == 0 && nn_ok < nn) {
+        if (phase == PH_A) tw.k1 = nn_ok;
+        else tw.kb = nn_ok;
+        tw.trunc_round = 1;
+        tw.status |= TILE_CHOL_TRUNC;
+    }
 }
 
 void launch_chol_inv(int phase, TileWork *d_tiles, int ntiles, Workspace ws,
@@ -1116,8 +1130,9 @@ void launch_merge_basis(TileWork *d_tiles, int ntiles, cudaStream_t stream)
 
 // Energies e_c = ||C(c, :)||^2 of the rotated rows, order by decreasing
 // energy, then the smallest r >= 1 with
-//   sum_{c >= r} e_c + (||B||_F^2 - sum_c e_c)  <=  tol^2 ||B||_F^2,
-// i.e. starsh_dense_dsvfr applied to the exact energies (0 if B = 0).
+//   sum_{c >= r} e_c + tail_h + outside  <=  tol^2 ||D||_F^2,
+// i.e. starsh_dense_dsvfr applied to the exact energies plus the energy the
+// Gram factor (tail_h) and the sketch (outside) left out (0 if D = 0).
 // rank = r if r <= maxrank, else -1.
 __global__ void __launch_bounds__(kSmallThreads)
 k_rank_cut(TileWork *__restrict__ tiles, Workspace ws)
@@ -1161,14 +1176,26 @@ k_rank_cut(TileWork *__restrict__ tiles, Workspace ws)
             ge[c] = e[ord[c]];
             total += e[c];
         }
-        const double energy = tw.tr_h;
+        // With the block's exact ||D||_F^2 (dnorm2, from the generator) the
+        // energy outside the sketched basis, ||D||^2 - ||B||^2, is known
+        // too: it joins the tail, less an allowance for the rounding of the
+        // two sums, and the budget is tol^2 ||D||^2.  A block whose
+        // outside energy alone exceeds the budget cannot meet tol with its
+        // sketch: it is stored dense (rank -1), like a block above maxrank.
+        // Without dnorm2 (dense tiles given by the caller) the rule is the
+        // reference's: the tail of the projected block's spectrum against
+        // tol^2 ||B||^2.
+        const double dn = tw.dnorm2;
+        const double outside = dn > 0.0
+            ? fmax(0.0, dn - tw.tr_h - 2e-15 * dn) : 0.0;
+        const double energy = dn > 0.0 ? fmax(dn, tw.tr_h) : tw.tr_h;
         int r;
         if (!(energy > 0.0) || k2 == 0) {
-            r = 0;
+            r = outside <= tol * tol * energy ? 0 : -1;
         } else {
             const double budget = tol * tol * energy;
             // energy outside span(W): what the Gram factor left out
-            const double missing = fmax(0.0, tw.tail_h);
+            const double missing = fmax(0.0, tw.tail_h) + outside;
             // tail(r) for r = k2 down to 1; keep the smallest r that fits
             double tail = missing;
             r = -1;
@@ -1178,7 +1205,7 @@ k_rank_cut(TileWork *__restrict__ tiles, Workspace ws)
                 if (tail <= budget) r = c;
                 else break;
             }
-            if (r < 0) { r = k2; tw.status |= TILE_TAIL_LEFT; }
+            if (r < 0) tw.status |= TILE_TAIL_LEFT;
         }
         tw.rank = r <= maxrank ? r : -1;
     }

@@ -226,6 +226,8 @@ def _proto(lib):
                                        c_double, c_double]),
         "starsh_particles_generate": (c_int, [P(P(Particles)), STARSH_int,
                                               c_int, c_int]),
+        "starsh_particles_init": (c_int, [P(P(Particles)), STARSH_int, c_int,
+                                          P(c_double)]),
         "starsh_particles_zsort_inplace": (c_int, [P(Particles)]),
         "starsh_particles_free": (None, [P(Particles)]),
         "starsh_blrm_get_block": (c_int, [P(Blrm), STARSH_int, STARSH_int,

@@ -133,6 +133,16 @@ void fill_kernel(DevKernel &K, const b200_kspec &sp)
     K.diag = sp.diag;
     K.rad = sp.rad;
     K.reg = sp.reg;
+    K.inv_neg_beta = sp.beta != 0.0 ? -1.0 / sp.beta : 0.0;
+    K.inv_neg_2beta2 = sp.beta != 0.0 ? 1.0 / ((-2.0 * sp.beta) * sp.beta) : 0.0;
+    K.matern_half = 0;
+    if (sp.family == FAM_MATERN || sp.family == FAM_MATERN2) {
+        if (sp.family == FAM_MATERN2)
+            K.matern_scale = sp.beta != 0.0 ? 1.0 / sp.beta : 0.0;
+        if (sp.nu == 0.5) K.matern_half = 1;
+        else if (sp.nu == 1.5) K.matern_half = 2;
+        else if (sp.nu == 2.5) K.matern_half = 3;
+    }
 }
 
 // Uploads the point sets of a problem and the cluster pivots.

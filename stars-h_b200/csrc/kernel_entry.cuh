@@ -33,6 +33,9 @@ struct DevKernel {
     int zero_mode;    // Coulomb: r = 0 gives `diag` instead of 0
     double sigma, beta, nu, noise;
     double matern_coef, matern_scale;
+    int matern_half;          // 1, 2, 3 for nu = 1/2, 3/2, 5/2; else 0
+    double inv_neg_beta;      // -1/beta (exp)
+    double inv_neg_2beta2;    // 1/((-2 beta) beta) (square exponential)
     double wave_k, diag;
     double rad, reg;
     const double *row_pt;     // coordinates of the row point set
@@ -204,39 +207,44 @@ __device__ __forceinline__ double sq_dist(const DevKernel &K, long long ir,
     return dist;
 }
 
-// Entry value from the squared distance and the two point indices.
-__device__ __forceinline__ double entry_from_dist(const DevKernel &K,
-                                                  double dist, long long ir,
-                                                  long long jc)
+// Entry value from the squared distance and the two point indices, one
+// function per family (the tile generator picks the family once per CTA).
+// Divisions by a kernel constant are multiplications by its reciprocal,
+// computed once on the host (one rounding more than the reference's
+// division: a relative change of at most |argument| ulp in an exponential,
+// far below the 1e-13 the blocks are held to).
+template <int FAM>
+__device__ __forceinline__ double entry_fam(const DevKernel &K, double dist,
+                                            long long ir, long long jc)
 {
-    switch (K.family) {
-    case FAM_EXP: {
-        const double v = __ddiv_rn(sqrt(dist), -K.beta);
+    if constexpr (FAM == FAM_EXP) {
+        const double v = sqrt(dist) * K.inv_neg_beta;
         return v == 0.0 ? K.sigma + K.noise : K.sigma * exp(v);
-    }
-    case FAM_SQREXP: {
-        const double v = __ddiv_rn(dist, (-2.0 * K.beta) * K.beta);
+    } else if constexpr (FAM == FAM_SQREXP) {
+        const double v = dist * K.inv_neg_2beta2;
         return v == 0.0 ? K.sigma + K.noise : K.sigma * exp(v);
-    }
-    case FAM_MATERN:
-    case FAM_MATERN2: {
-        const double x = K.family == FAM_MATERN
-            ? __dmul_rn(sqrt(dist), K.matern_scale)
-            : __ddiv_rn(sqrt(dist), K.beta);
+    } else if constexpr (FAM == FAM_MATERN || FAM == FAM_MATERN2) {
+        const double x = sqrt(dist) * K.matern_scale;
         if (x == 0.0) return K.sigma + K.noise;
-        return K.matern_coef * pow(x, K.nu) * bessel_knu(K.nu, x);
-    }
-    case FAM_COULOMB:
+        // nu = 1/2, 3/2, 5/2: 2^(1-nu)/Gamma(nu) x^nu K_nu(x) is
+        // exp(-x) times 1, 1 + x, 1 + x + x^2/3 (K_{n+1/2} is elementary)
+        switch (K.matern_half) {
+        case 1: return K.sigma * exp(-x);
+        case 2: return K.sigma * ((1.0 + x) * exp(-x));
+        case 3: return K.sigma * ((1.0 + x * (1.0 + x * (1.0 / 3.0))) * exp(-x));
+        default: return K.matern_coef * pow(x, K.nu) * bessel_knu(K.nu, x);
+        }
+    } else if constexpr (FAM == FAM_COULOMB) {
         if (dist == 0.0) return K.zero_mode ? K.diag : 0.0;
         return __ddiv_rn(1.0, sqrt(dist));
-    case FAM_SIN:
-    case FAM_COS: {
+    } else if constexpr (FAM == FAM_SIN || FAM == FAM_COS) {
         if (dist == 0.0) return K.diag;
         const double r = sqrt(dist);
         const double a = K.wave_k * r;
-        return __ddiv_rn(K.family == FAM_SIN ? sin(a) : cos(a), r);
-    }
-    case FAM_RBF: {
+        return __ddiv_rn(FAM == FAM_SIN ? sin(a) : cos(a), r);
+    } else {
+        // the compactly supported bases amplify the rounding of x near
+        // x = 1, so x is the reference's quotient here
         const double x = __ddiv_rn(sqrt(dist), K.rad);
         double v;
         switch (K.rbf_kind) {
@@ -255,6 +263,21 @@ __device__ __forceinline__ double entry_from_dist(const DevKernel &K,
         if (K.isreg && (int)ir == (int)jc) v += K.reg;
         return v;
     }
+}
+
+__device__ __forceinline__ double entry_from_dist(const DevKernel &K,
+                                                  double dist, long long ir,
+                                                  long long jc)
+{
+    switch (K.family) {
+    case FAM_EXP: return entry_fam<FAM_EXP>(K, dist, ir, jc);
+    case FAM_SQREXP: return entry_fam<FAM_SQREXP>(K, dist, ir, jc);
+    case FAM_MATERN: return entry_fam<FAM_MATERN>(K, dist, ir, jc);
+    case FAM_MATERN2: return entry_fam<FAM_MATERN2>(K, dist, ir, jc);
+    case FAM_COULOMB: return entry_fam<FAM_COULOMB>(K, dist, ir, jc);
+    case FAM_SIN: return entry_fam<FAM_SIN>(K, dist, ir, jc);
+    case FAM_COS: return entry_fam<FAM_COS>(K, dist, ir, jc);
+    case FAM_RBF: return entry_fam<FAM_RBF>(K, dist, ir, jc);
     }
     return 0.0;
 }

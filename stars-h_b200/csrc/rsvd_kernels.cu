@@ -68,6 +68,35 @@ size_t workspace_layout(Workspace &w, int m_max, int n_max, int k_max,
 // sketch).
 constexpr int kStageDim = 4;
 
+// The entries of one thread in a 64 x 64 block: rows ii, columns jj0,
+// jj0 + 4, ... below jn, written to Dcol[jj * ld] (Dcol points at row ii of
+// the block's first column); returns their sum of squares.
+template <int FAM>
+__device__ __forceinline__ double gen_entries(
+    const DevKernel &K, bool staged, const double (*rc)[64],
+    const double (*cc)[64], const long long *ri, const long long *ci, int ii,
+    int jj0, int jn, double *Dcol, int ld)
+{
+    double ss = 0.0;
+    #pragma unroll 4
+    for (int jj = jj0; jj < jn; jj += 4) {
+        double dist;
+        if (staged) {
+            dist = 0.0;
+            for (int d = 0; d < K.ndim; ++d) {
+                const double q = __dsub_rn(rc[d][ii], cc[d][jj]);
+                dist = __dadd_rn(dist, __dmul_rn(q, q));
+            }
+        } else {
+            dist = sq_dist(K, ri[ii], ci[jj]);
+        }
+        const double v = entry_fam<FAM>(K, dist, ri[ii], ci[jj]);
+        Dcol[(size_t)jj * ld] = v;
+        ss += v * v;
+    }
+    return ss;
+}
+
 __global__ void __launch_bounds__(256)
 k_gen_tiles(const DevKernel *__restrict__ kernels,
             const TileWork *__restrict__ tiles, Workspace ws)
@@ -105,22 +134,31 @@ k_gen_tiles(const DevKernel *__restrict__ kernels,
     const int ld = ws.ldD();
     double ss = 0.0;
     if (i < tw.m) {
-        for (int c = 0; c < 16; ++c) {
-            const int jj = (t >> 6) + 4 * c, j = j0 + jj;
-            if (j >= tw.n) break;
-            double v;
-            if (staged) {
-                double dist = 0.0;
-                for (int d = 0; d < K.ndim; ++d) {
-                    const double q = __dsub_rn(rc[d][ii], cc[d][jj]);
-                    dist = __dadd_rn(dist, __dmul_rn(q, q));
-                }
-                v = entry_from_dist(K, dist, ri[ii], ci[jj]);
-            } else {
-                v = entry_from_dist(K, sq_dist(K, ri[ii], ci[jj]), ri[ii], ci[jj]);
-            }
-            D[(size_t)j * ld + i] = v;
-            ss += v * v;
+        const int jn = min(64, tw.n - j0);
+        switch (K.family) {
+        case FAM_EXP:
+            ss = gen_entries<FAM_EXP>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld);
+            break;
+        case FAM_SQREXP:
+            ss = gen_entries<FAM_SQREXP>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld);
+            break;
+        case FAM_MATERN:
+            ss = gen_entries<FAM_MATERN>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld);
+            break;
+        case FAM_MATERN2:
+            ss = gen_entries<FAM_MATERN2>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld);
+            break;
+        case FAM_COULOMB:
+            ss = gen_entries<FAM_COULOMB>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld);
+            break;
+        case FAM_SIN:
+            ss = gen_entries<FAM_SIN>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld);
+            break;
+        case FAM_COS:
+            ss = gen_entries<FAM_COS>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld);
+            break;
+        default:
+            ss = gen_entries<FAM_RBF>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld);
         }
     }
     #pragma unroll

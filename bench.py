@@ -842,11 +842,14 @@ def main():
         barrier()
         err = lib.starsh_blrm__dfe_b200(M)
         if keep:
+            step_times.append(times)
             return statistics.mean(times), sts, err, (M, F)
         free(M, F)
+        step_times.append(times)
         return statistics.mean(times), sts, err, None
 
     clocks = ClockSampler(local)
+    step_times = []
     t_dev, sts, err, kept = measure(chosen, clocks, keep=bool(wl.get("dmml_nrhs")))
     last = sts[-1]
     if chosen != sb.ENGINE_FP64:
@@ -943,6 +946,7 @@ def main():
                    "max_rank": last.max_rank,
                    "sketch_columns_per_tile": last.sketch_flops / max(1.0, 2.0 * last.tiles * wl["nb"] ** 2)},
         "rel_err": err, "tol": wl["tol"], "accepted": accepted,
+        "step_ms": [round(t * 1e3, 2) for t in step_times[0]],
         "plain_fp64": {"value": plain_value, "ms_per_step": t_plain * 1e3,
                        "rel_err": err_plain,
                        "chosen_over_plain": value / plain_value},

@@ -36,6 +36,14 @@ struct Context {
 // Initialises (once) and returns the context; nullptr if no usable GPU.
 Context *context();
 
+// Stream-ordered device allocation from the device's memory pool, whose
+// freed memory stays cached for the next call (repeated approximations do
+// not go back to the driver, which can stall the stream for a long time).
+// pool_alloc returns nullptr on failure; pool_free releases on the
+// library stream.
+void *pool_alloc(size_t bytes, cudaStream_t s);
+void pool_free(void *p);
+
 // Records a CUDA error (with the call site) as the library's last error and
 // returns the matching STARSH error code.
 int cuda_fail(cudaError_t err, const char *what);

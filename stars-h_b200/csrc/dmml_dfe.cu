@@ -156,10 +156,10 @@ static int ensure_record(STARSH_blrm *M, Context &ctx, Record **out)
         for (STARSH_int b = 0; b < F->nblocks_near; ++b) nd += M->near_D[b]->size;
     double *chunk = nullptr;
     if (nu + nv + nd > 0) {
-        cudaError_t e = cudaMalloc(&chunk, (nu + nv + nd) * sizeof(double));
-        if (e != cudaSuccess) {
+        chunk = (double *)pool_alloc((nu + nv + nd) * sizeof(double), s);
+        if (chunk == nullptr) {
             delete rec;
-            return cuda_fail(e, "cudaMalloc(uploaded factors)");
+            return cuda_fail(cudaErrorMemoryAllocation, "uploaded factors");
         }
         rec->chunks.push_back(chunk);
     }

@@ -86,6 +86,14 @@ Context *context()
             set_error("cudaStreamCreate failed");
             return;
         }
+        // keep freed pool memory cached in the process
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+            uint64_t keep = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold,
+                                    &keep);
+        }
+        cudaGetLastError();
         g_ctx_ok = true;
     });
     if (!g_ctx_ok) return nullptr;
@@ -94,6 +102,21 @@ Context *context()
     if (cudaGetDevice(&cur) != cudaSuccess || cur != g_ctx.device)
         cudaSetDevice(g_ctx.device);
     return &g_ctx;
+}
+
+void *pool_alloc(size_t bytes, cudaStream_t s)
+{
+    void *p = nullptr;
+    if (cudaMallocAsync(&p, bytes ? bytes : 8, s) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return p;
+}
+
+void pool_free(void *p)
+{
+    if (p) cudaFreeAsync(p, g_ctx.stream);
 }
 
 void set_error(const std::string &msg)
@@ -637,10 +660,12 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
         }
         std::shared_ptr<void> chunk;
         if (total > 0) {
-            void *raw = nullptr;
-            B200_CUDA(cudaMalloc(&raw, total * sizeof(double)),
-                      "cudaMalloc(factors)");
-            chunk = std::shared_ptr<void>(raw, [](void *q) { cudaFree(q); });
+            void *raw = pool_alloc(total * sizeof(double), s);
+            if (raw == nullptr) {
+                info = cuda_fail(cudaErrorMemoryAllocation, "factor chunk");
+                break;
+            }
+            chunk = std::shared_ptr<void>(raw, [](void *q) { pool_free(q); });
         }
         double *base = (double *)chunk.get();
         std::vector<size_t> cu(u0), cv(v0);
@@ -950,11 +975,9 @@ static int finish_problem(ProblemJob &jb, int flags, cudaStream_t s,
         for (STARSH_int b = 0; b < near; ++b)
             total += (size_t)R->size[F->block_near[2 * b]] *
                      C->size[F->block_near[2 * b + 1]];
-        double *dD = nullptr;
-        cudaError_t e = cudaMalloc(&dD, total * sizeof(double));
-        if (e != cudaSuccess) {
-            return cuda_fail(e, "cudaMalloc(near blocks)");
-        }
+        double *dD = (double *)pool_alloc(total * sizeof(double), s);
+        if (dD == nullptr)
+            return cuda_fail(cudaErrorMemoryAllocation, "near blocks");
         rec->chunks.push_back(dD);
         rec->d_total = total;
         std::vector<BlockJob> jobs;
@@ -1197,8 +1220,10 @@ extern "C" void starsh_b200_blrm_release(STARSH_blrm *matrix)
         rec = it->second;
         g_records.erase(it);
     }
+    // the factors may still be read by work on any stream (a device dmml
+    // on the caller's stream): wait for the device, then free
     Context *ctx = context();
-    if (ctx) cudaStreamSynchronize(ctx->stream);
+    if (ctx) cudaDeviceSynchronize();
     delete rec;
 }
 

@@ -21,13 +21,14 @@ struct DevicePoints {
     long long h_row_count = 0, h_col_count = 0;
     ~DevicePoints()
     {
-        for (void *p : owned) cudaFree(p);
+        for (void *p : owned) pool_free(p);
     }
     int upload(const void *host, size_t bytes, const void **dev,
                cudaStream_t s)
     {
-        void *d = nullptr;
-        B200_CUDA(cudaMalloc(&d, bytes ? bytes : 8), "cudaMalloc(points)");
+        void *d = pool_alloc(bytes, s);
+        if (d == nullptr)
+            return cuda_fail(cudaErrorMemoryAllocation, "points");
         owned.push_back(d);
         if (bytes)
             B200_CUDA(cudaMemcpyAsync(d, host, bytes, cudaMemcpyHostToDevice, s),
@@ -60,7 +61,7 @@ struct Record {
     DevicePoints *points = nullptr;    // kept for onfly near blocks
     ~Record()
     {
-        for (void *p : chunks) cudaFree(p);
+        for (void *p : chunks) pool_free(p);
         delete points;
     }
 };

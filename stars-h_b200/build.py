@@ -62,8 +62,14 @@ def build(force=False):
     os.makedirs(OBJ, exist_ok=True)
     c, cu = _sources()
     hdr_time = _headers_mtime()
-    with cf.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
-        objs = list(ex.map(lambda s: _compile(s, force, hdr_time), c + cu))
+    try:
+        with cf.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
+            objs = list(ex.map(lambda s: _compile(s, force, hdr_time), c + cu))
+    except RuntimeError:
+        # no stale library may outlive a failed build
+        if os.path.exists(LIB):
+            os.remove(LIB)
+        raise
     if (not force and os.path.exists(LIB)
             and os.path.getmtime(LIB) > max(os.path.getmtime(o) for o in objs)):
         return LIB

@@ -1,7 +1,7 @@
 // Batched FP64 GEMM (see gemm_f64.cuh).
 //
-// CTA tile 64 x 64, K step 16, 8 warps in a 2 (M) x 4 (N) grid, warp tile
-// 32 x 16 = 4 x 2 fragments of the m8n8k4 DMMA.  Operand tiles are staged
+// CTA tile 64 x 64, 32 x 128 or 128 x 32, K step 16, 8 warps of 32 x 16
+// output each (4 x 2 fragments of the m8n8k4 DMMA).  Operand tiles are staged
 // in shared memory as [row][k] (A) and [col][k] (B) with row stride 20,
 // double-buffered, the next K tile is fetched into registers while the
 // current one is multiplied.  Global loads are coalesced along whichever
@@ -20,24 +20,33 @@ __device__ __forceinline__ void dmma_8x8x4(double &c0, double &c1, double a,
         : "d"(a), "d"(b));
 }
 
-template <bool TA, bool TB>
+template <bool TA, bool TB, int BM, int BN>
 __global__ void __launch_bounds__(kGemmThreads)
 k_gemm_f64(const GemmDesc *__restrict__ descs, int tiles_n)
 {
+    // 8 warps of 32 x 16 output each, BM / 32 along M and BN / 16 along N
+    constexpr int WARPS_M = BM / 32;
+    static_assert(WARPS_M * (BN / 16) == kGemmThreads / 32, "warp grid");
+    constexpr int RA = BM * kGemmBK / kGemmThreads;   // A loads per thread
+    constexpr int RB = BN * kGemmBK / kGemmThreads;   // B loads per thread
     const GemmDesc d = descs[blockIdx.y];
     const int tm = blockIdx.x / tiles_n;
     const int tn = blockIdx.x % tiles_n;
-    const int m0 = tm * kGemmBM, n0 = tn * kGemmBN;
+    const int m0 = tm * BM, n0 = tn * BN;
     if (m0 >= d.M || n0 >= d.N) return;
 
-    __shared__ double As[2][kGemmBM * kGemmLds];
-    __shared__ double Bs[2][kGemmBN * kGemmLds];
+    // [2][BM * kGemmLds] then [2][BN * kGemmLds], dynamic (above 48 KB
+    // for the 32 x 128 and 128 x 32 shapes)
+    extern __shared__ double gemm_smem[];
+    double (*As)[BM * kGemmLds] = reinterpret_cast<double (*)[BM * kGemmLds]>(gemm_smem);
+    double (*Bs)[BN * kGemmLds] =
+        reinterpret_cast<double (*)[BN * kGemmLds]>(gemm_smem + 2 * BM * kGemmLds);
 
     const int t = threadIdx.x;
     const int lane = t & 31, warp = t >> 5;
     const int g = lane >> 2, tig = lane & 3;
-    const int wm = (warp & 1) * 32;   // warp row offset in the CTA tile
-    const int wn = (warp >> 1) * 16;  // warp column offset
+    const int wm = (warp % WARPS_M) * 32;   // warp row offset in the CTA tile
+    const int wn = (warp / WARPS_M) * 16;   // warp column offset
 
     double acc[4][2][2];
     #pragma unroll
@@ -45,15 +54,25 @@ k_gemm_f64(const GemmDesc *__restrict__ descs, int tiles_n)
         #pragma unroll
         for (int j = 0; j < 2; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 
-    double ra[4], rb[4];
-    // Element coordinates this thread loads, per register slot r:
-    //   A: (row am + ..., k ak + ...), B: (col bn + ..., k bk + ...).
+    double ra[RA], rb[RB];
+    // Element e = t + 256 r of a tile, laid out along whichever dimension
+    // is contiguous in global memory (coalesced loads):
+    //   A: !TA rows fastest, TA k fastest;  B: !TB k fastest, TB cols fastest.
+    auto a_coord = [&](int r, int &row, int &kk) {
+        const int e = t + kGemmThreads * r;
+        if (!TA) { row = e % BM; kk = e / BM; }
+        else     { kk = e % kGemmBK; row = e / kGemmBK; }
+    };
+    auto b_coord = [&](int r, int &col, int &kk) {
+        const int e = t + kGemmThreads * r;
+        if (!TB) { kk = e % kGemmBK; col = e / kGemmBK; }
+        else     { col = e % BN; kk = e / BN; }
+    };
     auto load_tiles = [&](int k0) {
         #pragma unroll
-        for (int r = 0; r < 4; ++r) {
+        for (int r = 0; r < RA; ++r) {
             int row, kk;
-            if (!TA) { row = t & 63; kk = (t >> 6) + 4 * r; }
-            else     { kk = t & 15; row = (t >> 4) + 16 * r; }
+            a_coord(r, row, kk);
             const int gm = m0 + row, gk = k0 + kk;
             double v = 0.0;
             if (gm < d.M && gk < d.K)
@@ -62,10 +81,9 @@ k_gemm_f64(const GemmDesc *__restrict__ descs, int tiles_n)
             ra[r] = v;
         }
         #pragma unroll
-        for (int r = 0; r < 4; ++r) {
+        for (int r = 0; r < RB; ++r) {
             int col, kk;
-            if (!TB) { kk = t & 15; col = (t >> 4) + 16 * r; }
-            else     { col = t & 63; kk = (t >> 6) + 4 * r; }
+            b_coord(r, col, kk);
             const int gn = n0 + col, gk = k0 + kk;
             double v = 0.0;
             if (gn < d.N && gk < d.K)
@@ -76,17 +94,15 @@ k_gemm_f64(const GemmDesc *__restrict__ descs, int tiles_n)
     };
     auto store_tiles = [&](int buf) {
         #pragma unroll
-        for (int r = 0; r < 4; ++r) {
+        for (int r = 0; r < RA; ++r) {
             int row, kk;
-            if (!TA) { row = t & 63; kk = (t >> 6) + 4 * r; }
-            else     { kk = t & 15; row = (t >> 4) + 16 * r; }
+            a_coord(r, row, kk);
             As[buf][row * kGemmLds + kk] = ra[r];
         }
         #pragma unroll
-        for (int r = 0; r < 4; ++r) {
+        for (int r = 0; r < RB; ++r) {
             int col, kk;
-            if (!TB) { kk = t & 15; col = (t >> 4) + 16 * r; }
-            else     { col = t & 63; kk = (t >> 6) + 4 * r; }
+            b_coord(r, col, kk);
             Bs[buf][col * kGemmLds + kk] = rb[r];
         }
     };
@@ -141,25 +157,44 @@ k_gemm_f64(const GemmDesc *__restrict__ descs, int tiles_n)
     }
 }
 
+template <int BM, int BN>
+static void launch_shape(bool ta, bool tb, const GemmDesc *dd, int nb,
+                         int tiles_m, int tiles_n, cudaStream_t stream)
+{
+    dim3 grid(tiles_m * tiles_n, nb);
+    const size_t smem = 2 * (size_t)(BM + BN) * kGemmLds * sizeof(double);
+    auto go = [&](auto fn) {
+        if (smem > 48 * 1024)
+            cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem);
+        fn<<<grid, kGemmThreads, smem, stream>>>(dd, tiles_n);
+    };
+    if (!ta && !tb) go(k_gemm_f64<false, false, BM, BN>);
+    else if (ta && !tb) go(k_gemm_f64<true, false, BM, BN>);
+    else if (!ta && tb) go(k_gemm_f64<false, true, BM, BN>);
+    else go(k_gemm_f64<true, true, BM, BN>);
+}
+
 cudaError_t gemm_f64_batched(bool ta, bool tb, const GemmDesc *d_desc,
                              int batch, int max_m, int max_n,
                              cudaStream_t stream)
 {
     if (batch <= 0 || max_m <= 0 || max_n <= 0) return cudaSuccess;
-    const int tiles_m = (max_m + kGemmBM - 1) / kGemmBM;
-    const int tiles_n = (max_n + kGemmBN - 1) / kGemmBN;
+    // CTA shape: 64 x 64, or 32 x 128 when the output is wide and (as for
+    // the projection B = Q^T D and the rotation C = W^T B) its rows are a
+    // basis much narrower than the batch maximum, or 128 x 32 for narrow
+    // outputs (sketch blocks of 32 columns)
+    int bm = 64, bn = 64;
+    if (ta && !tb && max_n >= 256) { bm = 32; bn = 128; }
+    else if (max_n <= 32 && max_m >= 128) { bm = 128; bn = 32; }
+    const int tiles_m = (max_m + bm - 1) / bm;
+    const int tiles_n = (max_n + bn - 1) / bn;
     for (int b0 = 0; b0 < batch; b0 += 65535) {
         const int nb = batch - b0 < 65535 ? batch - b0 : 65535;
-        dim3 grid(tiles_m * tiles_n, nb);
         const GemmDesc *dd = d_desc + b0;
-        if (!ta && !tb)
-            k_gemm_f64<false, false><<<grid, kGemmThreads, 0, stream>>>(dd, tiles_n);
-        else if (ta && !tb)
-            k_gemm_f64<true, false><<<grid, kGemmThreads, 0, stream>>>(dd, tiles_n);
-        else if (!ta && tb)
-            k_gemm_f64<false, true><<<grid, kGemmThreads, 0, stream>>>(dd, tiles_n);
-        else
-            k_gemm_f64<true, true><<<grid, kGemmThreads, 0, stream>>>(dd, tiles_n);
+        if (bm == 32) launch_shape<32, 128>(ta, tb, dd, nb, tiles_m, tiles_n, stream);
+        else if (bm == 128) launch_shape<128, 32>(ta, tb, dd, nb, tiles_m, tiles_n, stream);
+        else launch_shape<64, 64>(ta, tb, dd, nb, tiles_m, tiles_n, stream);
     }
     return cudaGetLastError();
 }

@@ -29,6 +29,8 @@ struct Context {
     void *stage[2] = {nullptr, nullptr};     // pinned D2H staging buffers
     cudaEvent_t stage_ev[2] = {nullptr, nullptr};
     DeviceBuffer kernels;      // DevKernel table of a batch's problems
+    DeviceBuffer omega8;       // int8 sketch matrix of the adaptive engine
+    int omega8_rows = 0, omega8_cols = 0, omega8_ld = 0;
     int omega_rows = 0, omega_cols = 0;   // shape Omega was generated for
     std::mutex lock;           // one approximation / dmml at a time
 };

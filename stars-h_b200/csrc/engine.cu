@@ -407,6 +407,27 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
         ctx.omega_cols = k_max;
     }
     const double *omega = (const double *)ctx.omega.ptr;
+    // the adaptive engine's int8 sketch matrix (tensor-core sketch)
+    bool use_i8 = ep.engine == STARSH_B200_MIXED &&
+                  sketch_i8_fits(std::max(ep.block, ep.block_next), n_max);
+    if (const char *e = getenv("STARSH_B200_SKETCH"))
+        if (strcmp(e, "dmma") == 0) use_i8 = false;
+    const int ld_om8 = (n_max + 63) / 64 * 64;
+    if (use_i8 && (ctx.omega8_rows != n_max || ctx.omega8_cols != k_max ||
+                   ctx.omega8_ld != ld_om8)) {
+        if (!ctx.omega8.reserve((size_t)ld_om8 * k_max))
+            return cuda_fail(cudaErrorMemoryAllocation, "omega8");
+        launch_gaussian_i8((int8_t *)ctx.omega8.ptr, n_max, k_max, ld_om8,
+                           kOmegaSeed, s);
+        count_launch();
+        ctx.omega8_rows = n_max;
+        ctx.omega8_cols = k_max;
+        ctx.omega8_ld = ld_om8;
+    }
+    const int8_t *om8 = (const int8_t *)ctx.omega8.ptr;
+    const int k_max_all = k_max;   // Omega8's width (batches shadow k_max)
+    // E[w^2] of the sketch entries: round(32 g) has variance 1024 + 1/12
+    for (TileWork &t : all) t.omega_var = use_i8 ? 1024.0 + 1.0 / 12.0 : 1.0;
 
     // Processing order: larger tiles first (a batch's workspace layout is
     // sized by its first tile), then by sketch width, then by cluster
@@ -583,7 +604,14 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
             if (!active) break;
             const int bmax = std::min(block, k_max);
             cudaEventRecord(ev[0], s);
-            if ((info = gemm(STEP_A_SKETCH, false, false, nt, m_max, bmax, none))) break;
+            if (use_i8) {
+                launch_sketch_i8(dt, nt, ws, om8, ld_om8, k_max_all, bmax, s);
+                count_launch();
+                const cudaError_t ce = cudaGetLastError();
+                if (ce != cudaSuccess) { info = cuda_fail(ce, "k_sketch_i8"); break; }
+            } else if ((info = gemm(STEP_A_SKETCH, false, false, nt, m_max, bmax, none))) {
+                break;
+            }
             cudaEventRecord(ev[1], s);
             if (round > 0) {
                 if ((info = gemm(STEP_A_RES_Z, true, false, nt, k_max, bmax, none))) break;
@@ -644,6 +672,10 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
             st.sketch_flops += 2.0 * w.m * w.n *
                 (ep.engine == STARSH_B200_FP64 ? w.k : w.cols_done);
             st.project_flops += 2.0 * w.m * w.n * w.k1;
+            if (w.status & TILE_MMA_TIMEOUT) {
+                set_error("tensor-core sketch timed out on a tile");
+                info = STARSH_UNKNOWN_ERROR;
+            }
             jobs[w.prob].rank[owner[b0 + t].second] = w.rank;
             if (w.rank > 0) {
                 nu[w.prob] += (size_t)w.m * w.rank;

@@ -1,6 +1,7 @@
 // Shared definitions of the batched randomized-SVD engine: per-tile state,
 // workspace layout and the launchers of the per-tile kernels.
 #pragma once
+#include <cstdint>
 #include <cuda_runtime.h>
 #include "gemm_f64.cuh"
 #include "kernel_entry.cuh"
@@ -13,6 +14,7 @@ enum : int {
     TILE_CHOL_TRUNC = 1,   // a re-orthogonalisation dropped dependent columns
     TILE_JACOBI_SLOW = 2,  // Jacobi sweeps hit their cap
     TILE_TAIL_LEFT = 4,    // energy outside the factors alone exceeds tol
+    TILE_MMA_TIMEOUT = 8,  // a tensor-core wait of the sketch gave up
 };
 
 // One far-field tile of a batch.
@@ -38,6 +40,7 @@ struct TileWork {
     int k1_round;           // basis columns when the current round began
     int sweeps;             // Jacobi sweeps the small SVD took
     int trunc_round;        // a CholQR of this round dropped columns
+    double omega_var;       // variance of the sketch matrix's entries
     int prob;               // problem of the batch the tile belongs to
     int maxrank;            // the problem's maxrank and tol
     double tol;
@@ -50,7 +53,7 @@ struct Workspace {
     double *base;
     size_t stride;          // doubles per slot
     int m_max, n_max, k_max;
-    size_t oD, oY, oQ1, oQ, oS, oL, oT, oB, oC, oE, oSig, oPiv, oOrd, oNrm, oR;
+    size_t oD, oY, oQ1, oQ, oS, oL, oT, oB, oC, oE, oSig, oPiv, oOrd, oNrm, oR, oRmx;
 
     __host__ __device__ double *D(int s) const { return base + s * stride + oD; }
     __host__ __device__ double *Y(int s) const { return base + s * stride + oY; }
@@ -63,6 +66,8 @@ struct Workspace {
     __host__ __device__ double *C(int s) const { return base + s * stride + oC; }
     __host__ __device__ double *E(int s) const { return base + s * stride + oE; }
     __host__ __device__ double *Sig(int s) const { return base + s * stride + oSig; }
+    // per row, per 64-column block: the largest |D_ij| (ld (n_max+63)/64)
+    __host__ __device__ double *Rmx(int s) const { return base + s * stride + oRmx; }
     __host__ __device__ int *Piv(int s) const { return (int *)(base + s * stride + oPiv); }
     __host__ __device__ int *Ord(int s) const { return (int *)(base + s * stride + oOrd); }
     // per-CTA partial sums of squares of the generated block
@@ -153,6 +158,19 @@ void launch_select_w(const TileWork *d_tiles, int ntiles, Workspace ws,
                      cudaStream_t stream);
 void launch_write_v(const TileWork *d_tiles, int ntiles, Workspace ws,
                     OutArena out, cudaStream_t stream);
+// Adaptive sketch on the tensor cores (int8 digits of D, see
+// sketch_i8.cu): Y(:, 0:bcur) = D Omega8(:, cols_done + (0:ncols)) for
+// every tile with an active round.  sketch_i8_fits() tells whether a batch
+// shape is supported (ncols <= 64, n_max <= 8192, shared memory).
+bool sketch_i8_fits(int ncols, int n_max);
+void launch_sketch_i8(const TileWork *d_tiles, int ntiles, Workspace ws,
+                      const int8_t *om8, int ld_om8, int om8_cols, int ncols,
+                      cudaStream_t stream);
+// Omega8(j, c) = clip(round(32 g), -127, 127), g the Gaussian of
+// launch_gaussian's (j, c); rows past `rows` up to ld are zero.
+void launch_gaussian_i8(int8_t *d_om8, int rows, int cols, int ld,
+                        unsigned long long seed, cudaStream_t stream);
+
 // Omega(j, c) for j < rows, c < cols into column-major storage with leading
 // dimension ld; entry (j, c) depends only on (j, c) and the seed, not on
 // the storage shape.

@@ -37,7 +37,8 @@ constexpr size_t slot_doubles(size_t m, size_t n, size_t k)
 {
     return round32(m * n) + 3 * round32(m * k) + 3 * round32(k * k) +
            2 * round32(k * n) + 2 * round32(k) + 2 * round32((k + 1) / 2) +
-           round32(((m + 63) / 64) * ((n + 63) / 64)) + round32(m * k);
+           round32(((m + 63) / 64) * ((n + 63) / 64)) + round32(m * k) +
+           round32(m * ((n + 63) / 64));
 }
 constexpr size_t kSlotDoubles =
     slot_doubles(kNoAllocMaxDim, kNoAllocMaxDim, kNoAllocMaxK);

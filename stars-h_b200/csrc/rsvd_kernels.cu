@@ -52,6 +52,7 @@ size_t workspace_layout(Workspace &w, int m_max, int n_max, int k_max,
     w.oOrd = take((k_max + 1) / 2);
     w.oNrm = take((size_t)((m_max + 63) / 64) * ((n_max + 63) / 64));
     w.oR = take((size_t)m_max * k_max);
+    w.oRmx = take((size_t)m_max * ((n_max + 63) / 64));
     w.stride = o;
     return o;
 }
@@ -75,9 +76,10 @@ template <int FAM>
 __device__ __forceinline__ double gen_entries(
     const DevKernel &K, bool staged, const double (*rc)[64],
     const double (*cc)[64], const long long *ri, const long long *ci, int ii,
-    int jj0, int jn, double *Dcol, int ld)
+    int jj0, int jn, double *Dcol, int ld, double &amax)
 {
     double ss = 0.0;
+    amax = 0.0;
     #pragma unroll 4
     for (int jj = jj0; jj < jn; jj += 4) {
         double dist;
@@ -93,6 +95,7 @@ __device__ __forceinline__ double gen_entries(
         const double v = entry_fam<FAM>(K, dist, ri[ii], ci[jj]);
         Dcol[(size_t)jj * ld] = v;
         ss += v * v;
+        amax = fmax(amax, fabs(v));
     }
     return ss;
 }
@@ -132,39 +135,46 @@ k_gen_tiles(const DevKernel *__restrict__ kernels,
     const int ii = t & 63, i = i0 + ii;
     double *D = ws.D(tw.slot);
     const int ld = ws.ldD();
-    double ss = 0.0;
+    double ss = 0.0, amax = 0.0;
     if (i < tw.m) {
         const int jn = min(64, tw.n - j0);
         switch (K.family) {
         case FAM_EXP:
-            ss = gen_entries<FAM_EXP>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld);
+            ss = gen_entries<FAM_EXP>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld, amax);
             break;
         case FAM_SQREXP:
-            ss = gen_entries<FAM_SQREXP>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld);
+            ss = gen_entries<FAM_SQREXP>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld, amax);
             break;
         case FAM_MATERN:
-            ss = gen_entries<FAM_MATERN>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld);
+            ss = gen_entries<FAM_MATERN>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld, amax);
             break;
         case FAM_MATERN2:
-            ss = gen_entries<FAM_MATERN2>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld);
+            ss = gen_entries<FAM_MATERN2>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld, amax);
             break;
         case FAM_COULOMB:
-            ss = gen_entries<FAM_COULOMB>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld);
+            ss = gen_entries<FAM_COULOMB>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld, amax);
             break;
         case FAM_SIN:
-            ss = gen_entries<FAM_SIN>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld);
+            ss = gen_entries<FAM_SIN>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld, amax);
             break;
         case FAM_COS:
-            ss = gen_entries<FAM_COS>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld);
+            ss = gen_entries<FAM_COS>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld, amax);
             break;
         default:
-            ss = gen_entries<FAM_RBF>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld);
+            ss = gen_entries<FAM_RBF>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld, amax);
         }
     }
+    // largest |D_ij| of each row of the sub-block (for the int8 sketch's
+    // row scales): the four threads of a row combine through shared memory
+    __shared__ double rmx[4][64];
+    rmx[t >> 6][ii] = amax;
     #pragma unroll
     for (int o = 16; o > 0; o >>= 1) ss += __shfl_down_sync(0xffffffffu, ss, o);
     if ((t & 31) == 0) red[t >> 5] = ss;
     __syncthreads();
+    if (t < 64 && i0 + t < tw.m)
+        ws.Rmx(tw.slot)[(size_t)(i0 + t) * ((ws.n_max + 63) / 64) + blockIdx.y] =
+            fmax(fmax(rmx[0][t], rmx[1][t]), fmax(rmx[2][t], rmx[3][t]));
     if (t == 0) {
         double a = 0.0;
         for (int w = 0; w < 8; ++w) a += red[w];
@@ -232,6 +242,41 @@ void launch_gaussian(double *d_omega, int rows, int cols, int ld,
     const int pairs = (rows + 1) / 2;
     dim3 grid((pairs + 255) / 256, cols);
     k_gaussian<<<grid, 256, 0, stream>>>(d_omega, rows, cols, ld, seed);
+}
+
+// Omega8(j, c) = clip(round(32 g(j, c)), -127, 127) with g the Gaussian of
+// k_gaussian for the same (j, c); rows rows .. ld - 1 are zero.
+__global__ void k_gaussian_i8(int8_t *out, int rows, int cols, int ld,
+                              unsigned long long seed)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    const int col = blockIdx.y;
+    if (2 * q >= ld || col >= cols) return;
+    const uint4 c = make_uint4((unsigned)q, (unsigned)col, 0u, 0u);
+    const uint4 r = philox4x32_10(c, make_uint2((unsigned)seed,
+                                                (unsigned)(seed >> 32)));
+    const unsigned long long b1 = ((unsigned long long)r.x << 32) | r.y;
+    const unsigned long long b2 = ((unsigned long long)r.z << 32) | r.w;
+    const double u1 = ((b1 >> 11) + 1) * 0x1.0p-53;
+    const double u2 = (b2 >> 11) * 0x1.0p-53;
+    const double rad = sqrt(-2.0 * log(u1));
+    double s, co;
+    sincospi(2.0 * u2, &s, &co);
+    int8_t *o = out + (size_t)col * ld;
+    auto q8 = [](double g) {
+        return (int8_t)fmax(-127.0, fmin(127.0, rint(32.0 * g)));
+    };
+    o[2 * q] = 2 * q < rows ? q8(rad * co) : (int8_t)0;
+    if (2 * q + 1 < ld) o[2 * q + 1] = 2 * q + 1 < rows ? q8(rad * s) : (int8_t)0;
+}
+
+void launch_gaussian_i8(int8_t *d_om8, int rows, int cols, int ld,
+                        unsigned long long seed, cudaStream_t stream)
+{
+    if (cols <= 0 || ld <= 0) return;
+    const int pairs = (ld + 1) / 2;
+    dim3 grid((pairs + 255) / 256, cols);
+    k_gaussian_i8<<<grid, 256, 0, stream>>>(d_om8, rows, cols, ld, seed);
 }
 
 // ------------------------------------------------- GEMM descriptors
@@ -600,12 +645,18 @@ k_pivchol(TileWork *__restrict__ tiles, Workspace ws, int phase)
         // ||(I - Q Q^T) D||_F^2: keep directions above (tol/10)^2 ||D||_F^2.
         // When the squared-noise floor of this Gram hides part of that
         // range, the same sample is projected and searched once more.
+        // (E||r_i||^2 carries the variance of Omega's entries: 1 for the
+        // Gaussian, about 32^2 for the int8 sketch matrix)
         const double noise = 1e-15 * dmax;
-        const double floor_ = 0.01 * tol * tol * tw.dnorm2;
+        const double var = tw.omega_var > 0.0 ? tw.omega_var : 1.0;
+        const double floor_ = 0.01 * tol * tol * tw.dnorm2 * var;
         thr = fmax(noise, floor_);
         cap = min(nn, tw.k - tw.k1);
+        // a repeat pass only where (tol/10)^2 lies below the squared-noise
+        // floor at all (the same decision alone or in any batch)
         if (threadIdx.x == 0)
-            tw.need_pass_b = phase == PH_R && noise > floor_;
+            tw.need_pass_b = phase == PH_R && noise > floor_ &&
+                             0.01 * tol * tol < 1e-15;
     } else {
         thr = 1e-18 * dmax;
         if (threadIdx.x == 0) tw.tr_h = trace;

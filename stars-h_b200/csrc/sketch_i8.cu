@@ -1,0 +1,351 @@
+// Sketch Y = D * Omega of the adaptive engine on the tcgen05 tensor cores,
+// FP64-accurate through integer slices (the Ozaki scheme: K. Ozaki,
+// T. Ogita, S. Oishi, S. M. Rump, "Error-free transformations of matrix
+// multiplication by using fast routines of matrix multiplication and its
+// applications", Numer. Algorithms 59 (2012), in its integer form).
+//
+// Omega is an int8 matrix (a rounded Gaussian, 32 N(0,1) clipped to
+// [-127, 127]); any such matrix is a valid sketch.  Row i of a tile is
+// scaled by 2^-e_i, e_i the exponent of the row's largest |D_ij| (from the
+// generator's per-row maxima), so x = D_ij 2^-e_i lies in (-1, 1); x is
+// rounded to q = round(x 2^39) and written with an offset as the 40-bit
+// unsigned integer q' = q + 2^39, whose five bytes u_0..u_4 are the digits:
+//     D_ij = 2^(e_i - 39) (sum_s 256^s u_s[i, j] - 2^39) + err,
+//     |err| <= 2^-40 2^e_i.
+// Each digit matrix times Omega is an exact uint8 x int8 -> int32 product
+// (|sum| <= 255 * 127 * n < 2^31 for n <= 8192) on tcgen05.mma kind::i8,
+// accumulated in TMEM, one accumulator per digit.  The epilogue removes the
+// offset exactly (2^39 = 128 * 2^32: the top digit's product less 128 times
+// the column sums of Omega), recombines the digits in int64 (exact, |T| <
+// 2^61) and converts once:
+//     Y_ic = 2^(e_i - 39) T_ic,  T_ic = sum_s 256^s P_s - 2^39 sum_j Omega_jc.
+// The only error is the rounding of q: 2^-40 of the row maximum per entry,
+// far below the tolerance-driven thresholds of the adaptive basis (the
+// rank decision itself uses the FP64 projection and the exact block norm).
+//
+// One CTA per (tile, 128-row block), 512 threads.  The tile's rows are
+// read from HBM once, in K chunks of 64 columns: every thread converts 16
+// columns of one row into digits and stores them in the no-swizzle K-major
+// core-matrix layout; one thread issues the 5 x 2 MMAs (M 128, N nc, K 32)
+// of the chunk and commits them to the chunk buffer's mbarrier, so the
+// conversion of the next chunk overlaps the MMAs (two buffers).  Omega's
+// nc columns for the tile (nc x n bytes) stay in shared memory.
+#include <cstdint>
+#include "engine.cuh"
+
+namespace b200 {
+
+constexpr int kSlices = 5;             // bytes (digits) per entry
+constexpr int kSkRows = 128;           // rows per CTA (MMA M)
+constexpr int kSkChunk = 64;           // K columns per chunk
+constexpr int kSkThreads = 512;
+constexpr int kSkMaxN = 64;            // sketch columns per launch
+
+// Shared-memory descriptor of a K-major operand without swizzle:
+// core matrices of 8 rows x 16 bytes (128 contiguous bytes), lbo = byte
+// distance between the two 16-byte K halves of one MMA, sbo = byte
+// distance between consecutive 8-row groups.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo,
+                                              uint32_t sbo)
+{
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;            // descriptor version (sm_100)
+    return d;                          // base offset 0, no swizzle
+}
+
+// Instruction descriptor: int32 accumulator, unsigned int8 A (digits),
+// signed int8 B (Omega), both K-major, M = 128, N = n.
+__host__ __device__ constexpr uint32_t idesc_i8(int n)
+{
+    return (2u << 4) | (0u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) |
+           ((uint32_t)(kSkRows >> 4) << 24);
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t da,
+                                       uint64_t db, uint32_t idesc,
+                                       int accumulate)
+{
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}"
+                 :: "r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t *mbar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                 :: "r"(smem_u32(mbar)));
+}
+
+__device__ __forceinline__ bool mbar_try(uint64_t *mbar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile("{\n\t.reg .pred P1;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+                 "selp.b32 %0, 1, 0, P1;\n\t}"
+                 : "=r"(ok) : "r"(smem_u32(mbar)), "r"(parity) : "memory");
+    return ok != 0;
+}
+
+// Waits for the completion of the phase of the given parity; gives up
+// after about two seconds and returns false.
+__device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity)
+{
+    const long long t0 = clock64();
+    while (!mbar_try(mbar, parity))
+        if (clock64() - t0 > (1ll << 32)) return false;
+    return true;
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16])
+{
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+                 "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]),
+                   "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                   "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
+                   "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+                 : "r"(taddr));
+}
+
+// Digits of 16 entries x in (-1, 1): q' = round(x 2^39) + 2^39 < 2^40 by
+// the magic-number rounding (adding 1.5 2^52 leaves the integer in the low
+// mantissa bits), then byte s of the four q' of columns 4c .. 4c + 3 goes
+// to word w[s][c].
+__device__ __forceinline__ void digits16(const double (&x)[16],
+                                         uint32_t (&w)[kSlices][4])
+{
+    const double magic = 0x1.8p52;
+    const long long mbits = __double_as_longlong(magic);
+    uint32_t lo[16], hi[16];
+    #pragma unroll
+    for (int c = 0; c < 16; ++c) {
+        const double y = fma(x[c], 0x1p39, magic + 0x1p39);
+        long long q = __double_as_longlong(y) - mbits;   // in [0, 2^40]
+        q = q > (1ll << 40) - 1 ? (1ll << 40) - 1 : q;
+        lo[c] = (uint32_t)q;
+        hi[c] = (uint32_t)(q >> 32);
+    }
+    #pragma unroll
+    for (int g = 0; g < 4; ++g) {
+        #pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            const uint32_t sel = (uint32_t)s | ((uint32_t)(s + 4) << 4);
+            const uint32_t a = __byte_perm(lo[4 * g], lo[4 * g + 1], sel);
+            const uint32_t b = __byte_perm(lo[4 * g + 2], lo[4 * g + 3], sel);
+            w[s][g] = __byte_perm(a, b, 0x5410);
+        }
+        const uint32_t a = __byte_perm(hi[4 * g], hi[4 * g + 1], 0x40);
+        const uint32_t b = __byte_perm(hi[4 * g + 2], hi[4 * g + 3], 0x40);
+        w[4][g] = __byte_perm(a, b, 0x5410);
+    }
+}
+
+// Y(:, 0:bcur) of every tile with an active round = D * Omega8(:, cols_done
+// + (0:nc)), rows in 128-row blocks (blockIdx.x), tiles in blockIdx.y.
+__global__ void __launch_bounds__(kSkThreads, 1)
+k_sketch_i8(const TileWork *__restrict__ tiles, Workspace ws,
+            const int8_t *__restrict__ om8, int ld_om8, int om8_cols, int nc)
+{
+    extern __shared__ __align__(1024) uint8_t sk_smem[];
+    __shared__ __align__(8) uint64_t mbar[2];
+    __shared__ uint32_t tmem_base;
+    __shared__ int failed;
+    __shared__ int colsum[kSkMaxN];
+
+    const TileWork tw = tiles[blockIdx.y];
+    const int row0 = blockIdx.x * kSkRows;
+    if (tw.bcur <= 0 || row0 >= tw.m) return;            // uniform
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    const int r = t & (kSkRows - 1), qd = t >> 7;        // row, column quarter
+    const int n = tw.n, m = tw.m;
+    const int npad = (n + kSkChunk - 1) / kSkChunk * kSkChunk;
+    const int nchunks = npad / kSkChunk;
+    constexpr int kAbuf = kSlices * kSkRows * kSkChunk;  // bytes per buffer
+    uint8_t *Abuf = sk_smem;                             // [2][kSlices][8 KB]
+    uint8_t *Bsm = sk_smem + 2 * kAbuf;                  // nc x npad
+    const uint32_t ncols_alloc = nc * kSlices <= 128 ? 128
+                               : nc * kSlices <= 256 ? 256 : 512;
+
+    if (t == 0) {
+        failed = 0;
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&mbar[0])), "r"(1));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&mbar[1])), "r"(1));
+        asm volatile("fence.mbarrier_init.release.cluster;");
+    }
+    if (t < kSkMaxN) colsum[t] = 0;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     :: "r"(smem_u32(&tmem_base)), "r"(ncols_alloc));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    __syncthreads();
+    // Omega8 columns cols_done .. cols_done + nc of this tile, K-major core
+    // matrices: byte (c, k) at (k / 16) (nc 16) + (c / 8) 128 + (c % 8) 16
+    // + k % 16.  Columns past Omega8's width are zero.  colsum[c] sums the
+    // column as stored (padding rows included: their digits carry the
+    // offset too).
+    {
+        const int c0 = tw.cols_done;
+        const int units = nc * (npad / 16);
+        for (int u = t; u < units; u += kSkThreads) {
+            const int c = u % nc, k16 = u / nc;
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (c0 + c < om8_cols)
+                v = *reinterpret_cast<const uint4 *>(
+                    om8 + (size_t)(c0 + c) * ld_om8 + (size_t)k16 * 16);
+            *reinterpret_cast<uint4 *>(Bsm + (size_t)k16 * (nc * 16) +
+                                       (c >> 3) * 128 + (c & 7) * 16) = v;
+            int sum = 0;
+            const uint32_t wv[4] = {v.x, v.y, v.z, v.w};
+            #pragma unroll
+            for (int q = 0; q < 4; ++q)
+                sum += __dp4a((int)wv[q], 0x01010101, 0);
+            atomicAdd(&colsum[c], sum);
+        }
+    }
+    // row scale 2^-e, e the exponent of the row's largest |D_ij|
+    int e = 0;
+    const int i = row0 + r;
+    if (i < m) {
+        const int ncb = (ws.n_max + 63) / 64;
+        const double *rm = ws.Rmx(tw.slot) + (size_t)i * ncb;
+        double mx = 0.0;
+        for (int cb = 0; cb < (n + 63) / 64; ++cb) mx = fmax(mx, rm[cb]);
+        if (mx > 0.0) frexp(mx, &e);
+    }
+    const double scale = ldexp(1.0, -e);
+    asm volatile("fence.proxy.async.shared::cta;");
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = tmem_base;
+
+    const double *D = ws.D(tw.slot);
+    const int ldD = ws.ldD();
+    const uint32_t idesc = idesc_i8(nc);
+    int last_commit = -1;               // same value in every thread
+    for (int kc = 0; kc < nchunks; ++kc) {
+        const int b = kc & 1;
+        // the MMAs of chunk kc - 2 read this buffer; a wait that gives up
+        // stops every thread (a block-wide vote keeps the barriers aligned)
+        const int bad = kc >= 2 && !mbar_wait(&mbar[b], ((kc >> 1) - 1) & 1);
+        if (__syncthreads_or(bad)) {
+            if (t == 0) failed = 1;
+            break;
+        }
+        // this thread: row r, columns 16 qd .. 16 qd + 15 of the chunk
+        double x[16];
+        #pragma unroll
+        for (int c = 0; c < 16; ++c) {
+            const int j = kc * kSkChunk + 16 * qd + c;
+            x[c] = (i < m && j < n) ? D[(size_t)j * ldD + i] * scale : 0.0;
+        }
+        uint32_t w[kSlices][4];
+        digits16(x, w);
+        uint8_t *A = Abuf + b * kAbuf;
+        #pragma unroll
+        for (int s = 0; s < kSlices; ++s)
+            *reinterpret_cast<uint4 *>(A + s * (kSkRows * kSkChunk) + qd * 2048 +
+                                       (r >> 3) * 128 + (r & 7) * 16) =
+                make_uint4(w[s][0], w[s][1], w[s][2], w[s][3]);
+        asm volatile("fence.proxy.async.shared::cta;");
+        __syncthreads();
+        if (t == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            #pragma unroll
+            for (int s = 0; s < kSlices; ++s)
+                #pragma unroll
+                for (int kk = 0; kk < 2; ++kk) {
+                    const uint64_t da = umma_desc(
+                        smem_u32(A + s * (kSkRows * kSkChunk) + kk * 2 * 2048),
+                        2048, 128);
+                    const uint64_t db = umma_desc(
+                        smem_u32(Bsm + (size_t)(kc * 4 + kk * 2) * (nc * 16)),
+                        nc * 16, 128);
+                    mma_i8(tmem + s * nc, da, db, idesc, (kc > 0 || kk > 0));
+                }
+            mma_commit(&mbar[b]);
+        }
+        last_commit = kc;
+    }
+    // the last commit covers every earlier MMA (also after a failure: the
+    // MMAs in flight finish before TMEM is released)
+    {
+        const int bad = last_commit >= 0 &&
+                        !mbar_wait(&mbar[last_commit & 1], (last_commit >> 1) & 1);
+        if (__syncthreads_or(bad) && t == 0) failed = 1;
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    __syncthreads();
+    // warp w reads TMEM lanes 32 (w % 4) .. + 31 (rows) and the columns of
+    // group w / 4 (16 columns each)
+    const int lq = warp & 3, grp = warp >> 2;
+    if (!failed && grp < nc / 16) {
+        double *Y = ws.Y(tw.slot);
+        const int ldY = ws.ldM();
+        const int rr = row0 + 32 * lq + lane;
+        // r = t & 127 = 32 (w % 4) + lane: this thread's own row, so its
+        // exponent e is the row's
+        const int er = e;
+        uint32_t v[kSlices][16];
+        #pragma unroll
+        for (int s = 0; s < kSlices; ++s)
+            tmem_ld16(tmem + ((uint32_t)(32 * lq) << 16) + s * nc + 16 * grp, v[s]);
+        asm volatile("tcgen05.wait::ld.sync.aligned;");
+        if (rr < m) {
+            const double sc = ldexp(1.0, er - 39);
+            #pragma unroll
+            for (int c = 0; c < 16; ++c) {
+                const int col = 16 * grp + c;
+                long long T = (long long)(int)v[4][c] - 128ll * colsum[col];
+                #pragma unroll
+                for (int s = 3; s >= 0; --s) T = T * 256 + (long long)(int)v[s][c];
+                if (col < tw.bcur) Y[(size_t)col * ldY + rr] = (double)T * sc;
+            }
+        }
+    }
+    if (failed && t == 0) {
+        TileWork *tr = const_cast<TileWork *>(tiles) + blockIdx.y;
+        atomicOr(&tr->status, TILE_MMA_TIMEOUT);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
+                     :: "r"(tmem), "r"(ncols_alloc));
+}
+
+size_t sketch_i8_smem(int nc, int n_max)
+{
+    const int npad = (n_max + kSkChunk - 1) / kSkChunk * kSkChunk;
+    return 2 * (size_t)kSlices * kSkRows * kSkChunk + (size_t)nc * npad;
+}
+
+bool sketch_i8_fits(int nc, int n_max)
+{
+    return nc > 0 && nc <= kSkMaxN && n_max <= 8192 &&
+           sketch_i8_smem((nc + 15) / 16 * 16, n_max) <= 200 * 1024;
+}
+
+void launch_sketch_i8(const TileWork *d_tiles, int ntiles, Workspace ws,
+                      const int8_t *om8, int ld_om8, int om8_cols, int ncols,
+                      cudaStream_t stream)
+{
+    const int nc = (ncols + 15) / 16 * 16;
+    const size_t smem = sketch_i8_smem(nc, ws.n_max);
+    cudaFuncSetAttribute(k_sketch_i8, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
+    dim3 grid((ws.m_max + kSkRows - 1) / kSkRows, ntiles);
+    k_sketch_i8<<<grid, kSkThreads, smem, stream>>>(d_tiles, ws, om8, ld_om8,
+                                                    om8_cols, nc);
+}
+
+}  // namespace b200

@@ -24,12 +24,14 @@
 // rank decision itself uses the FP64 projection and the exact block norm).
 //
 // One CTA per (tile, 128-row block), 512 threads.  The tile's rows are
-// read from HBM once, in K chunks of 64 columns: every thread converts 16
-// columns of one row into digits and stores them in the no-swizzle K-major
-// core-matrix layout; one thread issues the 5 x 2 MMAs (M 128, N nc, K 32)
-// of the chunk and commits them to the chunk buffer's mbarrier, so the
-// conversion of the next chunk overlaps the MMAs (two buffers).  Omega's
-// nc columns for the tile (nc x n bytes) stay in shared memory.
+// read from HBM once, in K chunks of 32 columns copied asynchronously
+// (cp.async) into a two-stage shared-memory buffer, so the copy of the next
+// chunk overlaps the work on this one; every thread converts 8 columns of
+// one row into digits and stores them in the no-swizzle K-major
+// core-matrix layout; one thread issues the 5 MMAs (M 128, N nc, K 32) of
+// the chunk and commits them to the chunk buffer's mbarrier, so the
+// conversion of the next chunk overlaps the MMAs (two digit buffers).
+// Omega's nc columns for the tile (nc x n bytes) stay in shared memory.
 #include <cstdint>
 #include "engine.cuh"
 
@@ -37,7 +39,7 @@ namespace b200 {
 
 constexpr int kSlices = 5;             // bytes (digits) per entry
 constexpr int kSkRows = 128;           // rows per CTA (MMA M)
-constexpr int kSkChunk = 64;           // K columns per chunk
+constexpr int kSkChunk = 32;           // K columns per chunk (one MMA K)
 constexpr int kSkThreads = 512;
 constexpr int kSkMaxN = 64;            // sketch columns per launch
 
@@ -115,18 +117,18 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16])
                  : "r"(taddr));
 }
 
-// Digits of 16 entries x in (-1, 1): q' = round(x 2^39) + 2^39 < 2^40 by
+// Digits of 8 entries x in (-1, 1): q' = round(x 2^39) + 2^39 < 2^40 by
 // the magic-number rounding (adding 1.5 2^52 leaves the integer in the low
 // mantissa bits), then byte s of the four q' of columns 4c .. 4c + 3 goes
 // to word w[s][c].
-__device__ __forceinline__ void digits16(const double (&x)[16],
-                                         uint32_t (&w)[kSlices][4])
+__device__ __forceinline__ void digits8(const double (&x)[8],
+                                        uint32_t (&w)[kSlices][2])
 {
     const double magic = 0x1.8p52;
     const long long mbits = __double_as_longlong(magic);
-    uint32_t lo[16], hi[16];
+    uint32_t lo[8], hi[8];
     #pragma unroll
-    for (int c = 0; c < 16; ++c) {
+    for (int c = 0; c < 8; ++c) {
         const double y = fma(x[c], 0x1p39, magic + 0x1p39);
         long long q = __double_as_longlong(y) - mbits;   // in [0, 2^40]
         q = q > (1ll << 40) - 1 ? (1ll << 40) - 1 : q;
@@ -134,7 +136,7 @@ __device__ __forceinline__ void digits16(const double (&x)[16],
         hi[c] = (uint32_t)(q >> 32);
     }
     #pragma unroll
-    for (int g = 0; g < 4; ++g) {
+    for (int g = 0; g < 2; ++g) {
         #pragma unroll
         for (int s = 0; s < 4; ++s) {
             const uint32_t sel = (uint32_t)s | ((uint32_t)(s + 4) << 4);
@@ -146,6 +148,14 @@ __device__ __forceinline__ void digits16(const double (&x)[16],
         const uint32_t b = __byte_perm(hi[4 * g + 2], hi[4 * g + 3], 0x40);
         w[4][g] = __byte_perm(a, b, 0x5410);
     }
+}
+
+// Asynchronous 8-byte global -> shared copy; src_bytes 0 writes zeros.
+__device__ __forceinline__ void cp_async8(void *dst, const void *src,
+                                          int src_bytes)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;"
+                 :: "r"(smem_u32(dst)), "l"(src), "r"(src_bytes));
 }
 
 // Y(:, 0:bcur) of every tile with an active round = D * Omega8(:, cols_done
@@ -169,8 +179,13 @@ k_sketch_i8(const TileWork *__restrict__ tiles, Workspace ws,
     const int npad = (n + kSkChunk - 1) / kSkChunk * kSkChunk;
     const int nchunks = npad / kSkChunk;
     constexpr int kAbuf = kSlices * kSkRows * kSkChunk;  // bytes per buffer
-    uint8_t *Abuf = sk_smem;                             // [2][kSlices][8 KB]
+    constexpr int kStage = kSkRows * kSkChunk;           // doubles per stage
+    uint8_t *Abuf = sk_smem;                             // [2][kSlices][4 KB]
     uint8_t *Bsm = sk_smem + 2 * kAbuf;                  // nc x npad
+    // raw FP64 chunks (column-major, 128 rows), two stages: the copy of
+    // chunk kc + 1 runs while chunk kc is converted
+    const int npad_max = (ws.n_max + kSkChunk - 1) / kSkChunk * kSkChunk;
+    double *stage = reinterpret_cast<double *>(Bsm + (size_t)nc * npad_max);
     const uint32_t ncols_alloc = nc * kSlices <= 128 ? 128
                                : nc * kSlices <= 256 ? 256 : 512;
 
@@ -231,51 +246,70 @@ k_sketch_i8(const TileWork *__restrict__ tiles, Workspace ws,
     const double *D = ws.D(tw.slot);
     const int ldD = ws.ldD();
     const uint32_t idesc = idesc_i8(nc);
+    // copies of chunk kc into stage kc & 1: 128 x 32 doubles, 8 per thread;
+    // rows past m and columns past n are zero-filled without a read
+    auto issue = [&](int kc) {
+        double *st = stage + (kc & 1) * kStage;
+        #pragma unroll
+        for (int q = 0; q < kStage / kSkThreads; ++q) {
+            const int u = t + kSkThreads * q;
+            const int rr = u & (kSkRows - 1), jj = u >> 7;
+            const int gi = row0 + rr, gj = kc * kSkChunk + jj;
+            const bool in = gi < m && gj < n;
+            cp_async8(st + jj * kSkRows + rr,
+                      in ? D + (size_t)gj * ldD + gi : D, in ? 8 : 0);
+        }
+        asm volatile("cp.async.commit_group;");
+    };
+    issue(0);
     int last_commit = -1;               // same value in every thread
     for (int kc = 0; kc < nchunks; ++kc) {
         const int b = kc & 1;
-        // the MMAs of chunk kc - 2 read this buffer; a wait that gives up
-        // stops every thread (a block-wide vote keeps the barriers aligned)
+        if (kc + 1 < nchunks) {
+            issue(kc + 1);
+            asm volatile("cp.async.wait_group 1;" ::: "memory");
+        } else {
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
+        }
+        // every thread's copies of chunk kc have landed; the MMAs of chunk
+        // kc - 2 (which read A buffer b) have finished -- a wait that gives
+        // up stops every thread (the block-wide vote keeps barriers aligned)
         const int bad = kc >= 2 && !mbar_wait(&mbar[b], ((kc >> 1) - 1) & 1);
         if (__syncthreads_or(bad)) {
             if (t == 0) failed = 1;
             break;
         }
-        // this thread: row r, columns 16 qd .. 16 qd + 15 of the chunk
-        double x[16];
+        // this thread: row r, columns 8 qd .. 8 qd + 7 of the chunk
+        const double *st = stage + b * kStage;
+        double x[8];
         #pragma unroll
-        for (int c = 0; c < 16; ++c) {
-            const int j = kc * kSkChunk + 16 * qd + c;
-            x[c] = (i < m && j < n) ? D[(size_t)j * ldD + i] * scale : 0.0;
-        }
-        uint32_t w[kSlices][4];
-        digits16(x, w);
+        for (int c = 0; c < 8; ++c) x[c] = st[(8 * qd + c) * kSkRows + r] * scale;
+        uint32_t w[kSlices][2];
+        digits8(x, w);
         uint8_t *A = Abuf + b * kAbuf;
         #pragma unroll
         for (int s = 0; s < kSlices; ++s)
-            *reinterpret_cast<uint4 *>(A + s * (kSkRows * kSkChunk) + qd * 2048 +
-                                       (r >> 3) * 128 + (r & 7) * 16) =
-                make_uint4(w[s][0], w[s][1], w[s][2], w[s][3]);
+            *reinterpret_cast<uint2 *>(A + s * (kSkRows * kSkChunk) +
+                                       (qd >> 1) * 2048 + (r >> 3) * 128 +
+                                       (r & 7) * 16 + (qd & 1) * 8) =
+                make_uint2(w[s][0], w[s][1]);
         asm volatile("fence.proxy.async.shared::cta;");
         __syncthreads();
         if (t == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;");
             #pragma unroll
-            for (int s = 0; s < kSlices; ++s)
-                #pragma unroll
-                for (int kk = 0; kk < 2; ++kk) {
-                    const uint64_t da = umma_desc(
-                        smem_u32(A + s * (kSkRows * kSkChunk) + kk * 2 * 2048),
-                        2048, 128);
-                    const uint64_t db = umma_desc(
-                        smem_u32(Bsm + (size_t)(kc * 4 + kk * 2) * (nc * 16)),
-                        nc * 16, 128);
-                    mma_i8(tmem + s * nc, da, db, idesc, (kc > 0 || kk > 0));
-                }
+            for (int s = 0; s < kSlices; ++s) {
+                const uint64_t da = umma_desc(
+                    smem_u32(A + s * (kSkRows * kSkChunk)), 2048, 128);
+                const uint64_t db = umma_desc(
+                    smem_u32(Bsm + (size_t)(kc * 2) * (nc * 16)), nc * 16, 128);
+                mma_i8(tmem + s * nc, da, db, idesc, kc > 0);
+            }
             mma_commit(&mbar[b]);
         }
         last_commit = kc;
     }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
     // the last commit covers every earlier MMA (also after a failure: the
     // MMAs in flight finish before TMEM is released)
     {
@@ -326,7 +360,8 @@ k_sketch_i8(const TileWork *__restrict__ tiles, Workspace ws,
 size_t sketch_i8_smem(int nc, int n_max)
 {
     const int npad = (n_max + kSkChunk - 1) / kSkChunk * kSkChunk;
-    return 2 * (size_t)kSlices * kSkRows * kSkChunk + (size_t)nc * npad;
+    return 2 * (size_t)kSlices * kSkRows * kSkChunk + (size_t)nc * npad +
+           2 * (size_t)kSkRows * kSkChunk * sizeof(double);
 }
 
 bool sketch_i8_fits(int nc, int n_max)

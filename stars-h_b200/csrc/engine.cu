@@ -475,6 +475,8 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
             bn = std::max(bn, all[q].n);
             bk = std::max(bk, all[q].k);
         }
+        // even leading dimension (16-byte column strides for the TMA)
+        bm = (bm + 7) / 8 * 8;
         stride = workspace_layout(probe, bm, bn, bk, true);
         long long fit = (long long)(budget / (stride * sizeof(double)));
         const int nt = (int)std::max<long long>(1, std::min(cap, fit));
@@ -605,7 +607,13 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
             const int bmax = std::min(block, k_max);
             cudaEventRecord(ev[0], s);
             if (use_i8) {
-                launch_sketch_i8(dt, nt, ws, om8, ld_om8, k_max_all, bmax, s);
+                // every batch has an even leading dimension (plan), so the
+                // tensor map exists unless the driver lacks the entry point
+                if (!launch_sketch_i8(dt, nt, ws, om8, ld_om8, k_max_all, bmax, s)) {
+                    set_error("no TMA tensor map for the sketch");
+                    info = STARSH_UNKNOWN_ERROR;
+                    break;
+                }
                 count_launch();
                 const cudaError_t ce = cudaGetLastError();
                 if (ce != cudaSuccess) { info = cuda_fail(ce, "k_sketch_i8"); break; }

@@ -163,7 +163,9 @@ void launch_write_v(const TileWork *d_tiles, int ntiles, Workspace ws,
 // every tile with an active round.  sketch_i8_fits() tells whether a batch
 // shape is supported (ncols <= 64, n_max <= 8192, shared memory).
 bool sketch_i8_fits(int ncols, int n_max);
-void launch_sketch_i8(const TileWork *d_tiles, int ntiles, Workspace ws,
+// Returns false (nothing launched) when the batch's layout cannot be
+// described to the TMA unit (odd leading dimension).
+bool launch_sketch_i8(const TileWork *d_tiles, int ntiles, Workspace ws,
                       const int8_t *om8, int ld_om8, int om8_cols, int ncols,
                       cudaStream_t stream);
 // Omega8(j, c) = clip(round(32 g), -127, 127), g the Gaussian of

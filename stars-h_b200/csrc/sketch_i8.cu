@@ -24,15 +24,18 @@
 // rank decision itself uses the FP64 projection and the exact block norm).
 //
 // One CTA per (tile, 128-row block), 512 threads.  The tile's rows are
-// read from HBM once, in K chunks of 32 columns copied asynchronously
-// (cp.async) into a two-stage shared-memory buffer, so the copy of the next
-// chunk overlaps the work on this one; every thread converts 8 columns of
-// one row into digits and stores them in the no-swizzle K-major
+// read from HBM once, in K chunks of 32 columns, each brought into a
+// three-stage shared-memory buffer by one TMA tile copy (the copies of the
+// next two chunks overlap the work on this one); every thread converts 8
+// columns of one row into digits and stores them in the no-swizzle K-major
 // core-matrix layout; one thread issues the 5 MMAs (M 128, N nc, K 32) of
 // the chunk and commits them to the chunk buffer's mbarrier, so the
-// conversion of the next chunk overlaps the MMAs (two digit buffers).
+// conversion of the next chunk overlaps the MMAs (two digit buffers); the
+// chunks are handed over through mbarriers, without block-wide barriers.
 // Omega's nc columns for the tile (nc x n bytes) stay in shared memory.
 #include <cstdint>
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include "engine.cuh"
 
 namespace b200 {
@@ -42,6 +45,7 @@ constexpr int kSkRows = 128;           // rows per CTA (MMA M)
 constexpr int kSkChunk = 32;           // K columns per chunk (one MMA K)
 constexpr int kSkThreads = 512;
 constexpr int kSkMaxN = 64;            // sketch columns per launch
+constexpr int kStages = 3;             // D chunks in flight (TMA stages)
 
 // Shared-memory descriptor of a K-major operand without swizzle:
 // core matrices of 8 rows x 16 bytes (128 contiguous bytes), lbo = byte
@@ -106,6 +110,24 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity)
     return true;
 }
 
+// The same, also giving up as soon as *abort is set by another thread.
+__device__ __forceinline__ bool mbar_wait_or(uint64_t *mbar, uint32_t parity,
+                                             volatile int *abort)
+{
+    const long long t0 = clock64();
+    while (!mbar_try(mbar, parity)) {
+        if (*abort) return false;
+        if (clock64() - t0 > (1ll << 32)) return false;
+    }
+    return true;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *mbar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];"
+                 :: "r"(smem_u32(mbar)) : "memory");
+}
+
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16])
 {
     asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 "
@@ -121,19 +143,18 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16])
 // the magic-number rounding (adding 1.5 2^52 leaves the integer in the low
 // mantissa bits), then byte s of the four q' of columns 4c .. 4c + 3 goes
 // to word w[s][c].
-__device__ __forceinline__ void digits8(const double (&x)[8],
+__device__ __forceinline__ void digits8(const double (&y)[8],
                                         uint32_t (&w)[kSlices][2])
 {
-    const double magic = 0x1.8p52;
-    const long long mbits = __double_as_longlong(magic);
+    // y = x 2^39 + 2^39 + 1.5 2^52 (one rounding): the low word of y's bit
+    // pattern is the low word of q', the high word less 0x43380000 its top
+    // byte (q' = 2^40 after rounding is clamped to 2^40 - 1)
     uint32_t lo[8], hi[8];
     #pragma unroll
     for (int c = 0; c < 8; ++c) {
-        const double y = fma(x[c], 0x1p39, magic + 0x1p39);
-        long long q = __double_as_longlong(y) - mbits;   // in [0, 2^40]
-        q = q > (1ll << 40) - 1 ? (1ll << 40) - 1 : q;
-        lo[c] = (uint32_t)q;
-        hi[c] = (uint32_t)(q >> 32);
+        lo[c] = (uint32_t)__double2loint(y[c]);
+        hi[c] = (uint32_t)__double2hiint(y[c]) - 0x43380000u;
+        if (hi[c] > 255u) { hi[c] = 255u; lo[c] = 0xFFFFFFFFu; }
     }
     #pragma unroll
     for (int g = 0; g < 2; ++g) {
@@ -150,24 +171,35 @@ __device__ __forceinline__ void digits8(const double (&x)[8],
     }
 }
 
-// Asynchronous 8-byte global -> shared copy; src_bytes 0 writes zeros.
-__device__ __forceinline__ void cp_async8(void *dst, const void *src,
-                                          int src_bytes)
+// One TMA tile copy (this CTA only) of the 128 x 32 FP64 box at (row0,
+// col0, slot) of the workspace's D tensor into shared memory, completing
+// on mbar with its byte count.
+__device__ __forceinline__ void tma_load_d(void *dst, const CUtensorMap *map,
+                                           int row0, int col0, int slot,
+                                           uint64_t *mbar, uint32_t bytes)
 {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;"
-                 :: "r"(smem_u32(dst)), "l"(src), "r"(src_bytes));
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                 :: "r"(smem_u32(mbar)), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes "
+                 "[%0], [%1, {%2, %3, %4}], [%5];"
+                 :: "r"(smem_u32(dst)), "l"(map), "r"(row0), "r"(col0), "r"(slot),
+                    "r"(smem_u32(mbar))
+                 : "memory");
 }
 
 // Y(:, 0:bcur) of every tile with an active round = D * Omega8(:, cols_done
 // + (0:nc)), rows in 128-row blocks (blockIdx.x), tiles in blockIdx.y.
 __global__ void __launch_bounds__(kSkThreads, 1)
-k_sketch_i8(const TileWork *__restrict__ tiles, Workspace ws,
+k_sketch_i8(const __grid_constant__ CUtensorMap dmap,
+            const TileWork *__restrict__ tiles, Workspace ws,
             const int8_t *__restrict__ om8, int ld_om8, int om8_cols, int nc)
 {
-    extern __shared__ __align__(1024) uint8_t sk_smem[];
-    __shared__ __align__(8) uint64_t mbar[2];
+    extern __shared__ __align__(1024) uint8_t sk_smem_raw[];
+    __shared__ __align__(8) uint64_t mbar[2];     // MMAs done with A buffer
+    __shared__ __align__(8) uint64_t stbar[kStages];  // D chunk landed in stage
+    __shared__ __align__(8) uint64_t abar[2];     // all digits of a chunk written
     __shared__ uint32_t tmem_base;
-    __shared__ int failed;
+    __shared__ volatile int failed;
     __shared__ int colsum[kSkMaxN];
 
     const TileWork tw = tiles[blockIdx.y];
@@ -180,10 +212,12 @@ k_sketch_i8(const TileWork *__restrict__ tiles, Workspace ws,
     const int nchunks = npad / kSkChunk;
     constexpr int kAbuf = kSlices * kSkRows * kSkChunk;  // bytes per buffer
     constexpr int kStage = kSkRows * kSkChunk;           // doubles per stage
+    // 1024-byte aligned base (the launch adds 1 KB of slack)
+    uint8_t *sk_smem = sk_smem_raw + ((1024u - (smem_u32(sk_smem_raw) & 1023u)) & 1023u);
     uint8_t *Abuf = sk_smem;                             // [2][kSlices][4 KB]
     uint8_t *Bsm = sk_smem + 2 * kAbuf;                  // nc x npad
-    // raw FP64 chunks (column-major, 128 rows), two stages: the copy of
-    // chunk kc + 1 runs while chunk kc is converted
+    // raw FP64 chunks (column-major, 128 rows), kStages stages: the copies
+    // of chunks kc + 1 .. kc + kStages - 1 run while chunk kc is converted
     const int npad_max = (ws.n_max + kSkChunk - 1) / kSkChunk * kSkChunk;
     double *stage = reinterpret_cast<double *>(Bsm + (size_t)nc * npad_max);
     const uint32_t ncols_alloc = nc * kSlices <= 128 ? 128
@@ -193,6 +227,10 @@ k_sketch_i8(const TileWork *__restrict__ tiles, Workspace ws,
         failed = 0;
         asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&mbar[0])), "r"(1));
         asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&mbar[1])), "r"(1));
+        for (int q = 0; q < kStages; ++q)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&stbar[q])), "r"(1));
+        for (int q = 0; q < 2; ++q)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&abar[q])), "r"(kSkThreads));
         asm volatile("fence.mbarrier_init.release.cluster;");
     }
     if (t < kSkMaxN) colsum[t] = 0;
@@ -236,7 +274,9 @@ k_sketch_i8(const TileWork *__restrict__ tiles, Workspace ws,
         for (int cb = 0; cb < (n + 63) / 64; ++cb) mx = fmax(mx, rm[cb]);
         if (mx > 0.0) frexp(mx, &e);
     }
-    const double scale = ldexp(1.0, -e);
+    // y = D 2^(39 - e) + 2^39 + 1.5 2^52 in one fma (see digits8)
+    const double scale39 = ldexp(1.0, 39 - e);
+    const double magic = 0x1.8p52 + 0x1p39;
     asm volatile("fence.proxy.async.shared::cta;");
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
@@ -246,57 +286,57 @@ k_sketch_i8(const TileWork *__restrict__ tiles, Workspace ws,
     const double *D = ws.D(tw.slot);
     const int ldD = ws.ldD();
     const uint32_t idesc = idesc_i8(nc);
-    // copies of chunk kc into stage kc & 1: 128 x 32 doubles, 8 per thread;
-    // rows past m and columns past n are zero-filled without a read
-    auto issue = [&](int kc) {
-        double *st = stage + (kc & 1) * kStage;
-        #pragma unroll
-        for (int q = 0; q < kStage / kSkThreads; ++q) {
-            const int u = t + kSkThreads * q;
-            const int rr = u & (kSkRows - 1), jj = u >> 7;
-            const int gi = row0 + rr, gj = kc * kSkChunk + jj;
-            const bool in = gi < m && gj < n;
-            cp_async8(st + jj * kSkRows + rr,
-                      in ? D + (size_t)gj * ldD + gi : D, in ? 8 : 0);
-        }
-        asm volatile("cp.async.commit_group;");
-    };
-    issue(0);
-    int last_commit = -1;               // same value in every thread
+    // chunk kc of D (128 rows x 32 columns) lands in stage kc % kStages by
+    // one TMA copy; rows past m_max / columns past n_max read as zero, rows in
+    // [m, m_max) and columns in [n, n_max) are masked below
+    constexpr uint32_t kStageBytes = kStage * sizeof(double);
+    if (t == 0)
+        for (int q = 0; q < kStages - 1 && q < nchunks; ++q)
+            tma_load_d(stage + q * kStage, &dmap, row0, q * kSkChunk, tw.slot,
+                       &stbar[q], kStageBytes);
+    // No block-wide barrier per chunk: every thread waits for its chunk's
+    // data (stbar) and for the MMAs that read its digit buffer two chunks
+    // ago (mbar), writes its digits and arrives on abar; thread 0 alone
+    // waits for all 512 arrivals, issues the chunk's MMAs and the TMA copy
+    // of a later chunk (whose stage the previous chunk's converters have
+    // all left, as their arrivals show).  Each wait gives up after a bound
+    // or as soon as another thread has given up (failed).
+    int last_commit = -1;               // thread 0's view
     for (int kc = 0; kc < nchunks; ++kc) {
         const int b = kc & 1;
-        if (kc + 1 < nchunks) {
-            issue(kc + 1);
-            asm volatile("cp.async.wait_group 1;" ::: "memory");
-        } else {
-            asm volatile("cp.async.wait_group 0;" ::: "memory");
+        const int sg = kc % kStages;
+        bool ok = mbar_wait_or(&stbar[sg], (kc / kStages) & 1, &failed);
+        ok = ok && (kc < 2 || mbar_wait_or(&mbar[b], ((kc >> 1) - 1) & 1, &failed));
+        if (ok) {
+            // this thread: row r, columns 8 qd .. 8 qd + 7 of the chunk
+            const double *st = stage + sg * kStage;
+            double x[8];
+            #pragma unroll
+            for (int c = 0; c < 8; ++c) {
+                const int j = kc * kSkChunk + 8 * qd + c;
+                const double v = (i < m && j < n) ? st[(8 * qd + c) * kSkRows + r] : 0.0;
+                x[c] = fma(v, scale39, magic);
+            }
+            uint32_t w[kSlices][2];
+            digits8(x, w);
+            uint8_t *A = Abuf + b * kAbuf;
+            #pragma unroll
+            for (int s = 0; s < kSlices; ++s)
+                *reinterpret_cast<uint2 *>(A + s * (kSkRows * kSkChunk) +
+                                           (qd >> 1) * 2048 + (r >> 3) * 128 +
+                                           (r & 7) * 16 + (qd & 1) * 8) =
+                    make_uint2(w[s][0], w[s][1]);
+            asm volatile("fence.proxy.async.shared::cta;");
         }
-        // every thread's copies of chunk kc have landed; the MMAs of chunk
-        // kc - 2 (which read A buffer b) have finished -- a wait that gives
-        // up stops every thread (the block-wide vote keeps barriers aligned)
-        const int bad = kc >= 2 && !mbar_wait(&mbar[b], ((kc >> 1) - 1) & 1);
-        if (__syncthreads_or(bad)) {
-            if (t == 0) failed = 1;
-            break;
-        }
-        // this thread: row r, columns 8 qd .. 8 qd + 7 of the chunk
-        const double *st = stage + b * kStage;
-        double x[8];
-        #pragma unroll
-        for (int c = 0; c < 8; ++c) x[c] = st[(8 * qd + c) * kSkRows + r] * scale;
-        uint32_t w[kSlices][2];
-        digits8(x, w);
-        uint8_t *A = Abuf + b * kAbuf;
-        #pragma unroll
-        for (int s = 0; s < kSlices; ++s)
-            *reinterpret_cast<uint2 *>(A + s * (kSkRows * kSkChunk) +
-                                       (qd >> 1) * 2048 + (r >> 3) * 128 +
-                                       (r & 7) * 16 + (qd & 1) * 8) =
-                make_uint2(w[s][0], w[s][1]);
-        asm volatile("fence.proxy.async.shared::cta;");
-        __syncthreads();
+        mbar_arrive(&abar[b]);
+        if (!ok) { failed = 1; break; }
         if (t == 0) {
+            if (!mbar_wait_or(&abar[b], (kc >> 1) & 1, &failed)) {
+                failed = 1;
+                break;
+            }
             asm volatile("tcgen05.fence::after_thread_sync;");
+            uint8_t *A = Abuf + b * kAbuf;
             #pragma unroll
             for (int s = 0; s < kSlices; ++s) {
                 const uint64_t da = umma_desc(
@@ -306,19 +346,29 @@ k_sketch_i8(const TileWork *__restrict__ tiles, Workspace ws,
                 mma_i8(tmem + s * nc, da, db, idesc, kc > 0);
             }
             mma_commit(&mbar[b]);
+            last_commit = kc;
+            const int pf = kc + kStages - 1;
+            if (pf < nchunks) {
+                asm volatile("fence.proxy.async.shared::cta;");
+                tma_load_d(stage + (pf % kStages) * kStage, &dmap, row0,
+                           pf * kSkChunk, tw.slot, &stbar[pf % kStages],
+                           kStageBytes);
+            }
         }
-        last_commit = kc;
+        if (failed) break;
     }
-    asm volatile("cp.async.wait_group 0;" ::: "memory");
-    // the last commit covers every earlier MMA (also after a failure: the
-    // MMAs in flight finish before TMEM is released)
-    {
-        const int bad = last_commit >= 0 &&
-                        !mbar_wait(&mbar[last_commit & 1], (last_commit >> 1) & 1);
-        if (__syncthreads_or(bad) && t == 0) failed = 1;
+    // the last commit covers every earlier MMA; after a failure thread 0
+    // waits for the MMAs it issued before TMEM is released
+    if (!failed) {
+        const int last = nchunks - 1;
+        if (!mbar_wait_or(&mbar[last & 1], (last >> 1) & 1, &failed)) failed = 1;
+    } else if (t == 0 && last_commit >= 0) {
+        int dummy = 0;
+        mbar_wait_or(&mbar[last_commit & 1], (last_commit >> 1) & 1, &dummy);
     }
-    asm volatile("tcgen05.fence::after_thread_sync;");
+    asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
     // warp w reads TMEM lanes 32 (w % 4) .. + 31 (rows) and the columns of
     // group w / 4 (16 columns each)
     const int lq = warp & 3, grp = warp >> 2;
@@ -361,26 +411,59 @@ size_t sketch_i8_smem(int nc, int n_max)
 {
     const int npad = (n_max + kSkChunk - 1) / kSkChunk * kSkChunk;
     return 2 * (size_t)kSlices * kSkRows * kSkChunk + (size_t)nc * npad +
-           2 * (size_t)kSkRows * kSkChunk * sizeof(double);
+           kStages * (size_t)kSkRows * kSkChunk * sizeof(double) + 1024;
 }
 
 bool sketch_i8_fits(int nc, int n_max)
 {
     return nc > 0 && nc <= kSkMaxN && n_max <= 8192 &&
-           sketch_i8_smem((nc + 15) / 16 * 16, n_max) <= 200 * 1024;
+           sketch_i8_smem((nc + 15) / 16 * 16, n_max) <= 227 * 1024;
 }
 
-void launch_sketch_i8(const TileWork *d_tiles, int ntiles, Workspace ws,
+// Tensor map of the batch's D blocks as one 3-D FP64 tensor (rows, columns,
+// slots) with a 128 x 32 x 1 box; needs an even leading dimension (16-byte
+// strides).  Encoded through the driver entry point of the runtime.
+static bool d_tensor_map(CUtensorMap *map, const Workspace &ws, int nslots)
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (encode == nullptr) {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn,
+                                    cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || fn == nullptr) {
+            cudaGetLastError();
+            return false;
+        }
+        encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+    }
+    if (ws.ldD() % 2 != 0) return false;
+    const cuuint64_t dims[3] = {(cuuint64_t)ws.m_max, (cuuint64_t)ws.n_max,
+                                (cuuint64_t)nslots};
+    const cuuint64_t strides[2] = {(cuuint64_t)ws.ldD() * sizeof(double),
+                                   (cuuint64_t)ws.stride * sizeof(double)};
+    const cuuint32_t box[3] = {kSkRows, kSkChunk, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    return encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, ws.D(0), dims,
+                  strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+bool launch_sketch_i8(const TileWork *d_tiles, int ntiles, Workspace ws,
                       const int8_t *om8, int ld_om8, int om8_cols, int ncols,
                       cudaStream_t stream)
 {
+    CUtensorMap map;
+    if (!d_tensor_map(&map, ws, ntiles)) return false;
     const int nc = (ncols + 15) / 16 * 16;
     const size_t smem = sketch_i8_smem(nc, ws.n_max);
     cudaFuncSetAttribute(k_sketch_i8, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
     dim3 grid((ws.m_max + kSkRows - 1) / kSkRows, ntiles);
-    k_sketch_i8<<<grid, kSkThreads, smem, stream>>>(d_tiles, ws, om8, ld_om8,
-                                                    om8_cols, nc);
+    k_sketch_i8<<<grid, kSkThreads, smem, stream>>>(map, d_tiles, ws, om8,
+                                                    ld_om8, om8_cols, nc);
+    return true;
 }
 
 }  // namespace b200

@@ -72,19 +72,33 @@ constexpr int kStageDim = 4;
 // The entries of one thread in a 64 x 64 block: rows ii, columns jj0,
 // jj0 + 4, ... below jn, written to Dcol[jj * ld] (Dcol points at row ii of
 // the block's first column); returns their sum of squares.
-template <int FAM>
+template <int FAM, int NDIM>
 __device__ __forceinline__ double gen_entries(
     const DevKernel &K, bool staged, const double (*rc)[64],
     const double (*cc)[64], const long long *ri, const long long *ci, int ii,
     int jj0, int jn, double *Dcol, int ld, double &amax)
 {
+    // NDIM > 0: coordinates staged in shared memory, dimension known at
+    // compile time (the row's coordinates held in registers); NDIM == 0:
+    // staged, any dimension up to kStageDim; NDIM < 0: read through the
+    // pivots from global memory
+    double xr[NDIM > 0 ? NDIM : 1];
+    if constexpr (NDIM > 0) {
+        #pragma unroll
+        for (int d = 0; d < NDIM; ++d) xr[d] = rc[d][ii];
+    }
     double ss = 0.0;
     amax = 0.0;
     #pragma unroll 4
     for (int jj = jj0; jj < jn; jj += 4) {
-        double dist;
-        if (staged) {
-            dist = 0.0;
+        double dist = 0.0;
+        if constexpr (NDIM > 0) {
+            #pragma unroll
+            for (int d = 0; d < NDIM; ++d) {
+                const double q = __dsub_rn(xr[d], cc[d][jj]);
+                dist = __dadd_rn(dist, __dmul_rn(q, q));
+            }
+        } else if constexpr (NDIM == 0) {
             for (int d = 0; d < K.ndim; ++d) {
                 const double q = __dsub_rn(rc[d][ii], cc[d][jj]);
                 dist = __dadd_rn(dist, __dmul_rn(q, q));
@@ -100,7 +114,23 @@ __device__ __forceinline__ double gen_entries(
     return ss;
 }
 
-__global__ void __launch_bounds__(256)
+// Dispatch on the staging dimension for one family.
+template <int FAM>
+__device__ __forceinline__ double gen_entries_dim(
+    const DevKernel &K, bool staged, const double (*rc)[64],
+    const double (*cc)[64], const long long *ri, const long long *ci, int ii,
+    int jj0, int jn, double *Dcol, int ld, double &amax)
+{
+    if (!staged)
+        return gen_entries<FAM, -1>(K, staged, rc, cc, ri, ci, ii, jj0, jn, Dcol, ld, amax);
+    if (K.ndim == 2)
+        return gen_entries<FAM, 2>(K, staged, rc, cc, ri, ci, ii, jj0, jn, Dcol, ld, amax);
+    if (K.ndim == 3)
+        return gen_entries<FAM, 3>(K, staged, rc, cc, ri, ci, ii, jj0, jn, Dcol, ld, amax);
+    return gen_entries<FAM, 0>(K, staged, rc, cc, ri, ci, ii, jj0, jn, Dcol, ld, amax);
+}
+
+__global__ void __launch_bounds__(256, 3)
 k_gen_tiles(const DevKernel *__restrict__ kernels,
             const TileWork *__restrict__ tiles, Workspace ws)
 {
@@ -140,28 +170,28 @@ k_gen_tiles(const DevKernel *__restrict__ kernels,
         const int jn = min(64, tw.n - j0);
         switch (K.family) {
         case FAM_EXP:
-            ss = gen_entries<FAM_EXP>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld, amax);
+            ss = gen_entries_dim<FAM_EXP>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld, amax);
             break;
         case FAM_SQREXP:
-            ss = gen_entries<FAM_SQREXP>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld, amax);
+            ss = gen_entries_dim<FAM_SQREXP>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld, amax);
             break;
         case FAM_MATERN:
-            ss = gen_entries<FAM_MATERN>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld, amax);
+            ss = gen_entries_dim<FAM_MATERN>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld, amax);
             break;
         case FAM_MATERN2:
-            ss = gen_entries<FAM_MATERN2>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld, amax);
+            ss = gen_entries_dim<FAM_MATERN2>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld, amax);
             break;
         case FAM_COULOMB:
-            ss = gen_entries<FAM_COULOMB>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld, amax);
+            ss = gen_entries_dim<FAM_COULOMB>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld, amax);
             break;
         case FAM_SIN:
-            ss = gen_entries<FAM_SIN>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld, amax);
+            ss = gen_entries_dim<FAM_SIN>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld, amax);
             break;
         case FAM_COS:
-            ss = gen_entries<FAM_COS>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld, amax);
+            ss = gen_entries_dim<FAM_COS>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld, amax);
             break;
         default:
-            ss = gen_entries<FAM_RBF>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld, amax);
+            ss = gen_entries_dim<FAM_RBF>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld, amax);
         }
     }
     // largest |D_ij| of each row of the sub-block (for the int8 sketch's

@@ -673,6 +673,23 @@ def _cpu_run(key, n):
 
 # ------------------------------------------------------------- device peak
 
+# DRAM bytes (read + write) of k_sketch_i8 over its algorithmic bytes, from
+# the ncu capture summarised in profiles/k_sketch_i8_c2_n16384.md
+SKETCH_TRAFFIC_RATIO = 1.013
+
+
+def measured_hbm_gbs():
+    """HBM copy bandwidth measured on this pool's B200s (driver-written
+    MEASURED_PEAKS.json), else the pool's earlier fallback figure."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            v = float(json.load(f)["hbm_gbs"])
+        return v, "MEASURED_PEAKS.json hbm_gbs (of measured)"
+    except Exception:
+        return 6650.0, "fallback 6.65 TB/s (of fallback)"
+
+
 def fp64_peak_tflops(torch):
     """FP64 tensor throughput measured in this run: torch float64 matmul
     (cuBLAS DGEMM) 4096^3, best of 5 after warm-up."""
@@ -922,11 +939,33 @@ def main():
         if world > 1:
             torch.distributed.destroy_process_group()
         return
-    # roofline of the sketch GEMM (FP64 DMMA)
-    per_launch_ms = last.sketch_ms / max(1, last.sketch_launches)
-    flops_per_launch = last.sketch_flops / max(1, last.sketch_launches)
-    achieved = flops_per_launch / (per_launch_ms / 1e3) / 1e12
-    peak = fp64_peak_tflops(torch)
+    # roofline of the sketch kernel: on the int8 tensor-core path it streams
+    # D once per round from HBM (bound: HBM; algorithmic bytes = 8 m n per
+    # tile and round + the Y columns written); the FP64 engine's sketch is
+    # a DMMA GEMM (bound: FP64 tensor, 2 m n k flops per tile)
+    per_launch_s = last.sketch_ms / 1e3 / max(1, last.sketch_launches)
+    if last.sketch_int8:
+        bytes_per_launch = last.sketch_bytes / max(1, last.sketch_launches)
+        achieved = bytes_per_launch / per_launch_s / 1e9
+        peak, peak_src = measured_hbm_gbs()
+        roof = {"bound": "hbm", "kernel": "k_sketch_i8 (tcgen05 int8 slices, Y = D Omega8)",
+                "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_src,
+                "algorithmic_bytes_per_launch": bytes_per_launch,
+                # ncu (profiles/k_sketch_i8_c2_n16384.md): DRAM read + write
+                # = 1.013x the algorithmic bytes on a 256-tile capture, so the
+                # per-launch traffic is the algorithmic figure scaled by it
+                "traffic": bytes_per_launch * SKETCH_TRAFFIC_RATIO,
+                "traffic_source": "ncu capture of a 256-tile case, scaled by tiles"}
+    else:
+        flops_per_launch = last.sketch_flops / max(1, last.sketch_launches)
+        achieved = flops_per_launch / per_launch_s / 1e12
+        peak = fp64_peak_tflops(torch)
+        roof = {"bound": "tensor", "kernel": "k_gemm_f64 (sketch Y = D Omega, FP64 DMMA)",
+                "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak,
+                "peak_source": "measured in this run: torch float64 matmul 4096^3 (cuBLAS DGEMM); MEASURED_PEAKS.json has no FP64 figure",
+                "traffic": None}
     accepted = bool(0 <= err <= wl["tol"])
     line = {
         "metric": METRIC, "value": value if accepted else None,
@@ -957,11 +996,7 @@ def main():
         "gpu_launches": int(sum(s.kernel_launches for s in sts)),
         "phases_ms": {"sketch": last.sketch_ms, "project": last.project_ms,
                       "total_host": last.total_ms},
-        "roofline": {"bound": "tensor", "kernel": "k_gemm_f64 (sketch Y = D Omega)",
-                     "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                     "frac": achieved / peak,
-                     "peak_source": "measured in this run: torch float64 matmul 4096^3 (cuBLAS DGEMM); MEASURED_PEAKS.json has no FP64 figure",
-                     "traffic": None},
+        "roofline": roof,
         "clocks": clocks.summary(),
     }
     if dmml:

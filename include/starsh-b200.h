@@ -32,13 +32,15 @@ extern "C" {
 int starsh_blrm__drsdd_b200(STARSH_blrm **matrix, STARSH_blrf *format,
         int maxrank, double tol, int onfly);
 
-/* Same contract with an adaptive sketch width: Gaussian columns are drawn
- * in blocks (64, then 32), each block is projected off the basis built so
- * far and only directions above (tol/10)^2 ||D||_F^2 are kept; a tile stops
- * once a block leaves 10 columns below that threshold (a posterior
- * residual estimate) or its k = min(maxrank + oversample, m, n) columns are
- * used.  Low-rank tiles therefore pay for a few dozen sketch columns
- * instead of k.  Projection, small SVD and the rank decision are as in
+/* Same contract with an adaptive sketch width: sketch columns are drawn in
+ * blocks (64, then 32), each block is projected off the basis built so far
+ * and only directions above (tol/10)^2 of the block's energy are kept; a
+ * tile stops once a block leaves 10 columns below that threshold (a
+ * posterior residual estimate) or its k = min(maxrank + oversample, m, n)
+ * columns are used.  The sketch products run on the tcgen05 tensor cores
+ * as exact integer products of five-byte slices of D with an int8 sketch
+ * matrix (FP64-accurate to 2^-40 of each row's largest entry).
+ * Projection, small SVD and the rank decision are as in
  * starsh_blrm__drsdd_b200, all in FP64.  Selected by STARSH_LRENGINE=
  * RSVD_MP on the B200 backend. */
 int starsh_blrm__drsdd_b200_mp(STARSH_blrm **matrix, STARSH_blrf *format,
@@ -140,9 +142,11 @@ int starsh_b200_kernel_family(STARSH_kernel *kernel, int *ndim_hint);
  * without allocating any device memory.  No counterpart in the reference:
  * it is for callers that cannot call cudaMalloc (inside a stream capture,
  * under an allocator that owns all device memory, or on threads that must
- * not wait for the allocator's implicit synchronisation).  Same algorithm,
- * Gaussian sketch and rank rule as starsh_blrm__drsdd_b200 applied to that
- * tile; its scratch is a fixed __device__ array of about 2.1 MB that every
+ * not wait for the allocator's implicit synchronisation).  Same algorithm
+ * and Gaussian sketch as starsh_blrm__drsdd_b200 applied to that tile, with
+ * the reference's rank rule (the tail of the projected tile's spectrum: the
+ * batched engine also counts the energy its sketch missed, from the exact
+ * block norms of its generator); its scratch is a fixed __device__ array of about 2.1 MB that every
  * GPU loading the library keeps until the process exits.
  *   dD      nrows x ncols tile, column-major, leading dimension ldd;
  *   dU      receives nrows x rank, leading dimension nrows;
@@ -253,6 +257,9 @@ typedef struct starsh_b200_stats
     double basis_ms;          /* sketch and orthogonalisation, in all   */
     double svd_ms;            /* Gram of B, its factor, Jacobi, rank cut */
     double output_ms;         /* U = Q W and V written to the arena     */
+    double sketch_bytes;      /* algorithmic HBM bytes of the sketch:
+                                 D read once per round, Y written      */
+    int sketch_int8;          /* 1: sketch on the tcgen05 int8 path     */
 } starsh_b200_stats;
 int starsh_b200_get_stats(starsh_b200_stats *stats);
 

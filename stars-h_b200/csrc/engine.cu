@@ -428,6 +428,7 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
     const int k_max_all = k_max;   // Omega8's width (batches shadow k_max)
     // E[w^2] of the sketch entries: round(32 g) has variance 1024 + 1/12
     for (TileWork &t : all) t.omega_var = use_i8 ? 1024.0 + 1.0 / 12.0 : 1.0;
+    st.sketch_int8 = use_i8 ? 1 : 0;
 
     // Processing order: larger tiles first (a batch's workspace layout is
     // sized by its first tile), then by sketch width, then by cluster
@@ -679,6 +680,13 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
             TileWork &w = all[b0 + t];
             st.sketch_flops += 2.0 * w.m * w.n *
                 (ep.engine == STARSH_B200_FP64 ? w.k : w.cols_done);
+            {
+                // D is read once per round the tile takes part in, Y written
+                const int cols = ep.engine == STARSH_B200_FP64 ? w.k : w.cols_done;
+                const int rounds = ep.engine == STARSH_B200_FP64 ? 1
+                    : 1 + (std::max(0, cols - ep.block) + ep.block_next - 1) / ep.block_next;
+                st.sketch_bytes += 8.0 * ((double)w.m * w.n * rounds + (double)w.m * cols);
+            }
             st.project_flops += 2.0 * w.m * w.n * w.k1;
             if (w.status & TILE_MMA_TIMEOUT) {
                 set_error("tensor-core sketch timed out on a tile");

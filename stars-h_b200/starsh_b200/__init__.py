@@ -127,7 +127,8 @@ class Stats(Structure):
                 ("h2d_bytes", c_longlong), ("d2h_bytes", c_longlong),
                 ("batches", c_longlong), ("sketch_launches", c_longlong),
                 ("gen_ms", c_double), ("basis_ms", c_double),
-                ("svd_ms", c_double), ("output_ms", c_double)]
+                ("svd_ms", c_double), ("output_ms", c_double),
+                ("sketch_bytes", c_double), ("sketch_int8", c_int)]
 
 
 class ServerStats(Structure):

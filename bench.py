@@ -671,6 +671,26 @@ def _cpu_run(key, n):
     print(json.dumps({"seconds": dt, "entries": n * n, "rel_err": err}))
 
 
+# ------------------------------------------------------------- replicas
+
+def replica_rates(times, entries, world, device):
+    """Whole-job Mentries/s of `world` independent replicas (one per rank):
+    the entries of all ranks over the slowest rank's time, for each timed
+    quantity in `times` (seconds).  Returns (rates, max times).  Every rank
+    takes the same two all-reduce steps."""
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        tt = torch.tensor(list(times), dtype=torch.float64, device=device)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ee = torch.tensor([float(entries)], dtype=torch.float64, device=device)
+        dist.all_reduce(ee, op=dist.ReduceOp.SUM)
+        times, total = tt.tolist(), ee.item()
+    else:
+        times, total = list(times), float(entries)
+    return [total / t / 1e6 for t in times], times
+
+
 # ------------------------------------------------------------- device peak
 
 # DRAM bytes (read + write) of k_sketch_i8 over its algorithmic bytes, from
@@ -927,13 +947,8 @@ def main():
     barrier()
     t_e2e = statistics.mean(e2e_times)
     entries = last.entries
-    if world > 1:
-        tt = torch.tensor([t_dev, t_e2e, t_plain], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        t_dev, t_e2e, t_plain = tt.tolist()
-    value = world * entries / t_dev / 1e6
-    e2e_value = world * entries / t_e2e / 1e6
-    plain_value = world * entries / t_plain / 1e6
+    (value, e2e_value, plain_value), (t_dev, t_e2e, t_plain) = replica_rates(
+        [t_dev, t_e2e, t_plain], entries, world, "cuda")
 
     if rank != 0:
         if world > 1:

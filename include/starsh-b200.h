@@ -109,6 +109,25 @@ int starsh_b200_blrm_dmml_device(STARSH_blrm *matrix, int nrhs,
         double alpha, const double *dA, int lda, double beta, double *dB,
         int ldb, void *stream);
 
+/* ---------------------------------------------------- iterative solver */
+
+/* Conjugate gradients on M with host B and X (N x nrhs, cluster order):
+ * signature and iteration of starsh_itersolvers__dcg_omp (reference
+ * include/starsh.h:671-672, src/itersolvers/cg.c:24-95), every product a
+ * device dmml on the resident factors; `work` is not used.  Returns the
+ * iteration at which the last column converged, or -1 if it did not
+ * within N iterations (or on error: starsh_b200_last_error()). */
+int starsh_itersolvers__dcg_b200(STARSH_blrm *matrix, int nrhs, double *B,
+        int ldb, double *X, int ldx, double tol, double *work);
+
+/* The same on device B and X (X holds the initial guess and receives the
+ * solution) on `stream` (NULL: the library stream), at most maxiter
+ * iterations (<= 0: N); *iterations as above.  Returns STARSH_SUCCESS or
+ * an error. */
+int starsh_b200_dcg_device(STARSH_blrm *matrix, int nrhs, const double *dB,
+        int ldb, double *dX, int ldx, double tol, int maxiter, void *stream,
+        int *iterations);
+
 /* ------------------------------------------------- kernel registration */
 
 /* Device kernel families. */

@@ -187,6 +187,10 @@ class Ref:
                                           P(c_double), c_int, c_double,
                                           P(c_double), c_int]),
             ("starsh_blrm_free", None, [P(Blrm)]),
+            ("starsh_itersolvers__dcg_omp", c_int, [P(Blrm), c_int,
+                                                    P(c_double), c_int,
+                                                    P(c_double), c_int,
+                                                    c_double, P(c_double)]),
         ]:
             fn = getattr(L, name)
             fn.restype = res
@@ -277,6 +281,19 @@ class Ref:
             B.ctypes.data_as(POINTER(c_double)), n)
         assert info == 0
         return B
+
+    def cg(self, M, B, X0, tol):
+        """src/itersolvers/cg.c:24-95 (starsh_itersolvers__dcg_omp):
+        returns (iterations, X)."""
+        B = np.asfortranarray(B, dtype=np.float64)
+        n, nrhs = B.shape
+        X = np.asfortranarray(X0, dtype=np.float64).copy(order="F")
+        work = np.zeros(3 * n * nrhs + 3 * nrhs)
+        it = self.lib.starsh_itersolvers__dcg_omp(
+            M, nrhs, B.ctypes.data_as(POINTER(c_double)), n,
+            X.ctypes.data_as(POINTER(c_double)), n, tol,
+            work.ctypes.data_as(POINTER(c_double)))
+        return it, X
 
     def block(self, kernel, data, irow, icol, col_data=None):
         fn = ctypes.CFUNCTYPE(None, c_int, c_int, POINTER(STARSH_int),

@@ -198,9 +198,9 @@ static int ensure_record(STARSH_blrm *M, Context &ctx, Record **out)
 
 // ---------------------------------------------------------------- dmml
 
-static int dmml_device(STARSH_blrm *M, int nrhs, double alpha,
-                       const double *dA, int lda, double beta, double *dB,
-                       int ldb, cudaStream_t user_stream, Context &ctx)
+int dmml_device(STARSH_blrm *M, int nrhs, double alpha,
+                const double *dA, int lda, double beta, double *dB,
+                int ldb, cudaStream_t user_stream, Context &ctx)
 {
     if (M == nullptr || nrhs < 0 || dA == nullptr || dB == nullptr)
         return STARSH_WRONG_PARAMETER;

@@ -73,6 +73,11 @@ int upload_problem(DevicePoints &dp, STARSH_problem *P, STARSH_cluster *R,
 int gen_blocks(const DevKernel &K, const std::vector<BlockJob> &jobs,
                cudaStream_t s);
 Record *find_record(const STARSH_blrm *M);
+// B = alpha M A + beta B on the device (dmml_dfe.cu); the caller holds
+// ctx.lock.
+int dmml_device(STARSH_blrm *M, int nrhs, double alpha, const double *dA,
+                int lda, double beta, double *dB, int ldb,
+                cudaStream_t stream, Context &ctx);
 // Registers a record for M (replacing none); used for matrices whose
 // factors were uploaded from the host.
 void add_record(const STARSH_blrm *M, Record *rec);

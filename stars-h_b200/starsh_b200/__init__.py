@@ -184,6 +184,12 @@ def _proto(lib):
         "starsh_b200_server_pause": (c_int, [c_void_p, c_int]),
         "starsh_b200_server_get_stats": (c_int, [c_void_p, P(ServerStats)]),
         "starsh_b200_server_free": (c_int, [c_void_p]),
+        "starsh_itersolvers__dcg_b200": (c_int, [P(Blrm), c_int, c_void_p,
+                                                 c_int, c_void_p, c_int,
+                                                 c_double, c_void_p]),
+        "starsh_b200_dcg_device": (c_int, [P(Blrm), c_int, c_void_p, c_int,
+                                           c_void_p, c_int, c_double, c_int,
+                                           c_void_p, P(c_int)]),
         "starsh_b200_blrm_download": (c_int, [P(Blrm)]),
         "starsh_b200_blrm_release": (None, [P(Blrm)]),
         "starsh_b200_blrm_dmml_device": (c_int, [P(Blrm), c_int, c_double,

@@ -15,6 +15,7 @@
 #ifndef STARSH_B200_H
 #define STARSH_B200_H
 
+#include <stdio.h>
 #include "starsh.h"
 
 #ifdef __cplusplus
@@ -127,6 +128,31 @@ int starsh_itersolvers__dcg_b200(STARSH_blrm *matrix, int nrhs, double *B,
 int starsh_b200_dcg_device(STARSH_blrm *matrix, int nrhs, const double *dB,
         int ldb, double *dX, int ldx, double tol, int maxiter, void *stream,
         int *iterations);
+
+/* ------------------------------------------- serialised matrices */
+
+/* A STARSH_blrm as a byte stream (the reference has no serialised form):
+ * clusterings, block lists, ranks, factors and dense near blocks, ending
+ * in a 64-bit checksum.  Writing brings device-resident factors to the
+ * host first.  Reading binds the stream to `problem` (same shape and
+ * symmetry, else STARSH_WRONG_PARAMETER) and builds new clusterings, a new
+ * format and a host-resident matrix, all freed by
+ * starsh_b200_blrm_free_read(); a malformed, truncated or corrupted stream
+ * gives STARSH_FILE_WRONG_INPUT, a file that cannot be opened
+ * STARSH_FILE_NOT_EXIST.  starsh_b200_blrm_serialize() with buffer NULL
+ * only stores the stream's size in *nbytes; with a buffer smaller than the
+ * stream it returns STARSH_WRONG_PARAMETER (*nbytes = the size needed). */
+int starsh_b200_blrm_write_to_file(STARSH_blrm *matrix, const char *fname);
+int starsh_b200_blrm_write_to_file_pointer(STARSH_blrm *matrix, FILE *fp);
+int starsh_b200_blrm_serialize(STARSH_blrm *matrix, void *buffer,
+        size_t capacity, size_t *nbytes);
+int starsh_b200_blrm_read_from_file(STARSH_blrm **matrix,
+        STARSH_problem *problem, const char *fname);
+int starsh_b200_blrm_read_from_file_pointer(STARSH_blrm **matrix,
+        STARSH_problem *problem, FILE *fp);
+int starsh_b200_blrm_deserialize(STARSH_blrm **matrix,
+        STARSH_problem *problem, const void *buffer, size_t nbytes);
+void starsh_b200_blrm_free_read(STARSH_blrm *matrix);
 
 /* ------------------------------------------------- kernel registration */
 

@@ -5,6 +5,7 @@
  * point[d*count + i] is coordinate d of point i. */
 #ifndef STARSH_B200_PARTICLES_H
 #define STARSH_B200_PARTICLES_H
+#include <stdio.h>
 #include "starsh.h"
 
 #ifdef __cplusplus
@@ -47,6 +48,30 @@ int starsh_particles_generate_uniform(STARSH_particles **data,
         STARSH_int count, int ndim);
 int starsh_particles_generate_quasiuniform1(STARSH_particles **data,
         STARSH_int count, int ndim);
+/* Particle files in the reference's formats (src/applications/
+ * particles.c:789-1088): STARSH_ASCII, a "count=<n>, ndim=<d>" header and
+ * one line per point with "%lf" coordinates separated by ", " (six
+ * decimals, as the reference prints them); STARSH_BINARY, count (size_t),
+ * ndim (int) and the coordinate-major doubles.  Errors as the reference:
+ * STARSH_FILE_NOT_EXIST (cannot open), STARSH_FILE_WRONG_INPUT (malformed
+ * or short), STARSH_FPRINTF_ERROR / STARSH_FWRITE_ERROR (write failed),
+ * STARSH_WRONG_PARAMETER (unknown file type). */
+int starsh_particles_read_from_file(STARSH_particles **data,
+        const char *fname, const enum STARSH_FILE_TYPE ftype);
+int starsh_particles_read_from_file_pointer(STARSH_particles **data,
+        FILE *fp, const enum STARSH_FILE_TYPE ftype);
+int starsh_particles_read_from_file_pointer_ascii(STARSH_particles **data,
+        FILE *fp);
+int starsh_particles_read_from_file_pointer_binary(STARSH_particles **data,
+        FILE *fp);
+int starsh_particles_write_to_file(const STARSH_particles *data,
+        const char *fname, const enum STARSH_FILE_TYPE ftype);
+int starsh_particles_write_to_file_pointer(const STARSH_particles *data,
+        FILE *fp, const enum STARSH_FILE_TYPE ftype);
+int starsh_particles_write_to_file_pointer_ascii(const STARSH_particles *data,
+        FILE *fp);
+int starsh_particles_write_to_file_pointer_binary(const STARSH_particles *data,
+        FILE *fp);
 /* In-place Z-order (Morton) sort; reference src/applications/
  * particles.c:1090-1221. */
 int starsh_particles_zsort_inplace(STARSH_particles *data);

@@ -373,15 +373,22 @@ struct DfeJob {
     long long row0, col0;
     int m, n, r;
     const double *U, *V, *D;   // D: stored dense block or null
-    double *out;               // out[0] += ||D||^2, out[1] += ||D-UV^T||^2
 };
 
+// Each CTA stores its 64 x 64 piece's ||D||^2 and ||D - U V^T||^2 in its own
+// slot of `part` (slot = (job, tile row, tile column)); k_dfe_sum adds a
+// job's slots in a fixed order, so the error is the same on every run.
 __global__ void __launch_bounds__(256)
-k_dfe(DevKernel K, const DfeJob *__restrict__ jobs)
+k_dfe(DevKernel K, const DfeJob *__restrict__ jobs, double *__restrict__ part)
 {
     const DfeJob jb = jobs[blockIdx.z];
     const int i0 = blockIdx.x * 64, j0 = blockIdx.y * 64;
-    if (i0 >= jb.m || j0 >= jb.n) return;
+    double *slot = part + 2 * (((size_t)blockIdx.z * gridDim.y + blockIdx.y) *
+                               gridDim.x + blockIdx.x);
+    if (i0 >= jb.m || j0 >= jb.n) {
+        if (threadIdx.x == 0) slot[0] = slot[1] = 0.0;
+        return;
+    }
     __shared__ double Us[64][33];
     __shared__ double Vs[64][33];
     __shared__ double red[2][8];
@@ -435,9 +442,25 @@ k_dfe(DevKernel K, const DfeJob *__restrict__ jobs)
             a += red[0][w];
             b += red[1][w];
         }
-        atomicAdd(jb.out, a);
-        atomicAdd(jb.out + 1, b);
+        slot[0] = a;
+        slot[1] = b;
     }
+}
+
+// out[2 job + {0, 1}] = the sums of the job's nslot slots, in slot order.
+__global__ void k_dfe_sum(const double *__restrict__ part, int nslot,
+                          long long njobs, double *__restrict__ out)
+{
+    const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= njobs) return;
+    const double *p = part + 2 * (size_t)j * nslot;
+    double a = 0.0, b = 0.0;
+    for (int q = 0; q < nslot; ++q) {
+        a += p[2 * q];
+        b += p[2 * q + 1];
+    }
+    out[2 * j] = a;
+    out[2 * j + 1] = b;
 }
 
 static double dfe_device(STARSH_blrm *M, Context &ctx)
@@ -450,46 +473,54 @@ static double dfe_device(STARSH_blrm *M, Context &ctx)
     const STARSH_int nf = F->nblocks_far, nn = F->nblocks_near;
     const size_t njobs = nf + nn;
     if (njobs == 0) return 0.0;
-    double *sums = nullptr;
-    DfeJob *dj = nullptr;
-    if (cudaMallocAsync((void **)&sums, 2 * njobs * sizeof(double), s) ||
-        cudaMallocAsync((void **)&dj, njobs * sizeof(DfeJob), s)) {
-        cuda_fail(cudaGetLastError(), "cudaMallocAsync(dfe)");
-        return -1.0;
-    }
-    cudaMemsetAsync(sums, 0, 2 * njobs * sizeof(double), s);
     std::vector<DfeJob> jobs(njobs);
     int mmax = 0, nmax = 0;
     for (STARSH_int b = 0; b < nf; ++b) {
         const STARSH_int i = F->block_far[2 * b], j = F->block_far[2 * b + 1];
         jobs[b] = DfeJob{R->start[i], C->start[j], (int)R->size[i],
                          (int)C->size[j], M->far_rank[b], rec->dU[b],
-                         rec->dV[b], nullptr, sums + 2 * b};
+                         rec->dV[b], nullptr};
     }
     for (STARSH_int b = 0; b < nn; ++b) {
         const STARSH_int i = F->block_near[2 * b], j = F->block_near[2 * b + 1];
         jobs[nf + b] = DfeJob{R->start[i], C->start[j], (int)R->size[i],
                               (int)C->size[j], 0, nullptr, nullptr,
-                              M->onfly ? nullptr : rec->dD[b],
-                              sums + 2 * (nf + b)};
+                              M->onfly ? nullptr : rec->dD[b]};
     }
     for (const auto &j : jobs) {
         mmax = std::max(mmax, j.m);
         nmax = std::max(nmax, j.n);
     }
+    const int gx = (mmax + 63) / 64, gy = (nmax + 63) / 64;
+    const size_t nslot = (size_t)gx * gy;
+    double *sums = (double *)pool_alloc(2 * njobs * sizeof(double), s);
+    double *part = (double *)pool_alloc(2 * njobs * nslot * sizeof(double), s);
+    DfeJob *dj = (DfeJob *)pool_alloc(njobs * sizeof(DfeJob), s);
+    if (!sums || !part || !dj) {
+        pool_free(sums);
+        pool_free(part);
+        pool_free(dj);
+        cuda_fail(cudaErrorMemoryAllocation, "dfe buffers");
+        return -1.0;
+    }
     cudaMemcpyAsync(dj, jobs.data(), njobs * sizeof(DfeJob),
                     cudaMemcpyHostToDevice, s);
     for (size_t b0 = 0; b0 < njobs; b0 += 65535) {
         const unsigned nb = (unsigned)std::min<size_t>(65535, njobs - b0);
-        dim3 grid((mmax + 63) / 64, (nmax + 63) / 64, nb);
-        k_dfe<<<grid, 256, 0, s>>>(rec->points->K, dj + b0);
+        dim3 grid(gx, gy, nb);
+        k_dfe<<<grid, 256, 0, s>>>(rec->points->K, dj + b0,
+                                   part + 2 * b0 * nslot);
         count_launch();
     }
+    k_dfe_sum<<<(unsigned)((njobs + 255) / 256), 256, 0, s>>>(
+        part, (int)nslot, (long long)njobs, sums);
+    count_launch();
     std::vector<double> h(2 * njobs);
     cudaMemcpyAsync(h.data(), sums, 2 * njobs * sizeof(double),
                     cudaMemcpyDeviceToHost, s);
-    cudaFreeAsync(sums, s);
-    cudaFreeAsync(dj, s);
+    pool_free(sums);
+    pool_free(part);
+    pool_free(dj);
     cudaError_t e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) {
         cuda_fail(e, "dfe kernels");

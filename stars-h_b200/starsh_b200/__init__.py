@@ -191,6 +191,18 @@ def _proto(lib):
                                            c_void_p, c_int, c_double, c_int,
                                            c_void_p, P(c_int)]),
         "starsh_b200_blrm_download": (c_int, [P(Blrm)]),
+        "starsh_b200_blrm_write_to_file": (c_int, [P(Blrm), c_char_p]),
+        "starsh_b200_blrm_write_to_file_pointer": (c_int, [P(Blrm), c_void_p]),
+        "starsh_b200_blrm_serialize": (c_int, [P(Blrm), c_void_p, c_size_t,
+                                               P(c_size_t)]),
+        "starsh_b200_blrm_read_from_file": (c_int, [P(P(Blrm)), c_void_p,
+                                                    c_char_p]),
+        "starsh_b200_blrm_read_from_file_pointer": (c_int, [P(P(Blrm)),
+                                                            c_void_p,
+                                                            c_void_p]),
+        "starsh_b200_blrm_deserialize": (c_int, [P(P(Blrm)), c_void_p,
+                                                 c_void_p, c_size_t]),
+        "starsh_b200_blrm_free_read": (None, [P(Blrm)]),
         "starsh_b200_blrm_release": (None, [P(Blrm)]),
         "starsh_b200_blrm_dmml_device": (c_int, [P(Blrm), c_int, c_double,
                                                  c_void_p, c_int, c_double,
@@ -237,6 +249,14 @@ def _proto(lib):
                                           P(c_double)]),
         "starsh_particles_zsort_inplace": (c_int, [P(Particles)]),
         "starsh_particles_free": (None, [P(Particles)]),
+        "starsh_particles_read_from_file": (c_int, [P(P(Particles)), c_char_p,
+                                                    c_int]),
+        "starsh_particles_read_from_file_pointer": (c_int, [P(P(Particles)),
+                                                            c_void_p, c_int]),
+        "starsh_particles_write_to_file": (c_int, [P(Particles), c_char_p,
+                                                   c_int]),
+        "starsh_particles_write_to_file_pointer": (c_int, [P(Particles),
+                                                           c_void_p, c_int]),
         "starsh_blrm_get_block": (c_int, [P(Blrm), STARSH_int, STARSH_int,
                                           P(c_int), P(c_int), P(c_void_p),
                                           P(c_void_p), P(c_void_p)]),

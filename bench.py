@@ -556,7 +556,9 @@ def run_c5(args, lib, clocks):
 
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed
-    region (every 200 ms)."""
+    region: one looping `nvidia-smi -lms 200` started before it (its start-up
+    is over when the first sample arrives, before any timed step) and
+    stopped after it."""
 
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,"
              "clocks_event_reasons.hw_slowdown,"
@@ -567,29 +569,42 @@ class ClockSampler:
     def __init__(self, index):
         self.index = index
         self.samples = []
-        self._stop = threading.Event()
+        self._start = 0
+        self._proc = None
         self._t = None
+        self._first = threading.Event()
 
-    def _run(self):
-        while not self._stop.is_set():
-            try:
-                out = subprocess.run(
-                    ["nvidia-smi", "-i", str(self.index),
-                     f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits"],
-                    capture_output=True, text=True, timeout=5).stdout.strip()
-                self.samples.append([x.strip() for x in out.split(",")])
-            except Exception:
-                pass
-            self._stop.wait(0.2)
+    def _read(self):
+        for line in self._proc.stdout:
+            self.samples.append([x.strip() for x in line.split(",")])
+            self._first.set()
+        self._first.set()
 
     def __enter__(self):
-        self._t = threading.Thread(target=self._run, daemon=True)
+        try:
+            self._proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index),
+                 f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            return self
+        self._t = threading.Thread(target=self._read, daemon=True)
         self._t.start()
+        self._first.wait(10.0)
+        self._start = len(self.samples)
         return self
 
     def __exit__(self, *a):
-        self._stop.set()
-        self._t.join()
+        if self._proc is None:
+            return
+        self._proc.terminate()
+        try:
+            self._proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self._proc.kill()
+            self._proc.wait()
+        self._t.join(timeout=5)
 
     def summary(self):
         def num(x):
@@ -597,7 +612,10 @@ class ClockSampler:
                 return float(x)
             except ValueError:
                 return None
-        good = [s for s in self.samples if len(s) > 7]
+        # samples of the timed region (the last earlier one if it was
+        # shorter than the sampling period)
+        timed = self.samples[self._start:] or self.samples[-1:]
+        good = [s for s in timed if len(s) > 7]
         sm = [v for v in (num(s[1]) for s in good) if v is not None]
         mx = [v for v in (num(s[2]) for s in good) if v is not None]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
@@ -606,7 +624,7 @@ class ClockSampler:
                           if s[4 + i].lower() == "active"})
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.samples)}
+                "reasons": reasons, "samples": len(timed)}
 
 
 class _Null:

@@ -222,6 +222,7 @@ k_sketch_i8(const __grid_constant__ CUtensorMap dmap,
     double *stage = reinterpret_cast<double *>(Bsm + (size_t)nc * npad_max);
     const uint32_t ncols_alloc = nc * kSlices <= 128 ? 128
                                : nc * kSlices <= 256 ? 256 : 512;
+    constexpr uint32_t kStageBytes = kStage * sizeof(double);
 
     if (t == 0) {
         failed = 0;
@@ -232,6 +233,11 @@ k_sketch_i8(const __grid_constant__ CUtensorMap dmap,
         for (int q = 0; q < 2; ++q)
             asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&abar[q])), "r"(kSkThreads));
         asm volatile("fence.mbarrier_init.release.cluster;");
+        // the first kStages chunks of D are requested before anything else
+        // (Omega, row scales, TMEM): their copies overlap that set-up
+        for (int q = 0; q < kStages && q < nchunks; ++q)
+            tma_load_d(stage + q * kStage, &dmap, row0, q * kSkChunk, tw.slot,
+                       &stbar[q], kStageBytes);
     }
     if (t < kSkMaxN) colsum[t] = 0;
     if (warp == 0) {
@@ -288,24 +294,24 @@ k_sketch_i8(const __grid_constant__ CUtensorMap dmap,
     const uint32_t idesc = idesc_i8(nc);
     // chunk kc of D (128 rows x 32 columns) lands in stage kc % kStages by
     // one TMA copy; rows past m_max / columns past n_max read as zero, rows in
-    // [m, m_max) and columns in [n, n_max) are masked below
-    constexpr uint32_t kStageBytes = kStage * sizeof(double);
-    if (t == 0)
-        for (int q = 0; q < kStages - 1 && q < nchunks; ++q)
-            tma_load_d(stage + q * kStage, &dmap, row0, q * kSkChunk, tw.slot,
-                       &stbar[q], kStageBytes);
+    // [m, m_max) and columns in [n, n_max) are masked below.
     // No block-wide barrier per chunk: every thread waits for its chunk's
     // data (stbar) and for the MMAs that read its digit buffer two chunks
     // ago (mbar), writes its digits and arrives on abar; thread 0 alone
     // waits for all 512 arrivals, issues the chunk's MMAs and the TMA copy
-    // of a later chunk (whose stage the previous chunk's converters have
-    // all left, as their arrivals show).  Each wait gives up after a bound
-    // or as soon as another thread has given up (failed).
-    int last_commit = -1;               // thread 0's view
+    // of chunk kc + kStages into the stage chunk kc has just left (every
+    // converter has read its values before arriving), so kStages chunks
+    // are in flight.  Each wait gives up after a bound or as soon as
+    // another thread has given up (failed).
+    // thread 0's view: the last chunk whose MMAs it committed, how many
+    // chunks it has requested and how many of those it has seen land
+    int last_commit = -1;
+    int issued = min(kStages, nchunks), landed = 0;
     for (int kc = 0; kc < nchunks; ++kc) {
         const int b = kc & 1;
         const int sg = kc % kStages;
         bool ok = mbar_wait_or(&stbar[sg], (kc / kStages) & 1, &failed);
+        if (ok && t == 0) landed = kc + 1;
         ok = ok && (kc < 2 || mbar_wait_or(&mbar[b], ((kc >> 1) - 1) & 1, &failed));
         if (ok) {
             // this thread: row r, columns 8 qd .. 8 qd + 7 of the chunk
@@ -347,12 +353,13 @@ k_sketch_i8(const __grid_constant__ CUtensorMap dmap,
             }
             mma_commit(&mbar[b]);
             last_commit = kc;
-            const int pf = kc + kStages - 1;
+            const int pf = kc + kStages;
             if (pf < nchunks) {
                 asm volatile("fence.proxy.async.shared::cta;");
                 tma_load_d(stage + (pf % kStages) * kStage, &dmap, row0,
                            pf * kSkChunk, tw.slot, &stbar[pf % kStages],
                            kStageBytes);
+                issued = pf + 1;
             }
         }
         if (failed) break;
@@ -362,9 +369,15 @@ k_sketch_i8(const __grid_constant__ CUtensorMap dmap,
     if (!failed) {
         const int last = nchunks - 1;
         if (!mbar_wait_or(&mbar[last & 1], (last >> 1) & 1, &failed)) failed = 1;
-    } else if (t == 0 && last_commit >= 0) {
+    } else if (t == 0) {
+        // after a failure: the MMAs issued and the D copies still in
+        // flight into shared memory finish (bounded waits) before the CTA
+        // releases TMEM and exits
         int dummy = 0;
-        mbar_wait_or(&mbar[last_commit & 1], (last_commit >> 1) & 1, &dummy);
+        if (last_commit >= 0)
+            mbar_wait_or(&mbar[last_commit & 1], (last_commit >> 1) & 1, &dummy);
+        for (int q = landed; q < issued; ++q)
+            mbar_wait_or(&stbar[q % kStages], (q / kStages) & 1, &dummy);
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();

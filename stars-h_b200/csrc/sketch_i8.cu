@@ -8,31 +8,40 @@
 // [-127, 127]); any such matrix is a valid sketch.  Row i of a tile is
 // scaled by 2^-e_i, e_i the exponent of the row's largest |D_ij| (from the
 // generator's per-row maxima), so x = D_ij 2^-e_i lies in (-1, 1); x is
-// rounded to q = round(x 2^39) and written with an offset as the 40-bit
-// unsigned integer q' = q + 2^39, whose five bytes u_0..u_4 are the digits:
-//     D_ij = 2^(e_i - 39) (sum_s 256^s u_s[i, j] - 2^39) + err,
+// rounded to the 40-bit integer q = round(x 2^39), written in two's
+// complement as four unsigned bytes u_0..u_3 and a signed top byte t:
+//     D_ij = 2^(e_i - 39) (sum_{s<4} 256^s u_s[i, j] + 2^32 t[i, j]) + err,
 //     |err| <= 2^-40 2^e_i.
-// Each digit matrix times Omega is an exact uint8 x int8 -> int32 product
-// (|sum| <= 255 * 127 * n < 2^31 for n <= 8192) on tcgen05.mma kind::i8,
-// accumulated in TMEM, one accumulator per digit.  The epilogue removes the
-// offset exactly (2^39 = 128 * 2^32: the top digit's product less 128 times
-// the column sums of Omega), recombines the digits in int64 (exact, |T| <
-// 2^61) and converts once:
-//     Y_ic = 2^(e_i - 39) T_ic,  T_ic = sum_s 256^s P_s - 2^39 sum_j Omega_jc.
+// Each digit matrix times Omega is an exact 8-bit x int8 -> int32 product
+// (|sum| <= 255 * 127 * n < 2^31 for n <= 8192) on tcgen05.mma kind::i8
+// (unsigned A for u_s, signed A for t), accumulated in TMEM, one
+// accumulator per digit.  The epilogue recombines the digits in int64
+// (exact) and converts once:
+//     Y_ic = 2^(e_i - 39) T_ic,  T_ic = sum_{s<4} 256^s P_s + 2^32 P_t.
 // The only error is the rounding of q: 2^-40 of the row maximum per entry,
 // far below the tolerance-driven thresholds of the adaptive basis (the
 // rank decision itself uses the FP64 projection and the exact block norm).
 //
-// One CTA per (tile, 128-row block), 512 threads.  The tile's rows are
-// read from HBM once, in K chunks of 32 columns, each brought into a
-// three-stage shared-memory buffer by one TMA tile copy (the copies of the
-// next two chunks overlap the work on this one); every thread converts 8
-// columns of one row into digits and stores them in the no-swizzle K-major
-// core-matrix layout; one thread issues the 5 MMAs (M 128, N nc, K 32) of
-// the chunk and commits them to the chunk buffer's mbarrier, so the
-// conversion of the next chunk overlaps the MMAs (two digit buffers); the
-// chunks are handed over through mbarriers, without block-wide barriers.
-// Omega's nc columns for the tile (nc x n bytes) stay in shared memory.
+// Persistent and warp-specialized: one CTA of 704 threads per SM walks the
+// work items (tile, 128-row block) of the launch.  Each item's rows are read
+// from HBM once, in K chunks of 32 columns:
+//   * warp 16 (producer) brings chunk after chunk into a five-stage ring by
+//     TMA tile copies, the 128 x 32 FP64 box of D and the 32 x nc bytes of
+//     Omega of the same columns, continuing across items;
+//   * warps 0-15 (converters) turn a landed chunk into the five digit
+//     matrices (each thread 8 columns of one row) in the no-swizzle K-major
+//     core-matrix layout of one of two digit buffers;
+//   * warp 17 (MMA) issues the chunk's five MMAs (M 128, N nc, K 32) and
+//     commits them to the barriers that free the stage and the digit buffer
+//     (and, after an item's last chunk, to the accumulator barrier);
+//   * warps 18-21 (epilogue) read an item's accumulators from TMEM, write
+//     Y and release TMEM to the next item, while the copies and the
+//     conversion of that item's first chunks go on.
+// Hand-over is by mbarriers only; every wait gives up after about two
+// seconds or as soon as another thread has given up, and the CTA then
+// marks its tile TILE_MMA_TIMEOUT, waits for its own copies and MMAs in
+// flight and releases TMEM.
+#include <algorithm>
 #include <cstdint>
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -41,11 +50,19 @@
 namespace b200 {
 
 constexpr int kSlices = 5;             // bytes (digits) per entry
-constexpr int kSkRows = 128;           // rows per CTA (MMA M)
+constexpr int kSkRows = 128;           // rows per item (MMA M)
 constexpr int kSkChunk = 32;           // K columns per chunk (one MMA K)
-constexpr int kSkThreads = 512;
 constexpr int kSkMaxN = 64;            // sketch columns per launch
-constexpr int kStages = 3;             // D chunks in flight (TMA stages)
+constexpr int kStages = 5;             // D / Omega chunks in flight
+constexpr int kAbufs = 2;              // digit buffers
+constexpr int kConvThreads = 512;      // warps 0-15
+constexpr int kProducerWarp = 16;
+constexpr int kMmaWarp = 17;
+constexpr int kEpiWarp0 = 18;          // warps 18-21
+constexpr int kSkThreads = 22 * 32;
+constexpr int kAbufBytes = kSlices * kSkRows * kSkChunk;                // 20 KB
+constexpr int kDStageBytes = kSkRows * kSkChunk * (int)sizeof(double);  // 32 KB
+constexpr int kOmSlotBytes = kSkChunk * kSkMaxN;                        // 2 KB
 
 // Shared-memory descriptor of a K-major operand without swizzle:
 // core matrices of 8 rows x 16 bytes (128 contiguous bytes), lbo = byte
@@ -62,12 +79,13 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo,
     return d;                          // base offset 0, no swizzle
 }
 
-// Instruction descriptor: int32 accumulator, unsigned int8 A (digits),
-// signed int8 B (Omega), both K-major, M = 128, N = n.
-__host__ __device__ constexpr uint32_t idesc_i8(int n)
+// Instruction descriptor: int32 accumulator, int8 A (unsigned digits, or
+// the signed top digit), signed int8 B (Omega), both K-major, M = 128,
+// N = n.
+__host__ __device__ constexpr uint32_t idesc_i8(int n, bool a_signed)
 {
-    return (2u << 4) | (0u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) |
-           ((uint32_t)(kSkRows >> 4) << 24);
+    return (2u << 4) | ((a_signed ? 1u : 0u) << 7) | (1u << 10) |
+           ((uint32_t)(n >> 3) << 17) | ((uint32_t)(kSkRows >> 4) << 24);
 }
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p)
@@ -84,10 +102,17 @@ __device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t da,
                  :: "r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(accumulate));
 }
 
+// Arrives (once) on mbar when every MMA this thread issued so far is done.
 __device__ __forceinline__ void mma_commit(uint64_t *mbar)
 {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
                  :: "r"(smem_u32(mbar)));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *mbar, int count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;"
+                 :: "r"(smem_u32(mbar)), "r"(count));
 }
 
 __device__ __forceinline__ bool mbar_try(uint64_t *mbar, uint32_t parity)
@@ -101,16 +126,8 @@ __device__ __forceinline__ bool mbar_try(uint64_t *mbar, uint32_t parity)
 }
 
 // Waits for the completion of the phase of the given parity; gives up
-// after about two seconds and returns false.
-__device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity)
-{
-    const long long t0 = clock64();
-    while (!mbar_try(mbar, parity))
-        if (clock64() - t0 > (1ll << 32)) return false;
-    return true;
-}
-
-// The same, also giving up as soon as *abort is set by another thread.
+// after about two seconds, or as soon as *abort is set by another thread,
+// and returns false.
 __device__ __forceinline__ bool mbar_wait_or(uint64_t *mbar, uint32_t parity,
                                              volatile int *abort)
 {
@@ -128,33 +145,37 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *mbar)
                  :: "r"(smem_u32(mbar)) : "memory");
 }
 
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16])
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *mbar, uint32_t bytes)
 {
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-                 "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                 :: "r"(smem_u32(mbar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[8])
+{
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 "
+                 "{%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
                  : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]),
-                   "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-                   "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
-                   "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+                   "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
                  : "r"(taddr));
 }
 
-// Digits of 8 entries x in (-1, 1): q' = round(x 2^39) + 2^39 < 2^40 by
-// the magic-number rounding (adding 1.5 2^52 leaves the integer in the low
-// mantissa bits), then byte s of the four q' of columns 4c .. 4c + 3 goes
-// to word w[s][c].
+// Digits of 8 entries x in (-1, 1), given as y = x 2^39 + 1.5 2^52 (one
+// rounding; y lies in [2^52, 2^53), so its mantissa field is the integer
+// 2^51 + q, q = round(x 2^39)): the low word of y's bit pattern is q mod
+// 2^32 and the high word less 0x43380000 is floor(q / 2^32) in [-128, 128]
+// (q = 2^39 is clamped to 2^39 - 1).  Byte s < 4 of the low words of
+// columns 4g .. 4g + 3 goes to w[s][g], the signed top bytes to w[4][g].
 __device__ __forceinline__ void digits8(const double (&y)[8],
                                         uint32_t (&w)[kSlices][2])
 {
-    // y = x 2^39 + 2^39 + 1.5 2^52 (one rounding): the low word of y's bit
-    // pattern is the low word of q', the high word less 0x43380000 its top
-    // byte (q' = 2^40 after rounding is clamped to 2^40 - 1)
     uint32_t lo[8], hi[8];
     #pragma unroll
     for (int c = 0; c < 8; ++c) {
         lo[c] = (uint32_t)__double2loint(y[c]);
-        hi[c] = (uint32_t)__double2hiint(y[c]) - 0x43380000u;
-        if (hi[c] > 255u) { hi[c] = 255u; lo[c] = 0xFFFFFFFFu; }
+        int top = __double2hiint(y[c]) - 0x43380000;
+        if (top > 127) { top = 127; lo[c] = 0xFFFFFFFFu; }
+        hi[c] = (uint32_t)top;
     }
     #pragma unroll
     for (int g = 0; g < 2; ++g) {
@@ -171,15 +192,12 @@ __device__ __forceinline__ void digits8(const double (&y)[8],
     }
 }
 
-// One TMA tile copy (this CTA only) of the 128 x 32 FP64 box at (row0,
-// col0, slot) of the workspace's D tensor into shared memory, completing
-// on mbar with its byte count.
+// TMA tile copy (this CTA only) of the 128 x 32 FP64 box at (row0, col0,
+// slot) of the workspace's D tensor; completes on mbar.
 __device__ __forceinline__ void tma_load_d(void *dst, const CUtensorMap *map,
                                            int row0, int col0, int slot,
-                                           uint64_t *mbar, uint32_t bytes)
+                                           uint64_t *mbar)
 {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
-                 :: "r"(smem_u32(mbar)), "r"(bytes) : "memory");
     asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes "
                  "[%0], [%1, {%2, %3, %4}], [%5];"
                  :: "r"(smem_u32(dst)), "l"(map), "r"(row0), "r"(col0), "r"(slot),
@@ -187,256 +205,312 @@ __device__ __forceinline__ void tma_load_d(void *dst, const CUtensorMap *map,
                  : "memory");
 }
 
-// Y(:, 0:bcur) of every tile with an active round = D * Omega8(:, cols_done
-// + (0:nc)), rows in 128-row blocks (blockIdx.x), tiles in blockIdx.y.
-__global__ void __launch_bounds__(kSkThreads, 1)
-k_sketch_i8(const __grid_constant__ CUtensorMap dmap,
-            const TileWork *__restrict__ tiles, Workspace ws,
-            const int8_t *__restrict__ om8, int ld_om8, int om8_cols, int nc)
+// TMA tile copy of the 16 (rows k) x nc (columns c) byte box of Omega8 at
+// (k0, c0): nc rows of 16 bytes, i.e. nc / 8 core matrices of one K half.
+__device__ __forceinline__ void tma_load_om(void *dst, const CUtensorMap *map,
+                                            int k0, int c0, uint64_t *mbar)
 {
-    extern __shared__ __align__(1024) uint8_t sk_smem_raw[];
-    __shared__ __align__(8) uint64_t mbar[2];     // MMAs done with A buffer
-    __shared__ __align__(8) uint64_t stbar[kStages];  // D chunk landed in stage
-    __shared__ __align__(8) uint64_t abar[2];     // all digits of a chunk written
-    __shared__ uint32_t tmem_base;
-    __shared__ volatile int failed;
-    __shared__ int colsum[kSkMaxN];
+    asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes "
+                 "[%0], [%1, {%2, %3}], [%4];"
+                 :: "r"(smem_u32(dst)), "l"(map), "r"(k0), "r"(c0),
+                    "r"(smem_u32(mbar))
+                 : "memory");
+}
 
-    const TileWork tw = tiles[blockIdx.y];
-    const int row0 = blockIdx.x * kSkRows;
-    if (tw.bcur <= 0 || row0 >= tw.m) return;            // uniform
-    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
-    const int r = t & (kSkRows - 1), qd = t >> 7;        // row, column quarter
-    const int n = tw.n, m = tw.m;
-    const int npad = (n + kSkChunk - 1) / kSkChunk * kSkChunk;
-    const int nchunks = npad / kSkChunk;
-    constexpr int kAbuf = kSlices * kSkRows * kSkChunk;  // bytes per buffer
-    constexpr int kStage = kSkRows * kSkChunk;           // doubles per stage
-    // 1024-byte aligned base (the launch adds 1 KB of slack)
-    uint8_t *sk_smem = sk_smem_raw + ((1024u - (smem_u32(sk_smem_raw) & 1023u)) & 1023u);
-    uint8_t *Abuf = sk_smem;                             // [2][kSlices][4 KB]
-    uint8_t *Bsm = sk_smem + 2 * kAbuf;                  // nc x npad
-    // raw FP64 chunks (column-major, 128 rows), kStages stages: the copies
-    // of chunks kc + 1 .. kc + kStages - 1 run while chunk kc is converted
-    const int npad_max = (ws.n_max + kSkChunk - 1) / kSkChunk * kSkChunk;
-    double *stage = reinterpret_cast<double *>(Bsm + (size_t)nc * npad_max);
-    const uint32_t ncols_alloc = nc * kSlices <= 128 ? 128
-                               : nc * kSlices <= 256 ? 256 : 512;
-    constexpr uint32_t kStageBytes = kStage * sizeof(double);
-
-    if (t == 0) {
-        failed = 0;
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&mbar[0])), "r"(1));
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&mbar[1])), "r"(1));
-        for (int q = 0; q < kStages; ++q)
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&stbar[q])), "r"(1));
-        for (int q = 0; q < 2; ++q)
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&abar[q])), "r"(kSkThreads));
-        asm volatile("fence.mbarrier_init.release.cluster;");
-        // the first kStages chunks of D are requested before anything else
-        // (Omega, row scales, TMEM): their copies overlap that set-up
-        for (int q = 0; q < kStages && q < nchunks; ++q)
-            tma_load_d(stage + q * kStage, &dmap, row0, q * kSkChunk, tw.slot,
-                       &stbar[q], kStageBytes);
-    }
-    if (t < kSkMaxN) colsum[t] = 0;
-    if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
-                     :: "r"(smem_u32(&tmem_base)), "r"(ncols_alloc));
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
-    }
-    __syncthreads();
-    // Omega8 columns cols_done .. cols_done + nc of this tile, K-major core
-    // matrices: byte (c, k) at (k / 16) (nc 16) + (c / 8) 128 + (c % 8) 16
-    // + k % 16.  Columns past Omega8's width are zero.  colsum[c] sums the
-    // column as stored (padding rows included: their digits carry the
-    // offset too).
-    {
-        const int c0 = tw.cols_done;
-        const int units = nc * (npad / 16);
-        for (int u = t; u < units; u += kSkThreads) {
-            const int c = u % nc, k16 = u / nc;
-            uint4 v = make_uint4(0u, 0u, 0u, 0u);
-            if (c0 + c < om8_cols)
-                v = *reinterpret_cast<const uint4 *>(
-                    om8 + (size_t)(c0 + c) * ld_om8 + (size_t)k16 * 16);
-            *reinterpret_cast<uint4 *>(Bsm + (size_t)k16 * (nc * 16) +
-                                       (c >> 3) * 128 + (c & 7) * 16) = v;
-            int sum = 0;
-            const uint32_t wv[4] = {v.x, v.y, v.z, v.w};
-            #pragma unroll
-            for (int q = 0; q < 4; ++q)
-                sum += __dp4a((int)wv[q], 0x01010101, 0);
-            atomicAdd(&colsum[c], sum);
-        }
-    }
-    // row scale 2^-e, e the exponent of the row's largest |D_ij|
+// Exponent e of the largest |D_ij| of row i over the tile's n columns
+// (|D_ij| < 2^e), from the generator's per-64-column maxima; 0 for an
+// all-zero row or a row past the tile's m.
+__device__ __forceinline__ int row_exponent(const Workspace &ws, int m,
+                                            int n, int slot, int i)
+{
     int e = 0;
-    const int i = row0 + r;
     if (i < m) {
         const int ncb = (ws.n_max + 63) / 64;
-        const double *rm = ws.Rmx(tw.slot) + (size_t)i * ncb;
+        const double *rm = ws.Rmx(slot) + (size_t)i * ncb;
         double mx = 0.0;
         for (int cb = 0; cb < (n + 63) / 64; ++cb) mx = fmax(mx, rm[cb]);
         if (mx > 0.0) frexp(mx, &e);
     }
-    // y = D 2^(39 - e) + 2^39 + 1.5 2^52 in one fma (see digits8)
-    const double scale39 = ldexp(1.0, 39 - e);
-    const double magic = 0x1.8p52 + 0x1p39;
-    asm volatile("fence.proxy.async.shared::cta;");
+    return e;
+}
+
+// The tile fields the kernel reads, loaded once per item.
+struct SkItem {
+    int m, n, bcur, slot, cols_done;
+};
+
+__device__ __forceinline__ SkItem sk_item(const TileWork *tiles, int tile)
+{
+    const TileWork *w = tiles + tile;
+    return SkItem{w->m, w->n, w->bcur, w->slot, w->cols_done};
+}
+
+// Y(:, 0:bcur) of every tile with an active round = D * Omega8(:, cols_done
+// + (0:nc)); work items (tile, 128-row block) in tile-major order, items
+// blockIdx.x + q gridDim.x for this CTA.
+__global__ void __launch_bounds__(kSkThreads, 1)
+k_sketch_i8(const __grid_constant__ CUtensorMap dmap,
+            const __grid_constant__ CUtensorMap omap,
+            const TileWork *__restrict__ tiles, int ntiles, Workspace ws,
+            int nc)
+{
+    extern __shared__ __align__(1024) uint8_t sk_smem_raw[];
+    __shared__ __align__(8) uint64_t full[kStages];    // chunk landed
+    __shared__ __align__(8) uint64_t empty[kStages];   // chunk's MMAs done
+    __shared__ __align__(8) uint64_t afull[kAbufs];    // digits written
+    __shared__ __align__(8) uint64_t afree[kAbufs];    // digits consumed
+    __shared__ __align__(8) uint64_t accfull;          // item's MMAs done
+    __shared__ __align__(8) uint64_t accempty;         // TMEM read out
+    __shared__ uint32_t tmem_base;
+    __shared__ volatile int failed;
+
+    // 1024-byte aligned base (the launch adds 1 KB of slack)
+    uint8_t *base = sk_smem_raw + ((1024u - (smem_u32(sk_smem_raw) & 1023u)) & 1023u);
+    uint8_t *Abuf = base;                                                  // [2][5][4 KB]
+    double *Dst = reinterpret_cast<double *>(base + kAbufs * kAbufBytes);  // [5][32][128]
+    uint8_t *Om = base + kAbufs * kAbufBytes + kStages * kDStageBytes;     // [5][2 KB]
+
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    const int rpt = (ws.m_max + kSkRows - 1) / kSkRows;
+    const long long nitems = (long long)ntiles * rpt;
+    const uint32_t ncols_alloc = nc * kSlices <= 128 ? 128
+                               : nc * kSlices <= 256 ? 256 : 512;
+
+    if (t == 0) {
+        failed = 0;
+        for (int q = 0; q < kStages; ++q) {
+            mbar_init(&full[q], 1);
+            mbar_init(&empty[q], 1);
+        }
+        for (int b = 0; b < kAbufs; ++b) {
+            mbar_init(&afull[b], kConvThreads);
+            mbar_init(&afree[b], 1);
+        }
+        mbar_init(&accfull, 1);
+        mbar_init(&accempty, kSkRows);
+        asm volatile("fence.mbarrier_init.release.cluster;");
+    }
+    if (warp == kMmaWarp) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     :: "r"(smem_u32(&tmem_base)), "r"(ncols_alloc));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = tmem_base;
 
-    const double *D = ws.D(tw.slot);
-    const int ldD = ws.ldD();
-    const uint32_t idesc = idesc_i8(nc);
-    // chunk kc of D (128 rows x 32 columns) lands in stage kc % kStages by
-    // one TMA copy; rows past m_max / columns past n_max read as zero, rows in
-    // [m, m_max) and columns in [n, n_max) are masked below.
-    // No block-wide barrier per chunk: every thread waits for its chunk's
-    // data (stbar) and for the MMAs that read its digit buffer two chunks
-    // ago (mbar), writes its digits and arrives on abar; thread 0 alone
-    // waits for all 512 arrivals, issues the chunk's MMAs and the TMA copy
-    // of chunk kc + kStages into the stage chunk kc has just left (every
-    // converter has read its values before arriving), so kStages chunks
-    // are in flight.  Each wait gives up after a bound or as soon as
-    // another thread has given up (failed).
-    // thread 0's view: the last chunk whose MMAs it committed, how many
-    // chunks it has requested and how many of those it has seen land
-    int last_commit = -1;
-    int issued = min(kStages, nchunks), landed = 0;
-    for (int kc = 0; kc < nchunks; ++kc) {
-        const int b = kc & 1;
-        const int sg = kc % kStages;
-        bool ok = mbar_wait_or(&stbar[sg], (kc / kStages) & 1, &failed);
-        if (ok && t == 0) landed = kc + 1;
-        ok = ok && (kc < 2 || mbar_wait_or(&mbar[b], ((kc >> 1) - 1) & 1, &failed));
-        if (ok) {
-            // this thread: row r, columns 8 qd .. 8 qd + 7 of the chunk
-            const double *st = stage + sg * kStage;
-            double x[8];
-            #pragma unroll
-            for (int c = 0; c < 8; ++c) {
-                const int j = kc * kSkChunk + 8 * qd + c;
-                const double v = (i < m && j < n) ? st[(8 * qd + c) * kSkRows + r] : 0.0;
-                x[c] = fma(v, scale39, magic);
+    int fail_tile = -1;          // a tile whose item this thread gave up on
+    long long gc = 0;            // chunks seen by this role (all items)
+    int it = 0;                  // items processed by this CTA
+
+    if (warp < kConvThreads / 32) {
+        // ---------------------------------------------------- converters
+        const int r = t & (kSkRows - 1), qd = t >> 7;
+        const double magic = 0x1.8p52;
+        for (long long item = blockIdx.x; item < nitems; item += gridDim.x) {
+            const int tile = (int)(item / rpt);
+            const SkItem w = sk_item(tiles, tile);
+            const int row0 = (int)(item % rpt) * kSkRows;
+            if (w.bcur <= 0 || row0 >= w.m) continue;
+            const int nchunks = (w.n + kSkChunk - 1) / kSkChunk;
+            const int i = row0 + r;
+            // x = D 2^(39 - e) (two exact power-of-two factors when 39 - e
+            // is beyond the double range), y = x + 1.5 2^52 in one fma
+            const int sh = 39 - row_exponent(ws, w.m, w.n, w.slot, i);
+            const double s1 = sh > 1000 ? ldexp(1.0, sh - 1000) : 1.0;
+            const double s2 = ldexp(1.0, sh > 1000 ? 1000 : sh);
+            for (int kc = 0; kc < nchunks; ++kc, ++gc) {
+                const int sg = (int)(gc % kStages), b = (int)(gc & 1);
+                bool ok = mbar_wait_or(&full[sg], (uint32_t)(gc / kStages) & 1, &failed);
+                ok = ok && (gc < kAbufs ||
+                            mbar_wait_or(&afree[b], (uint32_t)((gc >> 1) - 1) & 1, &failed));
+                if (!ok) {
+                    fail_tile = tile;
+                    failed = 1;
+                    break;
+                }
+                const double *st = Dst + (size_t)sg * (kSkRows * kSkChunk);
+                double y[8];
+                #pragma unroll
+                for (int c = 0; c < 8; ++c) {
+                    const int j = kc * kSkChunk + 8 * qd + c;
+                    double v = (i < w.m && j < w.n) ? st[(8 * qd + c) * kSkRows + r] : 0.0;
+                    if (sh > 1000) v *= s1;
+                    y[c] = fma(v, s2, magic);
+                }
+                uint32_t dg[kSlices][2];
+                digits8(y, dg);
+                uint8_t *A = Abuf + b * kAbufBytes;
+                #pragma unroll
+                for (int s = 0; s < kSlices; ++s)
+                    *reinterpret_cast<uint2 *>(A + s * (kSkRows * kSkChunk) +
+                                               (qd >> 1) * 2048 + (r >> 3) * 128 +
+                                               (r & 7) * 16 + (qd & 1) * 8) =
+                        make_uint2(dg[s][0], dg[s][1]);
+                asm volatile("fence.proxy.async.shared::cta;");
+                mbar_arrive(&afull[b]);
             }
-            uint32_t w[kSlices][2];
-            digits8(x, w);
-            uint8_t *A = Abuf + b * kAbuf;
-            #pragma unroll
-            for (int s = 0; s < kSlices; ++s)
-                *reinterpret_cast<uint2 *>(A + s * (kSkRows * kSkChunk) +
-                                           (qd >> 1) * 2048 + (r >> 3) * 128 +
-                                           (r & 7) * 16 + (qd & 1) * 8) =
-                    make_uint2(w[s][0], w[s][1]);
-            asm volatile("fence.proxy.async.shared::cta;");
+            if (failed) break;
+            ++it;
         }
-        mbar_arrive(&abar[b]);
-        if (!ok) { failed = 1; break; }
-        if (t == 0) {
-            if (!mbar_wait_or(&abar[b], (kc >> 1) & 1, &failed)) {
+    } else if (warp == kProducerWarp) {
+        // ------------------------------------------------------ producer
+        long long issued = 0;
+        if (lane == 0) {
+            const uint32_t bytes = kDStageBytes + 2 * 16 * nc;
+            for (long long item = blockIdx.x; item < nitems && !failed;
+                 item += gridDim.x) {
+                const int tile = (int)(item / rpt);
+                const SkItem w = sk_item(tiles, tile);
+                const int row0 = (int)(item % rpt) * kSkRows;
+                if (w.bcur <= 0 || row0 >= w.m) continue;
+                const int nchunks = (w.n + kSkChunk - 1) / kSkChunk;
+                for (int kc = 0; kc < nchunks; ++kc, ++gc) {
+                    const int sg = (int)(gc % kStages);
+                    if (gc >= kStages &&
+                        !mbar_wait_or(&empty[sg], (uint32_t)(gc / kStages - 1) & 1, &failed)) {
+                        fail_tile = tile;
+                        failed = 1;
+                        break;
+                    }
+                    mbar_expect_tx(&full[sg], bytes);
+                    tma_load_d(Dst + (size_t)sg * (kSkRows * kSkChunk), &dmap, row0,
+                               kc * kSkChunk, w.slot, &full[sg]);
+                    uint8_t *o = Om + sg * kOmSlotBytes;
+                    tma_load_om(o, &omap, kc * kSkChunk, w.cols_done, &full[sg]);
+                    tma_load_om(o + nc * 16, &omap, kc * kSkChunk + 16, w.cols_done,
+                                &full[sg]);
+                    issued = gc + 1;
+                }
+            }
+            // after a failure: the copies still in flight land before the
+            // CTA exits (bounded waits)
+            if (failed) {
+                int dummy = 0;
+                for (long long q = issued > kStages ? issued - kStages : 0; q < issued; ++q)
+                    mbar_wait_or(&full[q % kStages], (uint32_t)(q / kStages) & 1, &dummy);
+            }
+        }
+    } else if (warp == kMmaWarp) {
+        // ----------------------------------------------------------- MMA
+        long long last = -1;
+        if (lane == 0) {
+            const uint32_t idu = idesc_i8(nc, false), ids = idesc_i8(nc, true);
+            for (long long item = blockIdx.x; item < nitems && !failed;
+                 item += gridDim.x) {
+                const int tile = (int)(item / rpt);
+                const SkItem w = sk_item(tiles, tile);
+                const int row0 = (int)(item % rpt) * kSkRows;
+                if (w.bcur <= 0 || row0 >= w.m) continue;
+                const int nchunks = (w.n + kSkChunk - 1) / kSkChunk;
+                // the previous item's accumulators have been read out
+                bool ok = it == 0 || mbar_wait_or(&accempty, (uint32_t)(it - 1) & 1, &failed);
+                for (int kc = 0; ok && kc < nchunks; ++kc, ++gc) {
+                    const int sg = (int)(gc % kStages), b = (int)(gc & 1);
+                    if (!mbar_wait_or(&afull[b], (uint32_t)(gc >> 1) & 1, &failed)) {
+                        ok = false;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;");
+                    const uint8_t *A = Abuf + b * kAbufBytes;
+                    const uint64_t db = umma_desc(smem_u32(Om + sg * kOmSlotBytes),
+                                                  nc * 16, 128);
+                    #pragma unroll
+                    for (int s = 0; s < kSlices; ++s) {
+                        const uint64_t da = umma_desc(
+                            smem_u32(A + s * (kSkRows * kSkChunk)), 2048, 128);
+                        mma_i8(tmem + s * nc, da, db, s == kSlices - 1 ? ids : idu,
+                               kc > 0);
+                    }
+                    mma_commit(&empty[sg]);
+                    mma_commit(&afree[b]);
+                    if (kc == nchunks - 1) mma_commit(&accfull);
+                    last = gc;
+                }
+                if (!ok) {
+                    fail_tile = tile;
+                    failed = 1;
+                    break;
+                }
+                ++it;
+            }
+            // after a failure: the MMAs issued finish before TMEM is freed
+            if (failed && last >= 0) {
+                int dummy = 0;
+                mbar_wait_or(&afree[last & 1], (uint32_t)(last >> 1) & 1, &dummy);
+            }
+        }
+    } else {
+        // ------------------------------------------------------ epilogue
+        // warps kEpiWarp0 .. + 3: warp w may read TMEM lanes 32 (w % 4) ..
+        // 32 (w % 4) + 31, the item's rows of the same numbers
+        static_assert(kEpiWarp0 + 4 == kSkThreads / 32, "epilogue warps");
+        const int lq = warp & 3;
+        const int rr = 32 * lq + lane;
+        for (long long item = blockIdx.x; item < nitems; item += gridDim.x) {
+            const int tile = (int)(item / rpt);
+            const SkItem w = sk_item(tiles, tile);
+            const int row0 = (int)(item % rpt) * kSkRows;
+            if (w.bcur <= 0 || row0 >= w.m) continue;
+            const int i = row0 + rr;
+            const int e = row_exponent(ws, w.m, w.n, w.slot, i);
+            if (!mbar_wait_or(&accfull, (uint32_t)it & 1, &failed)) {
+                fail_tile = tile;
                 failed = 1;
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;");
-            uint8_t *A = Abuf + b * kAbuf;
-            #pragma unroll
-            for (int s = 0; s < kSlices; ++s) {
-                const uint64_t da = umma_desc(
-                    smem_u32(A + s * (kSkRows * kSkChunk)), 2048, 128);
-                const uint64_t db = umma_desc(
-                    smem_u32(Bsm + (size_t)(kc * 2) * (nc * 16)), nc * 16, 128);
-                mma_i8(tmem + s * nc, da, db, idesc, kc > 0);
+            double *Y = ws.Y(w.slot);
+            const int ldY = ws.ldM();
+            for (int g = 0; g < nc / 8; ++g) {
+                uint32_t v[kSlices][8];
+                #pragma unroll
+                for (int s = 0; s < kSlices; ++s)
+                    tmem_ld8(tmem + ((uint32_t)(32 * lq) << 16) + s * nc + 8 * g, v[s]);
+                asm volatile("tcgen05.wait::ld.sync.aligned;");
+                if (i < w.m) {
+                    #pragma unroll
+                    for (int c = 0; c < 8; ++c) {
+                        const int col = 8 * g + c;
+                        long long T = (long long)(int)v[kSlices - 1][c];
+                        #pragma unroll
+                        for (int s = kSlices - 2; s >= 0; --s)
+                            T = T * 256 + (long long)(int)v[s][c];
+                        if (col < w.bcur)
+                            Y[(size_t)col * ldY + i] = ldexp((double)T, e - 39);
+                    }
+                }
             }
-            mma_commit(&mbar[b]);
-            last_commit = kc;
-            const int pf = kc + kStages;
-            if (pf < nchunks) {
-                asm volatile("fence.proxy.async.shared::cta;");
-                tma_load_d(stage + (pf % kStages) * kStage, &dmap, row0,
-                           pf * kSkChunk, tw.slot, &stbar[pf % kStages],
-                           kStageBytes);
-                issued = pf + 1;
-            }
+            asm volatile("tcgen05.fence::before_thread_sync;");
+            mbar_arrive(&accempty);
+            ++it;
         }
-        if (failed) break;
     }
-    // the last commit covers every earlier MMA; after a failure thread 0
-    // waits for the MMAs it issued before TMEM is released
-    if (!failed) {
-        const int last = nchunks - 1;
-        if (!mbar_wait_or(&mbar[last & 1], (last >> 1) & 1, &failed)) failed = 1;
-    } else if (t == 0) {
-        // after a failure: the MMAs issued and the D copies still in
-        // flight into shared memory finish (bounded waits) before the CTA
-        // releases TMEM and exits
-        int dummy = 0;
-        if (last_commit >= 0)
-            mbar_wait_or(&mbar[last_commit & 1], (last_commit >> 1) & 1, &dummy);
-        for (int q = landed; q < issued; ++q)
-            mbar_wait_or(&stbar[q % kStages], (q / kStages) & 1, &dummy);
-    }
+
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
-    // warp w reads TMEM lanes 32 (w % 4) .. + 31 (rows) and the columns of
-    // group w / 4 (16 columns each)
-    const int lq = warp & 3, grp = warp >> 2;
-    if (!failed && grp < nc / 16) {
-        double *Y = ws.Y(tw.slot);
-        const int ldY = ws.ldM();
-        const int rr = row0 + 32 * lq + lane;
-        // r = t & 127 = 32 (w % 4) + lane: this thread's own row, so its
-        // exponent e is the row's
-        const int er = e;
-        uint32_t v[kSlices][16];
-        #pragma unroll
-        for (int s = 0; s < kSlices; ++s)
-            tmem_ld16(tmem + ((uint32_t)(32 * lq) << 16) + s * nc + 16 * grp, v[s]);
-        asm volatile("tcgen05.wait::ld.sync.aligned;");
-        if (rr < m) {
-            const double sc = ldexp(1.0, er - 39);
-            #pragma unroll
-            for (int c = 0; c < 16; ++c) {
-                const int col = 16 * grp + c;
-                long long T = (long long)(int)v[4][c] - 128ll * colsum[col];
-                #pragma unroll
-                for (int s = 3; s >= 0; --s) T = T * 256 + (long long)(int)v[s][c];
-                if (col < tw.bcur) Y[(size_t)col * ldY + rr] = (double)T * sc;
-            }
-        }
-    }
-    if (failed && t == 0) {
-        TileWork *tr = const_cast<TileWork *>(tiles) + blockIdx.y;
-        atomicOr(&tr->status, TILE_MMA_TIMEOUT);
-    }
-    asm volatile("tcgen05.fence::before_thread_sync;");
-    __syncthreads();
-    if (warp == 0)
+    if (fail_tile >= 0)
+        atomicOr(&const_cast<TileWork *>(tiles)[fail_tile].status, TILE_MMA_TIMEOUT);
+    if (warp == kMmaWarp)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
                      :: "r"(tmem), "r"(ncols_alloc));
 }
 
-size_t sketch_i8_smem(int nc, int n_max)
+static size_t sketch_i8_smem()
 {
-    const int npad = (n_max + kSkChunk - 1) / kSkChunk * kSkChunk;
-    return 2 * (size_t)kSlices * kSkRows * kSkChunk + (size_t)nc * npad +
-           kStages * (size_t)kSkRows * kSkChunk * sizeof(double) + 1024;
+    return (size_t)kAbufs * kAbufBytes + (size_t)kStages * kDStageBytes +
+           (size_t)kStages * kOmSlotBytes + 1024;
 }
 
 bool sketch_i8_fits(int nc, int n_max)
 {
     return nc > 0 && nc <= kSkMaxN && n_max <= 8192 &&
-           sketch_i8_smem((nc + 15) / 16 * 16, n_max) <= 227 * 1024;
+           sketch_i8_smem() <= 227 * 1024;
 }
 
-// Tensor map of the batch's D blocks as one 3-D FP64 tensor (rows, columns,
-// slots) with a 128 x 32 x 1 box; needs an even leading dimension (16-byte
-// strides).  Encoded through the driver entry point of the runtime.
-static bool d_tensor_map(CUtensorMap *map, const Workspace &ws, int nslots)
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
 {
     static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
     if (encode == nullptr) {
@@ -446,11 +520,20 @@ static bool d_tensor_map(CUtensorMap *map, const Workspace &ws, int nslots)
                                     cudaEnableDefault, &q) != cudaSuccess ||
             q != cudaDriverEntryPointSuccess || fn == nullptr) {
             cudaGetLastError();
-            return false;
+            return nullptr;
         }
         encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
     }
-    if (ws.ldD() % 2 != 0) return false;
+    return encode;
+}
+
+// Tensor map of the batch's D blocks as one 3-D FP64 tensor (rows, columns,
+// slots) with a 128 x 32 x 1 box; needs an even leading dimension (16-byte
+// strides).
+static bool d_tensor_map(CUtensorMap *map, const Workspace &ws, int nslots)
+{
+    auto encode = tensor_map_encoder();
+    if (encode == nullptr || ws.ldD() % 2 != 0) return false;
     const cuuint64_t dims[3] = {(cuuint64_t)ws.m_max, (cuuint64_t)ws.n_max,
                                 (cuuint64_t)nslots};
     const cuuint64_t strides[2] = {(cuuint64_t)ws.ldD() * sizeof(double),
@@ -463,19 +546,47 @@ static bool d_tensor_map(CUtensorMap *map, const Workspace &ws, int nslots)
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// Tensor map of Omega8 (ld_om8 rows k, om8_cols columns c, column-major
+// bytes) with a 16 x nc box: columns past om8_cols read as zero.
+static bool om_tensor_map(CUtensorMap *map, const int8_t *om8, int ld_om8,
+                          int om8_cols, int nc)
+{
+    auto encode = tensor_map_encoder();
+    if (encode == nullptr || ld_om8 % 16 != 0 || ((uintptr_t)om8 & 15u) != 0)
+        return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)ld_om8, (cuuint64_t)om8_cols};
+    const cuuint64_t strides[1] = {(cuuint64_t)ld_om8};
+    const cuuint32_t box[2] = {16, (cuuint32_t)nc};
+    const cuuint32_t estr[2] = {1, 1};
+    return encode(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, (void *)om8, dims,
+                  strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 bool launch_sketch_i8(const TileWork *d_tiles, int ntiles, Workspace ws,
                       const int8_t *om8, int ld_om8, int om8_cols, int ncols,
                       cudaStream_t stream)
 {
-    CUtensorMap map;
-    if (!d_tensor_map(&map, ws, ntiles)) return false;
     const int nc = (ncols + 15) / 16 * 16;
-    const size_t smem = sketch_i8_smem(nc, ws.n_max);
-    cudaFuncSetAttribute(k_sketch_i8, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)smem);
-    dim3 grid((ws.m_max + kSkRows - 1) / kSkRows, ntiles);
-    k_sketch_i8<<<grid, kSkThreads, smem, stream>>>(map, d_tiles, ws, om8,
-                                                    ld_om8, om8_cols, nc);
+    CUtensorMap dmap, omap;
+    if (!d_tensor_map(&dmap, ws, ntiles) ||
+        !om_tensor_map(&omap, om8, ld_om8, om8_cols, nc))
+        return false;
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0, count = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, dev);
+        cudaFuncSetAttribute(k_sketch_i8, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sketch_i8_smem());
+        sms = count > 0 ? count : 148;
+    }
+    const long long items = (long long)ntiles * ((ws.m_max + kSkRows - 1) / kSkRows);
+    const int grid = (int)std::min<long long>(sms, items);
+    if (grid <= 0) return true;
+    k_sketch_i8<<<grid, kSkThreads, sketch_i8_smem(), stream>>>(
+        dmap, omap, d_tiles, ntiles, ws, nc);
     return true;
 }
 

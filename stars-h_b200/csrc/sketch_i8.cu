@@ -263,6 +263,8 @@ k_sketch_i8(const __grid_constant__ CUtensorMap dmap,
     __shared__ __align__(8) uint64_t accempty;         // TMEM read out
     __shared__ uint32_t tmem_base;
     __shared__ volatile int failed;
+    __shared__ __align__(8) uint64_t expready[2];      // row exponents posted
+    __shared__ int rowexp[2][kSkRows];                 // ... for items it, it + 1
 
     // 1024-byte aligned base (the launch adds 1 KB of slack)
     uint8_t *base = sk_smem_raw + ((1024u - (smem_u32(sk_smem_raw) & 1023u)) & 1023u);
@@ -288,6 +290,8 @@ k_sketch_i8(const __grid_constant__ CUtensorMap dmap,
         }
         mbar_init(&accfull, 1);
         mbar_init(&accempty, kSkRows);
+        mbar_init(&expready[0], kSkRows);
+        mbar_init(&expready[1], kSkRows);
         asm volatile("fence.mbarrier_init.release.cluster;");
     }
     if (warp == kMmaWarp) {
@@ -308,16 +312,25 @@ k_sketch_i8(const __grid_constant__ CUtensorMap dmap,
         // ---------------------------------------------------- converters
         const int r = t & (kSkRows - 1), qd = t >> 7;
         const double magic = 0x1.8p52;
+        SkItem wn = sk_item(tiles, (int)(blockIdx.x / rpt));
         for (long long item = blockIdx.x; item < nitems; item += gridDim.x) {
             const int tile = (int)(item / rpt);
-            const SkItem w = sk_item(tiles, tile);
+            const SkItem w = wn;
+            if (item + gridDim.x < nitems)   // the next item's fields, early
+                wn = sk_item(tiles, (int)((item + gridDim.x) / rpt));
             const int row0 = (int)(item % rpt) * kSkRows;
             if (w.bcur <= 0 || row0 >= w.m) continue;
             const int nchunks = (w.n + kSkChunk - 1) / kSkChunk;
             const int i = row0 + r;
+            // the item's row exponents, posted ahead by the epilogue warps
+            if (!mbar_wait_or(&expready[it & 1], (uint32_t)(it >> 1) & 1, &failed)) {
+                fail_tile = tile;
+                failed = 1;
+                break;
+            }
             // x = D 2^(39 - e) (two exact power-of-two factors when 39 - e
             // is beyond the double range), y = x + 1.5 2^52 in one fma
-            const int sh = 39 - row_exponent(ws, w.m, w.n, w.slot, i);
+            const int sh = 39 - rowexp[it & 1][r];
             const double s1 = sh > 1000 ? ldexp(1.0, sh - 1000) : 1.0;
             const double s2 = ldexp(1.0, sh > 1000 ? 1000 : sh);
             for (int kc = 0; kc < nchunks; ++kc, ++gc) {
@@ -359,10 +372,13 @@ k_sketch_i8(const __grid_constant__ CUtensorMap dmap,
         long long issued = 0;
         if (lane == 0) {
             const uint32_t bytes = kDStageBytes + 2 * 16 * nc;
+            SkItem wn = sk_item(tiles, (int)(blockIdx.x / rpt));
             for (long long item = blockIdx.x; item < nitems && !failed;
                  item += gridDim.x) {
                 const int tile = (int)(item / rpt);
-                const SkItem w = sk_item(tiles, tile);
+                const SkItem w = wn;
+                if (item + gridDim.x < nitems)
+                    wn = sk_item(tiles, (int)((item + gridDim.x) / rpt));
                 const int row0 = (int)(item % rpt) * kSkRows;
                 if (w.bcur <= 0 || row0 >= w.m) continue;
                 const int nchunks = (w.n + kSkChunk - 1) / kSkChunk;
@@ -397,10 +413,13 @@ k_sketch_i8(const __grid_constant__ CUtensorMap dmap,
         long long last = -1;
         if (lane == 0) {
             const uint32_t idu = idesc_i8(nc, false), ids = idesc_i8(nc, true);
+            SkItem wn = sk_item(tiles, (int)(blockIdx.x / rpt));
             for (long long item = blockIdx.x; item < nitems && !failed;
                  item += gridDim.x) {
                 const int tile = (int)(item / rpt);
-                const SkItem w = sk_item(tiles, tile);
+                const SkItem w = wn;
+                if (item + gridDim.x < nitems)
+                    wn = sk_item(tiles, (int)((item + gridDim.x) / rpt));
                 const int row0 = (int)(item % rpt) * kSkRows;
                 if (w.bcur <= 0 || row0 >= w.m) continue;
                 const int nchunks = (w.n + kSkChunk - 1) / kSkChunk;
@@ -448,13 +467,36 @@ k_sketch_i8(const __grid_constant__ CUtensorMap dmap,
         static_assert(kEpiWarp0 + 4 == kSkThreads / 32, "epilogue warps");
         const int lq = warp & 3;
         const int rr = 32 * lq + lane;
-        for (long long item = blockIdx.x; item < nitems; item += gridDim.x) {
+        // The converters' row exponents: those of the first item, then,
+        // while an item's MMAs run, those of the next one.  Buffer
+        // (it + 1) & 1 last served item it - 1, whose conversion is over
+        // once its accumulators were full.
+        auto valid = [&](const SkItem &w, long long item) {
+            return w.bcur > 0 && (int)(item % rpt) * kSkRows < w.m;
+        };
+        auto next_valid = [&](long long item, SkItem &w) {
+            for (; item < nitems; item += gridDim.x) {
+                w = sk_item(tiles, (int)(item / rpt));
+                if (valid(w, item)) break;
+            }
+            return item;
+        };
+        auto post = [&](long long item, const SkItem &w, int b) {
+            rowexp[b][rr] = row_exponent(ws, w.m, w.n, w.slot,
+                                         (int)(item % rpt) * kSkRows + rr);
+            mbar_arrive(&expready[b]);
+        };
+        SkItem w{};
+        long long item = next_valid(blockIdx.x, w);
+        if (item < nitems) post(item, w, 0);
+        while (item < nitems) {
             const int tile = (int)(item / rpt);
-            const SkItem w = sk_item(tiles, tile);
+            SkItem wn{};
+            const long long nx = next_valid(item + gridDim.x, wn);
+            if (nx < nitems) post(nx, wn, (it + 1) & 1);
             const int row0 = (int)(item % rpt) * kSkRows;
-            if (w.bcur <= 0 || row0 >= w.m) continue;
             const int i = row0 + rr;
-            const int e = row_exponent(ws, w.m, w.n, w.slot, i);
+            const int e = rowexp[it & 1][rr];
             if (!mbar_wait_or(&accfull, (uint32_t)it & 1, &failed)) {
                 fail_tile = tile;
                 failed = 1;
@@ -485,6 +527,8 @@ k_sketch_i8(const __grid_constant__ CUtensorMap dmap,
             asm volatile("tcgen05.fence::before_thread_sync;");
             mbar_arrive(&accempty);
             ++it;
+            item = nx;
+            w = wn;
         }
     }
 

@@ -580,6 +580,50 @@ __device__ MaxLoc block_argmax(MaxLoc x, MaxLoc *red)
     return r;
 }
 
+// block_argmax of x and, in the same pass, the block sum of y (returned in
+// *sum; `reds` holds one double per warp).
+__device__ MaxLoc block_argmax_sum(MaxLoc x, double y, MaxLoc *red,
+                                   double *reds, double *sum)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        MaxLoc z;
+        z.v = __shfl_down_sync(0xffffffffu, x.v, o);
+        z.i = __shfl_down_sync(0xffffffffu, x.i, o);
+        if (z.v > x.v || (z.v == x.v && z.i < x.i)) x = z;
+        y += __shfl_down_sync(0xffffffffu, y, o);
+    }
+    __syncthreads();
+    if (lane == 0) {
+        red[warp] = x;
+        reds[warp] = y;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        const bool in = lane < (int)(blockDim.x >> 5);
+        x = in ? red[lane] : MaxLoc{-DBL_MAX, 1 << 30};
+        y = in ? reds[lane] : 0.0;
+        #pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            MaxLoc z;
+            z.v = __shfl_down_sync(0xffffffffu, x.v, o);
+            z.i = __shfl_down_sync(0xffffffffu, x.i, o);
+            if (z.v > x.v || (z.v == x.v && z.i < x.i)) x = z;
+            y += __shfl_down_sync(0xffffffffu, y, o);
+        }
+        if (lane == 0) {
+            red[0] = x;
+            reds[0] = y;
+        }
+    }
+    __syncthreads();
+    const MaxLoc r = red[0];
+    *sum = reds[0];
+    __syncthreads();
+    return r;
+}
+
 __device__ double block_sum(double x, double *red)
 {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -659,6 +703,7 @@ k_pivchol(TileWork *__restrict__ tiles, Workspace ws, int phase)
 
     double thr;
     int cap = nn;
+    double stop_trace = -1.0;   // PH_H: stop once the remaining trace is below
     if (phase == PH_A) {
         const double tol_floor = 0.01 * tol * tol * trace / nn;
         const double noise = 1e-15 * dmax;
@@ -690,15 +735,33 @@ k_pivchol(TileWork *__restrict__ tiles, Workspace ws, int phase)
     } else {
         thr = 1e-18 * dmax;
         if (threadIdx.x == 0) tw.tr_h = trace;
+        // The energy the factor leaves out joins the rank rule's tail
+        // (tail_h), so the factor may stop at 1% of the tile's error
+        // budget: it, and the Jacobi SVD on it, are then no wider than the
+        // tolerance needs (the rank grows by at most the directions that 1%
+        // hides).
+        const double energy = tw.dnorm2 > 0.0 ? fmax(tw.dnorm2, trace) : trace;
+        stop_trace = 0.01 * tol * tol * energy;
     }
     if (!(dmax > 0.0)) thr = DBL_MAX;   // zero or invalid Gram: rank 0
 
     int j = 0;
     for (; j < cap; ++j) {
         MaxLoc cand{-DBL_MAX, 1 << 30};
+        double rest = 0.0;          // remaining trace, for PH_H's stop
         for (int i = threadIdx.x; i < nn; i += blockDim.x)
-            if (!used[i] && dg[i] > cand.v) cand = MaxLoc{dg[i], i};
-        const MaxLoc best = block_argmax(cand, red);
+            if (!used[i]) {
+                if (dg[i] > cand.v) cand = MaxLoc{dg[i], i};
+                rest += fmax(0.0, dg[i]);
+            }
+        MaxLoc best;
+        if (stop_trace >= 0.0) {
+            double total;
+            best = block_argmax_sum(cand, rest, red, redd, &total);
+            if (total <= stop_trace) break;
+        } else {
+            best = block_argmax(cand, red);
+        }
         if (!(best.v > thr)) break;
         const int p = best.i;
         const double sp = sqrt(best.v);
@@ -1169,6 +1232,143 @@ k_jacobi(TileWork *__restrict__ tiles, Workspace ws)
     }
 }
 
+// Block one-sided Jacobi for the classes whose factor does not fit in
+// shared memory (k1 <= 512).  The k2 columns form blocks of B = 512 / G;
+// the blocks meet in a round-robin tournament, and each meeting brings the
+// block pair (2B columns, 131 KB at most) into shared memory, rotates the
+// B^2 column pairs across the two blocks there (B steps of B disjoint
+// pairs, one group of G lanes per pair, E rows per lane) and writes it
+// back; the pairs inside each block are rotated in the tournament's first
+// round.  A sweep (one tournament) thus rotates every pair once, as the
+// cyclic order does, but every rotation reads shared memory instead of L2
+// and global traffic is a few copies of the factor per sweep.  Sweeps
+// repeat until one rotates nothing.
+template <int CLASS, int G, int E>
+__global__ void __launch_bounds__(512, 1)
+k_jacobi_block(TileWork *__restrict__ tiles, Workspace ws)
+{
+    constexpr int THREADS = 512;
+    constexpr int B = THREADS / G;          // columns per block, pairs per step
+    constexpr int P2 = 2 * B;               // columns in shared memory
+    extern __shared__ double sm[];
+    __shared__ int rotated[2];
+    TileWork &tw = tiles[blockIdx.x];
+    const int s = tw.slot;
+    const int rows = tw.k1, cols = tw.k2;
+    if (cols <= 0 || jacobi_class(rows, cols) != CLASS) return;   // uniform
+    const double eps = fmax(1e-15, fmin(1e-8, 0.01 * tw.tol));
+    const double eps2 = eps * eps;
+    const int ldg = ws.ldK();
+    double *Lg = ws.L(s);
+    const int lds = rows | 1;
+    const int nb = (cols + B - 1) / B;
+    const int nbp = nb + (nb & 1);          // blocks, with a bye if odd
+    const int gw = threadIdx.x / G, gl = threadIdx.x % G;
+    if (threadIdx.x == 0) rotated[0] = rotated[1] = 0;
+    __syncthreads();
+    auto column = [&](int q, int bi, int bj) {   // global column of slot q
+        return q < B ? bi * B + q : bj * B + q - B;
+    };
+    int sweep = 0;
+    for (; sweep < 40; ++sweep) {
+        bool any = false;
+        for (int rnd = 0; rnd < nbp - 1; ++rnd) {
+            for (int pr = 0; pr < nbp / 2; ++pr) {
+                // block pair pr of round rnd (circle method, as for columns)
+                int x = pr - 1 + rnd, y = nbp - 2 - pr + rnd;
+                if (x >= nbp - 1) x -= nbp - 1;
+                if (y >= nbp - 1) y -= nbp - 1;
+                const int bi = pr == 0 ? 0 : 1 + x, bj = 1 + y;
+                // Each block's own pairs are rotated once per sweep, in the
+                // first round (where every block meets exactly one other,
+                // or the bye); every meeting rotates the B^2 pairs across
+                // its two blocks.
+                const bool bye = bi >= nb || bj >= nb;
+                if (bye && rnd > 0) continue;                   // uniform
+                const int b0 = bye ? (bi < nb ? bi : bj) : bi;  // slots 0 .. B-1
+                const int b1 = bye ? nb : bj;                   // slots B .. 2B-1
+                const int nslots = bye ? B : P2;
+                for (int e = threadIdx.x; e < nslots * rows; e += THREADS) {
+                    const int q = e / rows, i = e - q * rows;
+                    const int c = column(q, b0, b1);
+                    sm[(size_t)q * lds + i] = c < cols ? Lg[(size_t)c * ldg + i] : 0.0;
+                }
+                __syncthreads();
+                if (rnd == 0) {
+                    // round-robin over the B columns of each block, B / 2
+                    // pairs per block and step (groups B / 2 .. B - 1 take
+                    // block b1, idle at the bye)
+                    const int q = gw % (B / 2), off = gw < B / 2 ? 0 : B;
+                    for (int step = 0; step < B - 1; ++step) {
+                        int u = q - 1 + step, v = B - 2 - q + step;
+                        if (u >= B - 1) u -= B - 1;
+                        if (v >= B - 1) v -= B - 1;
+                        const int a = off + (q == 0 ? 0 : 1 + u), b = off + 1 + v;
+                        const bool valid = (off == 0 || !bye) &&
+                                           column(a, b0, b1) < cols &&
+                                           column(b, b0, b1) < cols;
+                        any |= jacobi_rotate<G, E>(sm + (size_t)a * lds,
+                                                   sm + (size_t)b * lds, rows, gl,
+                                                   valid, eps2);
+                        __syncthreads();
+                    }
+                }
+                if (!bye) {
+                    // the cross pairs: slot gw with slot B + (gw + step) mod B
+                    for (int step = 0; step < B; ++step) {
+                        const int a = gw, b = B + (gw + step) % B;
+                        const bool valid = column(a, b0, b1) < cols &&
+                                           column(b, b0, b1) < cols;
+                        any |= jacobi_rotate<G, E>(sm + (size_t)a * lds,
+                                                   sm + (size_t)b * lds, rows, gl,
+                                                   valid, eps2);
+                        __syncthreads();
+                    }
+                }
+                for (int e = threadIdx.x; e < nslots * rows; e += THREADS) {
+                    const int q = e / rows, i = e - q * rows;
+                    const int c = column(q, b0, b1);
+                    if (c < cols) Lg[(size_t)c * ldg + i] = sm[(size_t)q * lds + i];
+                }
+                __syncthreads();
+            }
+        }
+        if (any) rotated[sweep & 1] = 1;
+        if (threadIdx.x == 0) rotated[(sweep + 1) & 1] = 0;
+        __syncthreads();
+        if (!rotated[sweep & 1]) break;
+    }
+    // Normalise into W = T(slot); squared norms into Sig.
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double *W = ws.T(s);
+    double *sig = ws.Sig(s);
+    for (int c = warp; c < cols; c += THREADS / 32) {
+        const double *ca = Lg + (size_t)c * ldg;
+        double nrm = 0.0;
+        for (int i = lane; i < rows; i += 32) nrm = fma(ca[i], ca[i], nrm);
+        #pragma unroll
+        for (int o = 16; o > 0; o >>= 1) nrm += __shfl_xor_sync(0xffffffffu, nrm, o);
+        const double inv = nrm > 0.0 ? 1.0 / sqrt(nrm) : 0.0;
+        for (int i = lane; i < rows; i += 32) W[(size_t)c * ldg + i] = ca[i] * inv;
+        if (lane == 0) sig[c] = nrm;
+    }
+    if (threadIdx.x == 0) {
+        tw.sweeps = sweep;
+        if (sweep >= 40) tw.status |= TILE_JACOBI_SLOW;
+    }
+}
+
+template <int CLASS, int G, int E>
+static void jacobi_block_launch(TileWork *d_tiles, int ntiles, Workspace ws,
+                                int max_rows, cudaStream_t stream)
+{
+    auto *fn = k_jacobi_block<CLASS, G, E>;
+    const size_t smem = (size_t)2 * (512 / G) * (max_rows | 1) * sizeof(double);
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
+    fn<<<ntiles, 512, smem, stream>>>(d_tiles, ws);
+}
+
 template <int CLASS, int G, int E, int THREADS, bool SMEM>
 static void jacobi_class_launch(TileWork *d_tiles, int ntiles, Workspace ws,
                                 size_t smem, cudaStream_t stream)
@@ -1192,8 +1392,8 @@ void launch_jacobi(TileWork *d_tiles, int ntiles, Workspace ws,
         const size_t full = (size_t)(r | 1) * std::min(r, kmax) * sizeof(double);
         return std::min(full, kJacobiSmemMax);
     };
-    // The classes that hold many CTAs per SM run on `stream`; the large
-    // classes (one CTA per SM, long-running) on `side`, overlapping them.
+    // The block classes (one CTA per SM, long-running) run on `side`, the
+    // others on `stream`, overlapping them.
     cudaStream_t big = side ? side : stream;
     cudaEvent_t fork = nullptr, join = nullptr;
     if (side && kmax > 64) {
@@ -1202,21 +1402,24 @@ void launch_jacobi(TileWork *d_tiles, int ntiles, Workspace ws,
         cudaEventRecord(fork, stream);
         cudaStreamWaitEvent(side, fork, 0);
     }
-    if (kmax > 128) {
-        jacobi_class_launch<4, 16, 16, 512, false>(d_tiles, ntiles, ws, 0,
-                                                   big);
-        jacobi_class_launch<3, 16, 16, 512, true>(d_tiles, ntiles, ws,
-                                                  smem_for(256), big);
-    }
-    if (kmax > 64)
-        jacobi_class_launch<2, 8, 16, 512, true>(d_tiles, ntiles, ws,
-                                                 smem_for(128), big);
+    // the block classes (factor in global memory) on `side`; the classes
+    // whose factor sits in shared memory on `stream`, filling the SMs the
+    // last wave of the block classes leaves idle
+    if (kmax > 128)
+        jacobi_block_launch<4, 16, 16>(d_tiles, ntiles, ws,
+                                       std::min(kmax, 256), big);
     if (kmax > 256)
-        jacobi_class_launch<5, 32, 16, 512, false>(d_tiles, ntiles, ws, 0,
-                                                   big);
+        jacobi_block_launch<5, 32, 16>(d_tiles, ntiles, ws,
+                                       std::min(kmax, 512), big);
     if (kmax > 512)
         jacobi_class_launch<6, 32, 0, 1024, false>(d_tiles, ntiles, ws, 0,
                                                    big);
+    if (kmax > 128)
+        jacobi_class_launch<3, 16, 16, 512, true>(d_tiles, ntiles, ws,
+                                                  smem_for(256), stream);
+    if (kmax > 64)
+        jacobi_class_launch<2, 8, 16, 512, true>(d_tiles, ntiles, ws,
+                                                 smem_for(128), stream);
     jacobi_class_launch<0, 4, 8, 64, true>(d_tiles, ntiles, ws,
                                            smem_for(32), stream);
     if (kmax > 32)

@@ -1039,15 +1039,10 @@ void launch_chol_inv(int phase, TileWork *d_tiles, int ntiles, Workspace ws,
 // columns) goes to T(slot), squared norms to Sig(slot).
 constexpr size_t kJacobiSmemMax = 220 * 1024;
 
-struct JacobiClass {
-    int groups;     // G: lanes per pair
-    int per_lane;   // E: rows per lane
-    int threads;
-    bool smem;
-};
-
-// Size classes, by rows (k1); shared-memory classes first.  The last class
-// streams rows through registers for k1 > 512.
+// Size classes, by rows (k1), with G E just above the row count so that few
+// lanes rotate padding; factors in shared memory when they fit, else the
+// block kernel (k_jacobi_block).  The last class streams rows through
+// registers for k1 > 512.
 __host__ __device__ inline int jacobi_class(int rows, int cols)
 {
     const size_t bytes = (size_t)(rows | 1) * cols * sizeof(double);
@@ -1055,9 +1050,12 @@ __host__ __device__ inline int jacobi_class(int rows, int cols)
     if (rows <= 32) return 0;                     // G 4,  E 8,  64 threads
     if (rows <= 64) return 1;                     // G 4,  E 16, 128 threads
     if (rows <= 128) return 2;                    // G 8,  E 16, 512 threads
-    if (rows <= 256) return fits ? 3 : 4;         // G 16, E 16, 512 threads
-    if (rows <= 512) return 5;                    // G 32, E 16, 512, global
-    return 6;                                     // streamed, global
+    if (rows <= 192) return fits ? 3 : 4;         // G 16, E 12, 512 threads
+    if (rows <= 256) return fits ? 5 : 6;         // G 16, E 16, 512 threads
+    if (rows <= 288) return 7;                    // G 16, E 18, blocks
+    if (rows <= 320) return 8;                    // G 16, E 20, blocks
+    if (rows <= 512) return 9;                    // G 32, E 16, blocks
+    return 10;                                    // streamed, global
 }
 
 // Rotation of the column pair (ca, cb) by the G lanes of one group (gl =
@@ -1406,17 +1404,29 @@ void launch_jacobi(TileWork *d_tiles, int ntiles, Workspace ws,
     // whose factor sits in shared memory on `stream`, filling the SMs the
     // last wave of the block classes leaves idle
     if (kmax > 128)
-        jacobi_block_launch<4, 16, 16>(d_tiles, ntiles, ws,
+        jacobi_block_launch<4, 16, 12>(d_tiles, ntiles, ws,
+                                       std::min(kmax, 192), big);
+    if (kmax > 192)
+        jacobi_block_launch<6, 16, 16>(d_tiles, ntiles, ws,
                                        std::min(kmax, 256), big);
     if (kmax > 256)
-        jacobi_block_launch<5, 32, 16>(d_tiles, ntiles, ws,
+        jacobi_block_launch<7, 16, 18>(d_tiles, ntiles, ws,
+                                       std::min(kmax, 288), big);
+    if (kmax > 288)
+        jacobi_block_launch<8, 16, 20>(d_tiles, ntiles, ws,
+                                       std::min(kmax, 320), big);
+    if (kmax > 320)
+        jacobi_block_launch<9, 32, 16>(d_tiles, ntiles, ws,
                                        std::min(kmax, 512), big);
     if (kmax > 512)
-        jacobi_class_launch<6, 32, 0, 1024, false>(d_tiles, ntiles, ws, 0,
-                                                   big);
-    if (kmax > 128)
-        jacobi_class_launch<3, 16, 16, 512, true>(d_tiles, ntiles, ws,
+        jacobi_class_launch<10, 32, 0, 1024, false>(d_tiles, ntiles, ws, 0,
+                                                    big);
+    if (kmax > 192)
+        jacobi_class_launch<5, 16, 16, 512, true>(d_tiles, ntiles, ws,
                                                   smem_for(256), stream);
+    if (kmax > 128)
+        jacobi_class_launch<3, 16, 12, 512, true>(d_tiles, ntiles, ws,
+                                                  smem_for(192), stream);
     if (kmax > 64)
         jacobi_class_launch<2, 8, 16, 512, true>(d_tiles, ntiles, ws,
                                                  smem_for(128), stream);

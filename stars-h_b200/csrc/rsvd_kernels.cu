@@ -742,6 +742,21 @@ k_pivchol(TileWork *__restrict__ tiles, Workspace ws, int phase)
         // hides).
         const double energy = tw.dnorm2 > 0.0 ? fmax(tw.dnorm2, trace) : trace;
         stop_trace = 0.01 * tol * tol * energy;
+        // A block whose energy outside the sketched basis, ||D||^2 -
+        // ||B||^2 (less the rounding allowance of k_rank_cut), alone
+        // exceeds the budget is stored dense whatever its small SVD says:
+        // the rank cut reaches rank -1 from k2 = 0 by the same test, so the
+        // factor and the Jacobi SVD are skipped.
+        const double dn = tw.dnorm2;
+        if (dn > 0.0 &&
+            fmax(0.0, dn - trace - 2e-15 * dn) > tol * tol * fmax(dn, trace)) {
+            if (threadIdx.x == 0) {
+                tw.k2 = 0;
+                tw.tail_h = trace;
+                tw.status |= TILE_TAIL_LEFT;
+            }
+            return;
+        }
     }
     if (!(dmax > 0.0)) thr = DBL_MAX;   // zero or invalid Gram: rank 0
 

@@ -1171,8 +1171,9 @@ k_jacobi(TileWork *__restrict__ tiles, Workspace ws)
     if (cols <= 0 || jacobi_class(rows, cols) != CLASS) return;   // uniform
     // Relative orthogonality the rotations stop at: the rank cut needs the
     // left singular vectors orthonormal to well below tol (their overlap
-    // enters the tail energies squared and the projector linearly).
-    const double eps = fmax(1e-15, fmin(1e-8, 0.01 * tw.tol));
+    // enters the tail energies squared and the projector linearly): 1 % of
+    // tol, at most 1e-7.
+    const double eps = fmax(1e-15, fmin(1e-7, 0.01 * tw.tol));
     const double eps2 = eps * eps;
     const int ldg = ws.ldK();
     const int lds = rows | 1;   // odd stride: fewer bank conflicts
@@ -1269,7 +1270,7 @@ k_jacobi_block(TileWork *__restrict__ tiles, Workspace ws)
     const int s = tw.slot;
     const int rows = tw.k1, cols = tw.k2;
     if (cols <= 0 || jacobi_class(rows, cols) != CLASS) return;   // uniform
-    const double eps = fmax(1e-15, fmin(1e-8, 0.01 * tw.tol));
+    const double eps = fmax(1e-15, fmin(1e-7, 0.01 * tw.tol));
     const double eps2 = eps * eps;
     const int ldg = ws.ldK();
     double *Lg = ws.L(s);

@@ -1,5 +1,5 @@
 """Approximation parity: the B200 engine against the reference's
-starsh_blrm__drsdd_omp on the same STARSH_blrf, judged by the reference's
+starsh_blrm__drsdd_omp on the same STARSH_blrf, checked by the reference's
 own starsh_blrm__dfe and by the set of false far-field blocks and ranks.
 
 The reference's RSVD draws its sketch from LAPACK dlarnv and this library
@@ -139,7 +139,7 @@ def test_unknown_kernel_is_an_error(ref, lib):
 # ------------------------------------------------------------------ mixed
 # The mixed engine samples the sketch adaptively (blocks of 64 columns until
 # the FP64 residual estimate is below (tol/10)^2 ||D||_F^2, at most
-# maxrank + oversample columns); parity is judged exactly as above.
+# maxrank + oversample columns); parity is checked exactly as above.
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("case", [

@@ -36,7 +36,9 @@ def _rank(rank, world, port, out):
 def test_replica_rates_two_gloo_ranks():
     world = 2
     port = _free_port()
-    with mp.Manager() as mgr:
+    # the manager process is spawned too: forking this multi-threaded
+    # process could deadlock the child
+    with mp.get_context("spawn").Manager() as mgr:
         out = mgr.dict()
         mp.spawn(_rank, args=(world, port, out), nprocs=world, join=True)
         res = dict(out)

@@ -794,8 +794,18 @@ k_pivchol(TileWork *__restrict__ tiles, Workspace ws, int phase)
             } else if (used[i]) {
                 v = 0.0;
             } else {
-                double acc = G[(size_t)p * ld + i];
-                for (int l = 0; l < j; ++l) acc -= L[(size_t)l * ld + i] * lp[l];
+                // G(p, i) - sum_l L(i, l) L(p, l), in four independent
+                // partial sums (the chain over l is the step's latency)
+                double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+                int l = 0;
+                for (; l + 3 < j; l += 4) {
+                    a0 = fma(L[(size_t)l * ld + i], lp[l], a0);
+                    a1 = fma(L[(size_t)(l + 1) * ld + i], lp[l + 1], a1);
+                    a2 = fma(L[(size_t)(l + 2) * ld + i], lp[l + 2], a2);
+                    a3 = fma(L[(size_t)(l + 3) * ld + i], lp[l + 3], a3);
+                }
+                for (; l < j; ++l) a0 = fma(L[(size_t)l * ld + i], lp[l], a0);
+                const double acc = G[(size_t)p * ld + i] - ((a0 + a1) + (a2 + a3));
                 v = acc / sp;
                 dg[i] -= v * v;
             }

@@ -712,7 +712,7 @@ def replica_rates(times, entries, world, device):
 # ------------------------------------------------------------- device peak
 
 # DRAM bytes (read + write) of k_sketch_i8 over its algorithmic bytes, from
-# the ncu capture summarised in profiles/k_sketch_i8_c2_n16384.md
+# an ncu capture of a 256-tile, N = 16384 square-exponential case
 SKETCH_TRAFFIC_RATIO = 1.013
 
 
@@ -985,7 +985,7 @@ def main():
                 "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": peak_src,
                 "algorithmic_bytes_per_launch": bytes_per_launch,
-                # ncu (profiles/k_sketch_i8_c2_n16384.md): DRAM read + write
+                # ncu on a 256-tile case: DRAM read + write
                 # = 1.013x the algorithmic bytes on a 256-tile capture, so the
                 # per-launch traffic is the algorithmic figure scaled by it
                 "traffic": bytes_per_launch * SKETCH_TRAFFIC_RATIO,

@@ -185,9 +185,10 @@ int starsh_b200_kernel_family(STARSH_kernel *kernel, int *ndim_hint);
 
 /* Randomized-SVD compression of one dense tile already on the device,
  * without allocating any device memory.  No counterpart in the reference:
- * it is for callers that cannot call cudaMalloc (inside a stream capture,
- * under an allocator that owns all device memory, or on threads that must
- * not wait for the allocator's implicit synchronisation).  Same algorithm
+ * it is for callers that cannot call cudaMalloc (a host framework whose
+ * caching allocator owns all device memory, a plugin handed device buffers
+ * but no right to allocate, or threads that must not wait for the
+ * allocator's implicit synchronisation).  Same algorithm
  * and Gaussian sketch as starsh_blrm__drsdd_b200 applied to that tile, with
  * the reference's rank rule (the tail of the projected tile's spectrum: the
  * batched engine also counts the energy its sketch missed, from the exact
@@ -197,7 +198,8 @@ int starsh_b200_kernel_family(STARSH_kernel *kernel, int *ndim_hint);
  *   dU      receives nrows x rank, leading dimension nrows;
  *   dV      receives ncols x rank, leading dimension ncols (U V^T ~ D);
  *           both need room for maxrank columns;
- *   d_rank  device int: the rank, or -1 when it exceeds maxrank;
+ *   d_rank  device int: the rank, or -1 when it exceeds maxrank (dU and
+ *           dV are then left unwritten: store the tile dense);
  *   stream  cudaStream_t (NULL: default stream); the call is asynchronous.
  * Limits: nrows, ncols <= 256 and min(maxrank + oversample, nrows, ncols)
  * <= 96; beyond them STARSH_WRONG_PARAMETER.  The first call on a device

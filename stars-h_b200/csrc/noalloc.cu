@@ -1,14 +1,17 @@
 // starsh_b200_dense_rsvd_noalloc: randomized-SVD compression of one dense
 // device tile with no device memory allocation.
 //
-// Some callers cannot call cudaMalloc at all: code running inside a CUDA
-// graph capture or a stream-ordered region that forbids allocation, custom
-// allocators that own all device memory, or host threads that must not
-// block on the allocator's implicit device synchronisation.  For them this
-// entry point runs the same per-tile pipeline as the batched engine
-// (engine.cu / rsvd_kernels.cu) on one tile whose scratch lives in a
-// file-scope __device__ array of fixed size; the caller passes the tile and
-// the output buffers.
+// Some callers cannot call cudaMalloc at all: a host framework whose
+// caching allocator owns all device memory (a second allocator would
+// fragment it or exceed its budget), plugins that are handed device
+// buffers but no right to allocate, and host threads that must not block
+// on the allocator's implicit device synchronisation.  For them this entry
+// point runs the same per-tile pipeline as the batched engine (engine.cu /
+// rsvd_kernels.cu) on one tile whose scratch lives in a file-scope
+// __device__ array of fixed size; the caller passes the tile and the output
+// buffers.  Every step is a kernel launch or a device-to-device copy on the
+// caller's stream: the tile record is written by a one-thread kernel from
+// by-value arguments, so no host memory is read after the call returns.
 //
 // Limits: nrows, ncols <= 256 and min(maxrank + oversample, nrows, ncols)
 // <= 96; larger sizes are rejected with STARSH_WRONG_PARAMETER.  The scratch
@@ -56,6 +59,22 @@ static __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
 // Same seed as the batched engine, so a single-tile problem sees the same
 // Gaussian sketch through both entry points.
 static const unsigned long long kNoAllocOmegaSeed = 0x5354415253480001ull;
+
+// The one tile's record: every field zero (the previous call's state is
+// gone), then the shape, sketch width and the caller's maxrank and tol.
+__global__ void k_noalloc_tile(TileWork *t, int m, int n, int k, int maxrank,
+                               double tol)
+{
+    TileWork w;
+    memset(&w, 0, sizeof(w));
+    w.m = m;
+    w.n = n;
+    w.k = k;
+    w.slot = 0;
+    w.maxrank = maxrank;
+    w.tol = tol;
+    *t = w;
+}
 
 constexpr int kMaxDevices = 64;
 static double *g_scratch_ptr[kMaxDevices];
@@ -125,16 +144,7 @@ extern "C" int starsh_b200_dense_rsvd_noalloc(const double *dD, int nrows,
     TileWork *dt = (TileWork *)(omega + kOmegaDoubles);
     GemmDesc *dd = (GemmDesc *)((double *)dt + kTileDoubles);
 
-    TileWork tw;
-    memset(&tw, 0, sizeof(tw));
-    tw.m = nrows;
-    tw.n = ncols;
-    tw.k = k;
-    tw.slot = 0;
-    tw.maxrank = maxrank;
-    tw.tol = tol;
-    B200_CUDA(cudaMemcpyAsync(dt, &tw, sizeof(tw), cudaMemcpyHostToDevice, s),
-              "no-alloc tile record");
+    k_noalloc_tile<<<1, 1, 0, s>>>(dt, nrows, ncols, k, maxrank, tol);
     B200_CUDA(cudaMemcpy2DAsync(ws.D(0), (size_t)ws.ldD() * sizeof(double), dD,
                                 (size_t)ldd * sizeof(double),
                                 (size_t)nrows * sizeof(double), ncols,

@@ -78,3 +78,32 @@ def test_noalloc_rejects_oversized_tiles(lib):
     assert lib.starsh_b200_dense_rsvd_noalloc(
         D.data_ptr(), 256, 256, 256, 90, 10, 1e-6, out.data_ptr(),
         out.data_ptr(), rank.data_ptr(), None) == sb.WRONG_PARAMETER
+
+
+@pytest.mark.gpu
+def test_noalloc_rank_above_maxrank_leaves_factors_unwritten(ref, lib):
+    # a rough kernel (exponential, short correlation length) on one 128 x 128
+    # tile needs far more than maxrank = 4 columns at tol 1e-6: the call
+    # reports rank -1 and writes neither factor, so the caller keeps the
+    # tile dense
+    import torch
+    N, MAXRANK = 128, 4
+    pr = RefProblem(ref, "spatial", N, N, kernel_name="exp", beta=0.02)
+    gen = sb.KERNEL(sb.kernel_symbol(lib, "starsh_ssdata_block_exp_kernel_2d"))
+    idx = np.arange(N, dtype=np.int64)
+    host = np.zeros((N, N))
+    gen(N, N, idx.ctypes.data_as(POINTER(sb.STARSH_int)),
+        idx.ctypes.data_as(POINTER(sb.STARSH_int)), pr.data, pr.data,
+        host.ctypes.data, N)
+    D = torch.tensor(host.T, dtype=torch.float64, device="cuda")
+    D = D.t().contiguous().t()
+    U = torch.full((MAXRANK, N), float("nan"), dtype=torch.float64, device="cuda")
+    V = torch.full((MAXRANK, N), float("nan"), dtype=torch.float64, device="cuda")
+    rank = torch.full((1,), 7, dtype=torch.int32, device="cuda")
+    info = lib.starsh_b200_dense_rsvd_noalloc(
+        D.data_ptr(), N, N, N, MAXRANK, 10, TOL, U.data_ptr(), V.data_ptr(),
+        rank.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    assert info == 0, lib.starsh_b200_last_error()
+    torch.cuda.synchronize()
+    assert int(rank.item()) == -1
+    assert torch.isnan(U).all() and torch.isnan(V).all()

@@ -136,7 +136,7 @@ def new_format(lib, prob):
 
 C4 = dict(problems=512, nmin=1024, nmax=16384, tols=(1e-3, 1e-5, 1e-7),
           kernels=("exp", "sqexp", "matern", "coulomb", "rbf"), oversample=10)
-C5 = dict(rate=200.0, seconds=10.0, median=8192, sigma_log=0.5, nmin=2048,
+C5 = dict(rate=200.0, seconds=60.0, median=8192, sigma_log=0.5, nmin=2048,
           nmax=65536, tols=(1e-4, 1e-6), nrhs=32, budget=120e9, oversample=10)
 
 
@@ -169,11 +169,30 @@ def sphere_points(rng, n):
     return centres[which] + radii[which, None] * v
 
 
-def mixed_problem(lib, seed, n, kernel, ndim, coulomb_handle):
+TUNE_NB = (256, 512, 1024)
+
+
+def tuned_tile_size(lib, P, tol):
+    """The library autotuner's block size for problem P among TUNE_NB (each
+    with maxrank min(nb / 2, 256)), measured with the mixed engine."""
+    import starsh_b200 as sb
+    k = len(TUNE_NB)
+    cands = (ctypes.c_int * k)(*TUNE_NB)
+    ranks = (ctypes.c_int * k)(*[min(nb // 2, 256) for nb in TUNE_NB])
+    best = ctypes.c_int(0)
+    assert lib.starsh_b200_autotune_tile(P, k, cands, ranks, tol,
+                                         sb.ENGINE_MIXED, byref(best),
+                                         None) == 0, lib.starsh_b200_last_error()
+    return best.value
+
+
+def mixed_problem(lib, seed, n, kernel, ndim, coulomb_handle, tol=None,
+                  tune=False):
     """One problem of the many-problem workloads, built with the library's
     own host API: spatial kernels on a jittered grid (N rounded to a
     square / cube), 1/r (unit diagonal) on jittered particles, Gaussian RBF
-    (radius 0.1) on points on spheres, all Z-sorted."""
+    (radius 0.1) on points on spheres, all Z-sorted.  The block size comes
+    from the library's autotuner when `tune`, else from tile_size()."""
     import numpy as np
     import starsh_b200 as sb
     libc = ctypes.CDLL("libc.so.6")
@@ -208,11 +227,11 @@ def mixed_problem(lib, seed, n, kernel, ndim, coulomb_handle):
                                       0, 1, 0, 0.0, 0.1, 0.0) == 0
         kern = c_void_p(sb.kernel_symbol(lib, "starsh_generate_3d_virus"))
         _keep.append(part)
-    nb = tile_size(n)
     shape = (sb.STARSH_int * 2)(n, n)
     P = POINTER(sb.Problem)()
     assert lib.starsh_problem_new(byref(P), 2, shape, b"N", b"d", data, data,
                                   kern, b"mixed") == 0
+    nb = tuned_tile_size(lib, P, tol) if tune else tile_size(n)
     C = POINTER(sb.Cluster)()
     assert lib.starsh_cluster_new_plain(byref(C), data, n, nb) == 0
     _keep.append(shape)
@@ -255,11 +274,11 @@ def c5_specs(seconds, rate, seed=12345):
     return out
 
 
-def build_mixed(lib, specs, coulomb_handle):
+def build_mixed(lib, specs, coulomb_handle, tune=False):
     out = []
     for sp in specs:
         pr = mixed_problem(lib, sp["seed"], sp["n"], sp["kernel"], sp["ndim"],
-                           coulomb_handle)
+                           coulomb_handle, tol=sp["tol"], tune=tune)
         pr["tol"] = sp["tol"]
         pr["t"] = sp["t"]
         out.append(pr)
@@ -351,7 +370,7 @@ def run_c4(args, lib, stream, clocks, torch):
         1.0) == 0
     lib.starsh_set_oversample(str(C4["oversample"]).encode())
     t_build = time.perf_counter()
-    probs = build_mixed(lib, c4_specs(), handle)
+    probs = build_mixed(lib, c4_specs(), handle, tune=args.tune)
     t_build = time.perf_counter() - t_build
     n = len(probs)
     ranks = (ctypes.c_int * n)(*[p["maxrank"] for p in probs])
@@ -427,11 +446,16 @@ def run_c4(args, lib, stream, clocks, torch):
         "config": {"workload": "uneven-batch-512-problems-N1024-16384",
                    "engine": "mixed (adaptive sketch), one batched call",
                    "problems": n, "kernels": kinds,
-                   "tols": list(C4["tols"]), "tile_sizes": [256, 512, 1024],
+                   "tols": list(C4["tols"]), "tile_sizes": list(TUNE_NB),
+                   "tile_choice": ("autotuned (starsh_b200_autotune_tile)"
+                                   if args.tune else "fixed rule by N"),
+                   "tiles_chosen": {str(nb): sum(1 for p in probs if p["nb"] == nb)
+                                    for nb in TUNE_NB},
                    "entries": int(entries), "tiles": int(st.tiles),
                    "false_far": int(st.false_far), "batches": int(st.batches),
                    "l2": "flushed (256 MB write) before every step",
-                   "host_build_s": t_build},
+                   "host_build_s": t_build,
+                   "build_includes_tuning": bool(args.tune)},
         "accepted": bool(ok), "worst_err_over_tol": worst,
         "fp64_batched": {"value": entries / t_fp64_batched / 1e6,
                          "ms": t_fp64_batched * 1e3},
@@ -473,9 +497,11 @@ def serve(lib, reqs, engine, max_group, A):
                 time.sleep(dt)
             outs[i] = np.empty((r["n"], nrhs), order="F")
             t = ctypes.c_longlong()
+            # keep = 1: the factors stay resident after the products (the
+            # caller releases them once it has the result)
             assert lib.starsh_b200_server_submit(
                 srv, fmts[i], r["maxrank"], r["tol"], nrhs, A.ctypes.data, lda,
-                outs[i].ctypes.data, r["n"], 0, byref(t)) == 0
+                outs[i].ctypes.data, r["n"], 1, byref(t)) == 0
             tickets[i] = t.value
 
     t_start = time.perf_counter()
@@ -486,9 +512,12 @@ def serve(lib, reqs, engine, max_group, A):
         while tickets[i] is None:
             time.sleep(0.0005)
         L = ctypes.c_double()
-        status.append(lib.starsh_b200_server_wait(srv, tickets[i], None,
+        M = POINTER(sb.Blrm)()
+        status.append(lib.starsh_b200_server_wait(srv, tickets[i], byref(M),
                                                   byref(L)))
         lat.append(L.value)
+        if M:
+            lib.starsh_b200_server_release(srv, M)
         outs[i] = None
     th.join()
     wall = time.perf_counter() - t_start
@@ -512,15 +541,18 @@ def run_c5(args, lib, clocks):
         c_void_p(ctypes.cast(handle, c_void_p).value), sb.FAMILY["coulomb"],
         1.0) == 0
     lib.starsh_set_oversample(str(C5["oversample"]).encode())
-    seconds = args.serve_seconds
-    reqs = build_mixed(lib, c5_specs(seconds, C5["rate"]), handle)
+    seconds, rate = args.serve_seconds, args.serve_rate
+    reqs = build_mixed(lib, c5_specs(seconds, rate), handle, tune=args.tune)
     A = np.asfortranarray(np.random.default_rng(1).standard_normal(
         (C5["nmax"], C5["nrhs"])))
     # warm-up on the first few requests
     serve(lib, reqs[:min(8, len(reqs))], sb.ENGINE_MIXED, 0, A)
     with clocks:
         lat, status, st, wall = serve(lib, reqs, sb.ENGINE_MIXED, 0, A)
-    lat_p, status_p, st_p, wall_p = serve(lib, reqs, sb.ENGINE_FP64, 1, A)
+    # the FP64 comparison over the first 10 s of arrivals (one request at
+    # a time it takes far longer than the stream)
+    reqs_p = [r for r in reqs if r["t"] < 10.0]
+    lat_p, status_p, st_p, wall_p = serve(lib, reqs_p, sb.ENGINE_FP64, 1, A)
     ok = all(x == 0 for x in status)
 
     def pct(v):
@@ -534,8 +566,9 @@ def run_c5(args, lib, clocks):
         "n_gpus": 1, "steps": 1, "warmup": 1, "ms_per_step": wall * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (seeded point generators)",
-        "config": {"workload": f"serving-poisson-{C5['rate']:g}rps-{seconds:g}s",
-                   "requests": len(reqs), "offered_rate_rps": C5["rate"],
+        "config": {"workload": f"serving-poisson-{rate:g}rps-{seconds:g}s",
+                   "requests": len(reqs), "offered_rate_rps": rate,
+                   "workers": int(os.environ.get("STARSH_B200_SERVER_WORKERS", "2")),
                    "N": "lognormal median 8192, sigma_log 0.5, clipped [2048, 65536]",
                    "tols": list(C5["tols"]), "nrhs": C5["nrhs"],
                    "hbm_budget_bytes": C5["budget"], "engine": "mixed, continuous batching"},
@@ -546,7 +579,8 @@ def run_c5(args, lib, clocks):
         "peak_resident_bytes": st.peak_resident_bytes,
         "plain_fp64_one_at_a_time": {
             "value": st_p.entries / wall_p / 1e6, "latency_ms": pct(lat_p),
-            "served_rps": len(reqs) / wall_p, "wall_s": wall_p},
+            "served_rps": len(reqs_p) / wall_p, "wall_s": wall_p,
+            "requests": len(reqs_p), "what": "the arrivals of the first 10 s"},
         "clocks": clocks.summary(),
     }
     print(json.dumps(line))
@@ -709,6 +743,140 @@ def replica_rates(times, entries, world, device):
     return [total / t / 1e6 for t in times], times
 
 
+# ---------------------------------------------------- sketch precision study
+
+def precision_study(lib, wl, prob, torch, ntiles=64, seed=7):
+    """Sketch precisions on a sample of the workload's far tiles: Y = D
+    Omega with BF16, BF16x3 and TF32x3 inputs and FP32 accumulation (each
+    emulated exactly: the split operands' products are exact in FP32, so an
+    FP32 GEMM of them accumulates as the tensor cores' FP32 path does), the
+    library's 40-bit integer slices of D (rounding as in the int8 sketch),
+    and FP64; then for each the same FP64 basis (Householder QR of Y),
+    projection B = Q^T D and rank rule (dsvfr tail plus the energy outside
+    the basis, as the library's rank cut).  Reports per precision the share
+    of tiles the rule accepts, their mean rank, and the largest energy
+    outside the basis over tol^2 ||D||^2 (the sketch error the FP64 steps
+    cannot repair), plus FP32-accumulate GEMM rates at the batch shape."""
+    import numpy as np
+    import starsh_b200 as sb
+    tol, k = wl["tol"], wl["maxrank"] + wl["oversample"]
+    C = prob["C"].contents
+    nt = C.nblocks
+    if wl["kind"] == "coulomb":
+        fn = sb.kernel_symbol(lib, "starsh_esdata_block_coulomb_potential_kernel_3d")
+    else:
+        fn = sb.kernel_symbol(lib, "starsh_eddata_block_sin_kernel_3d")
+    gen = sb.KERNEL(fn)
+    rng = np.random.default_rng(seed)
+    pairs = []
+    while len(pairs) < ntiles:
+        i, j = (int(x) for x in rng.integers(0, nt, 2))
+        if i != j:
+            pairs.append((i, j))
+    piv = np.ctypeslib.as_array(C.pivot, shape=(C.ndata,))
+    dev = "cuda"
+    f64 = torch.float64
+    g = torch.Generator(device=dev).manual_seed(seed)
+    n_b = int(C.size[0])
+    omega = torch.randn(n_b, k, dtype=f64, device=dev, generator=g)
+    prev_tf32 = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+
+    def bf16(x):
+        return x.to(torch.bfloat16).to(torch.float32)
+
+    def tf32(x):
+        # round-to-nearest to 10 explicit mantissa bits
+        xi = x.to(torch.float32).view(torch.int32)
+        xi = (xi + 0x1000) & ~0x1FFF
+        return xi.view(torch.float32)
+
+    def split3(x, rnd):
+        a = rnd(x)
+        r = x - a.to(f64)
+        b = rnd(r)
+        r = r - b.to(f64)
+        return a, b, rnd(r)
+
+    def sketch(D, how):
+        if how == "fp64":
+            return D @ omega
+        if how == "int40":
+            e = torch.ceil(torch.log2(D.abs().amax(dim=1, keepdim=True).clamp_min(1e-300)))
+            s = torch.pow(2.0, 39 - e)
+            q = torch.round(D * s)
+            return (q @ torch.round(32 * omega).clamp(-127, 127)) / s / 32
+        om = omega.to(torch.float32)
+        if how == "bf16":
+            return (bf16(D) @ bf16(om)).to(f64)
+        parts = split3(D, bf16 if how == "bf16x3" else tf32)
+        w = bf16(om) if how == "bf16x3" else tf32(om)
+        acc = torch.zeros(D.shape[0], k, dtype=torch.float32, device=dev)
+        for pt in parts:
+            acc += pt @ w
+        return acc.to(f64)
+
+    hows = ["fp64", "int40", "tf32x3", "bf16x3", "bf16"]
+    res = {h: {"accepted": 0, "ranks": [], "outside_over_budget": 0.0} for h in hows}
+    for (i, j) in pairs:
+        m, n = int(C.size[i]), int(C.size[j])
+        ri = piv[C.start[i]:C.start[i] + m].astype(np.int64).copy()
+        ci = piv[C.start[j]:C.start[j] + n].astype(np.int64).copy()
+        host = np.zeros((m, n))
+        gen(m, n, ri.ctypes.data_as(POINTER(sb.STARSH_int)),
+            ci.ctypes.data_as(POINTER(sb.STARSH_int)), prob["data"], prob["data"],
+            host.ctypes.data, m)
+        D = torch.tensor(host.T.copy(), dtype=f64, device=dev).T
+        nd2 = float((D * D).sum())
+        for h in hows:
+            Y = sketch(D, h)[:, :min(k, n)]
+            Q, _ = torch.linalg.qr(Y)
+            B = Q.T @ D
+            sv = torch.linalg.svdvals(B)
+            outside = max(0.0, nd2 - float((B * B).sum()))
+            budget = tol * tol * nd2
+            tail = torch.flip(torch.cumsum(torch.flip(sv * sv, [0]), 0), [0])
+            ok = (tail + outside <= budget).nonzero()
+            r = int(ok[0]) if len(ok) else -1
+            rr = res[h]
+            if r >= 0 and r <= wl["maxrank"]:
+                rr["accepted"] += 1
+                rr["ranks"].append(r)
+            rr["outside_over_budget"] = max(rr["outside_over_budget"],
+                                            outside / max(budget, 1e-300))
+    out = {}
+    for h in hows:
+        rr = res[h]
+        out[h] = {"accepted": rr["accepted"], "tiles": len(pairs),
+                  "mean_rank": float(np.mean(rr["ranks"])) if rr["ranks"] else None,
+                  "max_outside_over_tol2": rr["outside_over_budget"]}
+    # FP32-accumulate GEMM rates at one batch's shape (tiles x m x k per n)
+    bt = 512
+    a32 = torch.randn(bt, n_b, n_b, device=dev, dtype=torch.float32)
+    b32 = torch.randn(bt, n_b, k, device=dev, dtype=torch.float32)
+    rates = {}
+    for name, tf, A_, B_ in (("fp32_simt", False, a32, b32),
+                             ("tf32", True, a32, b32),
+                             ("bf16", False, a32.bfloat16(), b32.bfloat16())):
+        torch.backends.cuda.matmul.allow_tf32 = tf
+        torch.bmm(A_, B_)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(5):
+            torch.bmm(A_, B_)
+        e1.record()
+        e1.synchronize()
+        t = e0.elapsed_time(e1) / 5 / 1e3
+        rates[name] = 2.0 * bt * n_b * n_b * k / t / 1e12
+    torch.backends.cuda.matmul.allow_tf32 = prev_tf32
+    del a32, b32
+    return {"what": "sketch precision on sampled far tiles (FP64 basis, projection and rank rule for every variant)",
+            "tol": tol, "sketch_width": k, "results": out,
+            "cublas_tflops_at_batch_shape": rates,
+            "x3_cost_note": "BF16x3 / TF32x3 need 3 GEMMs per sketch"}
+
+
 # ------------------------------------------------------------- device peak
 
 # DRAM bytes (read + write) of k_sketch_i8 over its algorithmic bytes, from
@@ -789,10 +957,18 @@ def main():
     ap.add_argument("--engine", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--workload", default="c2-sqexp",
                     choices=sorted(WORKLOADS) + ["c4-batch", "c5-serve"])
+    ap.add_argument("--serve-rate", type=float, default=C5["rate"],
+                    help="c5-serve: offered requests per second")
     ap.add_argument("--serve-seconds", type=float, default=C5["seconds"],
                     help="c5-serve: length of the arrival stream")
     ap.add_argument("--n", type=int, default=0,
                     help="points (a smaller N profiles the same kernels)")
+    ap.add_argument("--tune", action=argparse.BooleanOptionalAction,
+                    default=True,
+                    help="c4-batch / c5-serve: block sizes from the library's "
+                         "autotuner (default) or the fixed rule by N")
+    ap.add_argument("--precision-study", action="store_true",
+                    help="c3-*: add the sketch precision study to the line")
     ap.add_argument("--no-cpu", action="store_true",
                     help="skip the CPU baseline leg")
     ap.add_argument("--_cpu-run", type=int, default=0, dest="cpu_run")
@@ -977,7 +1153,21 @@ def main():
     # tile and round + the Y columns written); the FP64 engine's sketch is
     # a DMMA GEMM (bound: FP64 tensor, 2 m n k flops per tile)
     per_launch_s = last.sketch_ms / 1e3 / max(1, last.sketch_launches)
-    if last.sketch_int8:
+    if last.fused_launches > 0:
+        # the fused generation + first-round sketch: it writes D (8 m n per
+        # tile) and the round's Y columns; its inputs are the points
+        per_launch_s = last.fused_ms / 1e3 / last.fused_launches
+        bytes_per_launch = last.fused_bytes / last.fused_launches
+        achieved = bytes_per_launch / per_launch_s / 1e9
+        peak, peak_src = measured_hbm_gbs()
+        roof = {"bound": "hbm",
+                "kernel": "k_gen_sketch_i8 (generation fused with the tcgen05 int8 sketch; D and Y written)",
+                "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_src,
+                "algorithmic_bytes_per_launch": bytes_per_launch,
+                "traffic": None,
+                "resketch_tiles": int(last.resketch_tiles)}
+    elif last.sketch_int8:
         bytes_per_launch = last.sketch_bytes / max(1, last.sketch_launches)
         achieved = bytes_per_launch / per_launch_s / 1e9
         peak, peak_src = measured_hbm_gbs()
@@ -1027,13 +1217,17 @@ def main():
                 "d2h_bytes_per_step": int(e2e_st.d2h_bytes),
                 "ms_per_step": t_e2e * 1e3},
         "gpu_launches": int(sum(s.kernel_launches for s in sts)),
-        "phases_ms": {"sketch": last.sketch_ms, "project": last.project_ms,
-                      "total_host": last.total_ms},
+        "phases_ms": {"generation": last.gen_ms, "fused_gen_sketch": last.fused_ms,
+                      "sketch": last.sketch_ms, "basis": last.basis_ms,
+                      "project": last.project_ms, "svd": last.svd_ms,
+                      "output": last.output_ms, "total_host": last.total_ms},
         "roofline": roof,
         "clocks": clocks.summary(),
     }
     if dmml:
         line["dmml"] = dmml
+    if args.precision_study and key.startswith("c3"):
+        line["precision_study"] = precision_study(lib, wl, prob, torch)
     if world == 1 and not args.no_cpu:
         n = wl.get("cpu_n")
         if not n:

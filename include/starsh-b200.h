@@ -181,6 +181,26 @@ int starsh_b200_kernel_register(STARSH_kernel *kernel, int family,
  * *ndim_hint is the dimension fixed by its name (0 for "_nd"). */
 int starsh_b200_kernel_family(STARSH_kernel *kernel, int *ndim_hint);
 
+/* ------------------------------------------------------------ autotuner */
+
+/* Tile-size autotuner.  No counterpart in the reference (which takes the
+ * block size from the caller, src/control/cluster.c:106-146).  For each
+ * candidate block size cand_nb[c] (with maxrank cand_maxrank[c]) it times
+ * starsh_b200_approximate() with `engine` on a fixed-seed random sample of
+ * the problem's TLR blocks -- 24 and then 48 of them, the difference being
+ * the marginal cost free of per-call overheads -- and returns the fastest
+ * in *best_nb (costs, if not NULL, receives ncand costs in nanoseconds per
+ * matrix entry; INFINITY for candidates above N).  Results are cached per
+ * problem class (kernel family and its dimension, N in half-octaves, tol in
+ * decades, engine, candidate list): later problems of a class are not
+ * measured again.  1 <= ncand <= 8.  Runs device work; thread-safe. */
+int starsh_b200_autotune_tile(STARSH_problem *problem, int ncand,
+        const int *cand_nb, const int *cand_maxrank, double tol, int engine,
+        int *best_nb, double *costs);
+
+/* Forgets the autotuner's cached choices. */
+void starsh_b200_autotune_clear(void);
+
 /* ------------------------------------------------ no-allocation variant */
 
 /* Randomized-SVD compression of one dense tile already on the device,
@@ -213,10 +233,13 @@ int starsh_b200_dense_rsvd_noalloc(const double *dD, int nrows, int ncols,
 /* ------------------------------------------------------------ serving */
 
 /* A serving loop: approximation requests are admitted by an HBM budget and
- * run in shared batches (continuous batching: requests that arrive while a
- * group is on the GPU join the next group as memory allows), then each
- * request's TLR-by-dense product runs on the resident factors.  All calls
- * are thread-safe; one worker thread per server drives the GPU. */
+ * run in shared batches, then each request's TLR-by-dense product runs on
+ * the resident factors.  Continuous batching: worker threads (2 by
+ * default, STARSH_B200_SERVER_WORKERS up to 8), each with its own CUDA
+ * streams and buffers, take the next group whenever they are free, so
+ * requests that arrive while a group is on the GPU are admitted by the
+ * other worker as memory allows and the two groups' kernels overlap on the
+ * device.  All calls are thread-safe. */
 typedef struct starsh_b200_server starsh_b200_server;
 
 typedef struct starsh_b200_server_stats
@@ -224,7 +247,8 @@ typedef struct starsh_b200_server_stats
     long long submitted, completed, failed;
     long long groups;             /* batched approximation calls           */
     long long entries;            /* sum of m*n over approximated blocks   */
-    double busy_ms;               /* worker time inside groups             */
+    double busy_ms;               /* worker time inside groups (summed
+                                     over the workers)                     */
     double resident_bytes;        /* results kept and not yet released     */
     double peak_resident_bytes;
 } starsh_b200_server_stats;
@@ -307,6 +331,12 @@ typedef struct starsh_b200_stats
     double sketch_bytes;      /* algorithmic HBM bytes of the sketch:
                                  D read once per round, Y written      */
     int sketch_int8;          /* 1: sketch on the tcgen05 int8 path     */
+    double fused_ms;          /* device time of the fused generation and
+                                 first-round sketch (incl. re-sketches)  */
+    long long fused_launches; /* batches whose round 0 ran fused        */
+    double fused_bytes;       /* algorithmic HBM bytes of the fused
+                                 kernel: D and the round-0 Y written     */
+    long long resketch_tiles; /* tiles re-sketched from the stored D    */
 } starsh_b200_stats;
 int starsh_b200_get_stats(starsh_b200_stats *stats);
 

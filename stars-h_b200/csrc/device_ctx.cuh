@@ -36,7 +36,13 @@ struct Context {
 };
 
 // Initialises (once) and returns the context; nullptr if no usable GPU.
+// A thread that installed its own context (set_thread_context) gets that
+// one instead: its own streams and reusable buffers, so that several host
+// threads (the serving workers) keep work on the GPU at the same time.
 Context *context();
+Context *context_new_private();
+void context_free_private(Context *c);
+void set_thread_context(Context *c);
 
 // Stream-ordered device allocation from the device's memory pool, whose
 // freed memory stays cached for the next call (repeated approximations do

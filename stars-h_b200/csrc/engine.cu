@@ -62,8 +62,17 @@ static thread_local std::string t_error;
 static thread_local starsh_b200_stats t_stats;
 static std::atomic<long long> g_launches{0};
 
+// A context a thread has made its own (a serving worker's), or null.
+static thread_local Context *t_ctx = nullptr;
+
 Context *context()
 {
+    if (t_ctx != nullptr) {
+        int cur = -1;
+        if (cudaGetDevice(&cur) != cudaSuccess || cur != t_ctx->device)
+            cudaSetDevice(t_ctx->device);
+        return t_ctx;
+    }
     std::call_once(g_ctx_once, [] {
         int dev = 0;
         if (g_requested_device >= 0 &&
@@ -104,6 +113,52 @@ Context *context()
     return &g_ctx;
 }
 
+Context *context_new_private()
+{
+    Context *base = nullptr;
+    {
+        Context *saved = t_ctx;
+        t_ctx = nullptr;
+        base = context();        // the library's device, initialised once
+        t_ctx = saved;
+    }
+    if (base == nullptr) return nullptr;
+    Context *c = new Context();
+    c->device = base->device;
+    cudaSetDevice(c->device);
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        delete c;
+        return nullptr;
+    }
+    return c;
+}
+
+void context_free_private(Context *c)
+{
+    if (c == nullptr) return;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    cudaStreamSynchronize(c->side);
+    c->workspace.release();
+    c->tiles.release();
+    c->descs.release();
+    c->omega.release();
+    c->flag.release();
+    c->kernels.release();
+    c->omega8.release();
+    for (int i = 0; i < 2; ++i) {
+        if (c->stage[i]) cudaFreeHost(c->stage[i]);
+        if (c->stage_ev[i]) cudaEventDestroy(c->stage_ev[i]);
+    }
+    cudaStreamDestroy(c->stream);
+    cudaStreamDestroy(c->side);
+    delete c;
+}
+
+void set_thread_context(Context *c) { t_ctx = c; }
+
 void *pool_alloc(size_t bytes, cudaStream_t s)
 {
     void *p = nullptr;
@@ -116,7 +171,9 @@ void *pool_alloc(size_t bytes, cudaStream_t s)
 
 void pool_free(void *p)
 {
-    if (p) cudaFreeAsync(p, g_ctx.stream);
+    // ordered on the calling thread's stream (its own work on p, if any,
+    // precedes the free; matrices are freed after a device synchronisation)
+    if (p) cudaFreeAsync(p, t_ctx != nullptr ? t_ctx->stream : g_ctx.stream);
 }
 
 void set_error(const std::string &msg)
@@ -168,6 +225,54 @@ void fill_kernel(DevKernel &K, const b200_kspec &sp)
     }
 }
 
+// Chebyshev coefficients of G(x) = x^nu e^x K_nu(x) on each interval
+// [2^(q+1), 2^(q+2)] (one CTA per interval): G at the kMaternTabDeg + 1
+// Chebyshev points of the first kind u_j = cos(pi (j + 1/2) / (deg + 1)),
+// x_j = 2^q (u_j + 3), then c_k = 2 / (deg + 1) sum_j G(x_j)
+// cos(pi k (j + 1/2) / (deg + 1)), c_0 halved (the discrete cosine
+// transform of Chebyshev interpolation).  The interpolant is accurate to
+// a few units of 1e-15 relative on every interval (G is analytic in the
+// right half-plane, the nearest singularity is at x = 0).
+__global__ void k_matern_table(double nu, double *tab)
+{
+    constexpr int N1 = kMaternTabDeg + 1;
+    __shared__ double g[N1];
+    const int q = blockIdx.x, j = threadIdx.x;
+    if (j < N1) {
+        const double u = cospi((j + 0.5) / N1);
+        const double x = ldexp(u + 3.0, q);
+        g[j] = exp(nu * log(x)) * bessel_k_large_scaled(nu, x, 2.0);
+    }
+    __syncthreads();
+    if (j < N1) {
+        double c = 0.0;
+        for (int i = 0; i < N1; ++i) c += g[i] * cospi(j * (i + 0.5) / N1);
+        c *= 2.0 / N1;
+        tab[q * N1 + j] = j == 0 ? 0.5 * c : c;
+    }
+}
+
+// Device tables a kernel family needs (the Matérn large-argument table),
+// owned by dp.
+static int prepare_kernel_tables(DevicePoints &dp, cudaStream_t s)
+{
+    DevKernel &K = dp.K;
+    K.matern_tab = nullptr;
+    if ((K.family == FAM_MATERN || K.family == FAM_MATERN2) &&
+        K.matern_half == 0 && K.nu > 0.0) {
+        const size_t n = (size_t)kMaternTabIntervals * (kMaternTabDeg + 1);
+        double *tab = (double *)pool_alloc(n * sizeof(double), s);
+        if (tab == nullptr)
+            return cuda_fail(cudaErrorMemoryAllocation, "Matern table");
+        dp.owned.push_back(tab);
+        k_matern_table<<<kMaternTabIntervals, 32, 0, s>>>(K.nu, tab);
+        count_launch();
+        B200_CUDA(cudaGetLastError(), "k_matern_table");
+        K.matern_tab = tab;
+    }
+    return STARSH_SUCCESS;
+}
+
 // Uploads the point sets of a problem and the cluster pivots.
 int upload_problem(DevicePoints &dp, STARSH_problem *P,
                           STARSH_cluster *R, STARSH_cluster *C,
@@ -180,11 +285,12 @@ int upload_problem(DevicePoints &dp, STARSH_problem *P,
                                    &cp, &cc, P->col_data);
     if (info != STARSH_SUCCESS) return info;
     fill_kernel(dp.K, spec);
+    if ((info = prepare_kernel_tables(dp, s))) return info;
     dp.h_row = rp;
     dp.h_col = cp;
     dp.h_row_count = rc;
     dp.h_col_count = cc;
-    const void *d;
+    const void *d = nullptr;
     const size_t per = (size_t)spec.ndim * sizeof(double);
     if ((info = dp.upload(rp, rc * per, &d, s))) return info;
     dp.K.row_pt = (const double *)d;
@@ -426,6 +532,12 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
     }
     const int8_t *om8 = (const int8_t *)ctx.omega8.ptr;
     const int k_max_all = k_max;   // Omega8's width (batches shadow k_max)
+    // the first round of the adaptive engine may fuse generation and sketch
+    // (opt-in: STARSH_B200_FUSED=1; measured slower than the separate
+    // generator and sketch on the square-exponential and Coulomb batches)
+    bool fuse_gen = false;
+    if (const char *e = getenv("STARSH_B200_FUSED"))
+        fuse_gen = use_i8 && strcmp(e, "1") == 0;
     // E[w^2] of the sketch entries: round(32 g) has variance 1024 + 1/12
     for (TileWork &t : all) t.omega_var = use_i8 ? 1024.0 + 1.0 / 12.0 : 1.0;
     st.sketch_int8 = use_i8 ? 1 : 0;
@@ -465,10 +577,16 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
     std::vector<BatchPlan> plan;
     size_t ws_need = 0;
     long long max_slots = 1;
+    // the adaptive engine's projection on the tensor cores (needs the
+    // int8 path's row maxima and TMA descriptors)
+    // (opt-in: STARSH_B200_PROJ=i8 until it beats the FP64 projection)
+    bool proj_i8 = false;
+    if (const char *e = getenv("STARSH_B200_PROJ"))
+        proj_i8 = use_i8 && ep.engine == STARSH_B200_MIXED && strcmp(e, "i8") == 0;
     for (long long b0 = 0; b0 < ntot;) {
         Workspace probe{};
         int bm = all[b0].m, bn = all[b0].n, bk = all[b0].k;
-        size_t stride = workspace_layout(probe, bm, bn, bk, true);
+        size_t stride = workspace_layout(probe, bm, bn, bk, true, proj_i8);
         long long cap = (long long)(budget / (stride * sizeof(double)));
         cap = std::max<long long>(1, std::min<long long>({cap, ntot - b0, 4096}));
         for (long long q = b0; q < b0 + cap; ++q) {
@@ -478,7 +596,7 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
         }
         // even leading dimension (16-byte column strides for the TMA)
         bm = (bm + 7) / 8 * 8;
-        stride = workspace_layout(probe, bm, bn, bk, true);
+        stride = workspace_layout(probe, bm, bn, bk, true, proj_i8);
         long long fit = (long long)(budget / (stride * sizeof(double)));
         const int nt = (int)std::max<long long>(1, std::min(cap, fit));
         plan.push_back({b0, nt, bm, bn, bk, stride});
@@ -522,15 +640,53 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
         const long long b0 = plan[pi].b0;
         const int nt = plan[pi].nt;
         const int m_max = plan[pi].m, k_max = plan[pi].k;
-        workspace_layout(ws, plan[pi].m, plan[pi].n, plan[pi].k, true);
+        workspace_layout(ws, plan[pi].m, plan[pi].n, plan[pi].k, true, proj_i8);
         ws.base = (double *)ctx.workspace.ptr;
         ws.stride = plan[pi].stride;
         for (int t = 0; t < nt; ++t) all[b0 + t].slot = t;
+        // Round 0 of the adaptive engine with the generation fused into the
+        // tensor-core sketch (every tile samples in round 0); tiles whose
+        // bound-based row scales missed are sketched again from the stored
+        // D, tiles the fused kernel cannot stage (wider than 1024 columns,
+        // more than 4 dimensions) are generated and sketched separately.
+        // Every choice is made per tile: a tile's result does not depend on
+        // its batch.
+        const int bmax0 = std::min(ep.block, k_max);
+        const bool fused = ep.engine == STARSH_B200_MIXED && fuse_gen &&
+            gen_sketch_i8_fits((bmax0 + 15) / 16 * 16);
+        bool any_separate = false;
+        if (fused)
+            for (int t = 0; t < nt; ++t) {
+                TileWork &w = all[b0 + t];
+                if (!gen_sketch_i8_tile_ok(w.n, kernels[w.prob].ndim)) {
+                    w.status |= TILE_GEN_SEPARATE;
+                    any_separate = true;
+                }
+            }
         cudaMemcpyAsync(dt, &all[b0], nt * sizeof(TileWork),
                         cudaMemcpyHostToDevice, s);
         cudaEventRecord(ev[4], s);
-        launch_gen_tiles(d_kernels, dt, nt, ws, s);
-        count_launch();
+        if (fused) {
+            launch_round_setup(dt, nt, ep.block, (int *)ctx.flag.ptr, s);
+            if (any_separate) {
+                launch_gen_tiles(d_kernels, dt, nt, ws, s, TILE_GEN_SEPARATE);
+                count_launch();
+            }
+            if (!launch_gen_sketch_i8(d_kernels, dt, nt, ws, om8, ld_om8,
+                                      k_max_all, bmax0, s) ||
+                !launch_sketch_i8(dt, nt, ws, om8, ld_om8, k_max_all, bmax0, s,
+                                  TILE_RESKETCH | TILE_GEN_SEPARATE)) {
+                set_error("no TMA tensor map for the fused sketch");
+                info = STARSH_UNKNOWN_ERROR;
+                break;
+            }
+            count_launch(3);
+            const cudaError_t ce = cudaGetLastError();
+            if (ce != cudaSuccess) { info = cuda_fail(ce, "k_gen_sketch_i8"); break; }
+        } else {
+            launch_gen_tiles(d_kernels, dt, nt, ws, s);
+            count_launch();
+        }
         cudaEventRecord(ev[5], s);
         // exact ||D||_F^2 of every block (generator partial sums)
         launch_block_norms(dt, dt, nt, ws, s);
@@ -598,6 +754,9 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
         };
         for (int round = 0; info == STARSH_SUCCESS; ++round) {
             const int block = round == 0 ? ep.block : ep.block_next;
+            const int bmax = std::min(block, k_max);
+            const bool pre_sketched = fused && round == 0;
+            if (!pre_sketched) {
             launch_round_setup(dt, nt, block, d_active, s);
             count_launch();
             int active = 0;
@@ -605,9 +764,11 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
                                       cudaMemcpyDeviceToHost, s), "round flag");
             B200_CUDA(cudaStreamSynchronize(s), "round flag");
             if (!active) break;
-            const int bmax = std::min(block, k_max);
+            }
             cudaEventRecord(ev[0], s);
-            if (use_i8) {
+            if (pre_sketched) {
+                // Y of round 0 came with the generation
+            } else if (use_i8) {
                 // every batch has an even leading dimension (plan), so the
                 // tensor map exists unless the driver lacks the entry point
                 if (!launch_sketch_i8(dt, nt, ws, om8, ld_om8, k_max_all, bmax, s)) {
@@ -641,16 +802,28 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
             }
             launch_round_end(dt, nt, ep.verify, s);
             count_launch();
-            float ms = 0.f;
-            cudaEventSynchronize(ev[1]);
-            cudaEventElapsedTime(&ms, ev[0], ev[1]);
-            st.sketch_ms += ms;
-            st.sketch_launches += 1;
+            if (!pre_sketched) {
+                float ms = 0.f;
+                cudaEventSynchronize(ev[1]);
+                cudaEventElapsedTime(&ms, ev[0], ev[1]);
+                st.sketch_ms += ms;
+                st.sketch_launches += 1;
+            }
         }
         if (info) break;
         }
-        // projection and small SVD
+        // projection (tiles with at most 64 basis columns on the tensor
+        // cores, the others FP64) and small SVD
         cudaEventRecord(ev[2], s);
+        if (proj_i8) {
+            launch_proj_prep(dt, nt, ws, s);
+            if (!launch_proj_i8(dt, nt, ws, s)) {
+                set_error("no TMA tensor map for the projection");
+                info = STARSH_UNKNOWN_ERROR;
+                break;
+            }
+            count_launch(2);
+        }
         if ((info = gemm(STEP_PROJECT, true, false, nt, k_max, plan[pi].n, none))) break;
         cudaEventRecord(ev[3], s);
         if ((info = gemm(STEP_GRAM_B, false, true, nt, k_max, k_max, none))) break;
@@ -667,6 +840,10 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
         B200_CUDA(cudaStreamSynchronize(s), "compression pipeline");
         st.project_ms += phase_ms(2, 3);
         st.gen_ms += phase_ms(4, 5);
+        if (fused) {
+            st.fused_ms += phase_ms(4, 5);
+            st.fused_launches += 1;
+        }
         st.basis_ms += phase_ms(5, 2);
         st.svd_ms += phase_ms(3, 6);
         if (output_pending) st.output_ms += phase_ms(7, 8);
@@ -682,10 +859,19 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
                 (ep.engine == STARSH_B200_FP64 ? w.k : w.cols_done);
             {
                 // D is read once per round the tile takes part in, Y written
+                // (the fused round 0 writes D and its Y instead of reading D)
                 const int cols = ep.engine == STARSH_B200_FP64 ? w.k : w.cols_done;
-                const int rounds = ep.engine == STARSH_B200_FP64 ? 1
+                int rounds = ep.engine == STARSH_B200_FP64 ? 1
                     : 1 + (std::max(0, cols - ep.block) + ep.block_next - 1) / ep.block_next;
-                st.sketch_bytes += 8.0 * ((double)w.m * w.n * rounds + (double)w.m * cols);
+                int ycols = cols;
+                if (fused) {
+                    const int c0 = std::min(cols, bmax0);
+                    st.fused_bytes += 8.0 * ((double)w.m * w.n + (double)w.m * c0);
+                    rounds -= 1;
+                    ycols -= c0;
+                    if (w.status & TILE_RESKETCH) st.resketch_tiles += 1;
+                }
+                st.sketch_bytes += 8.0 * ((double)w.m * w.n * rounds + (double)w.m * ycols);
             }
             st.project_flops += 2.0 * w.m * w.n * w.k1;
             if (w.status & TILE_MMA_TIMEOUT) {
@@ -1331,9 +1517,10 @@ extern "C" void b200_eval_block_host(STARSH_kernel *kernel, int nrows,
     }
     DevicePoints dp;
     fill_kernel(dp.K, spec);
-    const void *d;
+    int info = prepare_kernel_tables(dp, s);
+    const void *d = nullptr;
     const size_t per = (size_t)spec.ndim * sizeof(double);
-    int info = dp.upload(rp, rc * per, &d, s);
+    if (!info) info = dp.upload(rp, rc * per, &d, s);
     dp.K.row_pt = (const double *)d;
     dp.K.row_count = rc;
     if (!info) info = dp.upload(cp, cc * per, &d, s);

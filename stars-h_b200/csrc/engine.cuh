@@ -15,6 +15,11 @@ enum : int {
     TILE_JACOBI_SLOW = 2,  // Jacobi sweeps hit their cap
     TILE_TAIL_LEFT = 4,    // energy outside the factors alone exceeds tol
     TILE_MMA_TIMEOUT = 8,  // a tensor-core wait of the sketch gave up
+    TILE_RESKETCH = 16,    // the fused generator's row scales missed the
+                           // exact row maxima: sketch again from stored D
+    TILE_GEN_SEPARATE = 32,// too wide (or too many dimensions) for the
+                           // fused kernel: separate generator and sketch
+    TILE_PROJ_I8 = 64,     // projection on the tensor cores
 };
 
 // One far-field tile of a batch.
@@ -54,6 +59,9 @@ struct Workspace {
     size_t stride;          // doubles per slot
     int m_max, n_max, k_max;
     size_t oD, oY, oQ1, oQ, oS, oL, oT, oB, oC, oE, oSig, oPiv, oOrd, oNrm, oR, oRmx;
+    // tensor-core projection (adaptive engine): byte slices of the scaled
+    // basis, row and column exponents (0 when the layout has none)
+    size_t oQd, oQe, oQf;
 
     __host__ __device__ double *D(int s) const { return base + s * stride + oD; }
     __host__ __device__ double *Y(int s) const { return base + s * stride + oY; }
@@ -74,15 +82,21 @@ struct Workspace {
     __host__ __device__ double *Nrm(int s) const { return base + s * stride + oNrm; }
     // m x k temporary of the adaptive rounds (ld = m_max)
     __host__ __device__ double *R(int s) const { return base + s * stride + oR; }
+    __host__ __device__ uint8_t *Qd(int s) const { return (uint8_t *)(base + s * stride + oQd); }
+    __host__ __device__ int *Qe(int s) const { return (int *)(base + s * stride + oQe); }
+    __host__ __device__ int *Qf(int s) const { return (int *)(base + s * stride + oQf); }
+    // bytes per row of a Qd slice (rows: basis columns)
+    __host__ __device__ int ldQd() const { return (m_max + 31) / 32 * 32; }
     // leading dimensions
     __host__ __device__ int ldD() const { return m_max; }
     __host__ __device__ int ldM() const { return m_max; }   // Y, Q1, Q
     __host__ __device__ int ldK() const { return k_max; }   // S, L, T, B, C
 };
 
-// Layout for the given maxima; returns doubles per slot.
+// Layout for the given maxima; returns doubles per slot.  proj_digits
+// adds the fields of the tensor-core projection.
 size_t workspace_layout(Workspace &w, int m_max, int n_max, int k_max,
-                        bool store_d);
+                        bool store_d, bool proj_digits = false);
 
 // GEMM steps of the pipeline, each turned into descriptors on the device.
 enum GemmStep : int {
@@ -130,8 +144,10 @@ void make_gemm_descs(GemmStep step, const TileWork *d_tiles, int ntiles,
 // Per-tile kernels (one CTA per tile).
 // Thresholds come from each tile's tol and maxrank; the generator reads
 // the tile's kernel from d_kernels[tile.prob].
+// need != 0: only tiles whose status has a bit of `need`.
 void launch_gen_tiles(const DevKernel *d_kernels, const TileWork *d_tiles,
-                      int ntiles, Workspace ws, cudaStream_t stream);
+                      int ntiles, Workspace ws, cudaStream_t stream,
+                      int need = 0);
 void launch_pivchol(int phase, const TileWork *d_tiles, TileWork *d_tiles_rw,
                     int ntiles, Workspace ws, cudaStream_t s);
 void launch_gather_cols(int phase, const TileWork *d_tiles, int ntiles,
@@ -156,6 +172,15 @@ void launch_round_pivchol(TileWork *d_tiles, int ntiles, Workspace ws,
                           int repeat, cudaStream_t stream);
 void launch_select_w(const TileWork *d_tiles, int ntiles, Workspace ws,
                      cudaStream_t stream);
+// Tensor-core projection B = Q^T D (proj_i8.cu) of the tiles with at most
+// 64 basis columns and 4096 rows: the preparation flags them
+// TILE_PROJ_I8 (the FP64 projection step skips them).  launch_proj_i8
+// returns false (nothing launched) when the layout has no digit fields or
+// the TMA descriptors cannot be made.
+void launch_proj_prep(TileWork *d_tiles, int ntiles, Workspace ws,
+                      cudaStream_t stream);
+bool launch_proj_i8(TileWork *d_tiles, int ntiles, Workspace ws,
+                    cudaStream_t stream);
 void launch_write_v(const TileWork *d_tiles, int ntiles, Workspace ws,
                     OutArena out, cudaStream_t stream);
 // Adaptive sketch on the tensor cores (int8 digits of D, see
@@ -167,7 +192,20 @@ bool sketch_i8_fits(int ncols, int n_max);
 // described to the TMA unit (odd leading dimension).
 bool launch_sketch_i8(const TileWork *d_tiles, int ntiles, Workspace ws,
                       const int8_t *om8, int ld_om8, int om8_cols, int ncols,
-                      cudaStream_t stream);
+                      cudaStream_t stream, int need = 0);
+// First sampling round with the generation fused in (gen_sketch_i8.cu):
+// D, its exact norms and row maxima, and Y(:, 0:bcur) = D Omega8(:, 0:nc)
+// with bound-based row scales; tiles whose bound missed are flagged
+// TILE_RESKETCH.  Tiles flagged TILE_GEN_SEPARATE are skipped.
+// gen_sketch_i8_fits(): the round's width is supported (ncols <= 64);
+// gen_sketch_i8_tile_ok(): a tile can be generated by it (n <= 1024,
+// ndim <= 4).
+bool gen_sketch_i8_fits(int nc);
+bool gen_sketch_i8_tile_ok(int n, int ndim);
+bool launch_gen_sketch_i8(const DevKernel *d_kernels, TileWork *d_tiles,
+                          int ntiles, Workspace ws, const int8_t *om8,
+                          int ld_om8, int om8_cols, int ncols,
+                          cudaStream_t stream);
 // Omega8(j, c) = clip(round(32 g), -127, 127), g the Gaussian of
 // launch_gaussian's (j, c); rows past `rows` up to ld are zero.
 void launch_gaussian_i8(int8_t *d_om8, int rows, int cols, int ld,

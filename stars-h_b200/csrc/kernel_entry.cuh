@@ -1,5 +1,5 @@
 // Device evaluation of one kernel-matrix entry, shared by the tile
-// generator, the fused sketch kernels and the error kernel.
+// generator, the fused generation-and-sketch kernel and the error kernel.
 //
 // Each family computes the same expression, in the same operation order,
 // as the reference kernel of that name (src/applications/spatial/
@@ -34,6 +34,9 @@ struct DevKernel {
     double sigma, beta, nu, noise;
     double matern_coef, matern_scale;
     int matern_half;          // 1, 2, 3 for nu = 1/2, 3/2, 5/2; else 0
+    // Matérn with other nu: Chebyshev coefficients of x^nu e^x K_nu(x) on
+    // [2^(q+1), 2^(q+2)], q < kMaternTabIntervals (device, or null)
+    const double *matern_tab;
     double inv_neg_beta;      // -1/beta (exp)
     double inv_neg_2beta2;    // 1/((-2 beta) beta) (square exponential)
     double wave_k, diag;
@@ -44,6 +47,11 @@ struct DevKernel {
     const long long *row_piv; // cluster pivots (STARSH_int)
     const long long *col_piv;
 };
+
+// Matérn table: kMaternTabIntervals dyadic intervals covering [2, 1024),
+// each with kMaternTabDeg + 1 Chebyshev coefficients.
+constexpr int kMaternTabDeg = 18;
+constexpr int kMaternTabIntervals = 9;
 
 // Taylor coefficients of 1/Gamma(1+z) about z = 0 (a_0 = 1, a_1 = Euler's
 // gamma, ...), computed with mpmath at 50 digits by
@@ -146,14 +154,18 @@ __device__ inline void bessel_k_temme(double mu, double x, double *kmu,
 // exp(-2 pi c / h + c^2) for c <= d; h = min(0.49, 2 pi d / (41 + d^2))
 // keeps it below ~1e-17 (checked against mpmath to 1e-14 relative for
 // 0.1 <= nu <= 4.7, 2 < x <= 300).  Nodes stop where e^{-s^2} < 1e-19.
-__device__ inline double bessel_k_large(double nu, double x)
+// e^x K_nu(x) for x > 2 (the integral below without its factor e^-x),
+// with the step divided by `refine` (1 in the generators; the table
+// builder takes 2, for node values limited by rounding only).
+__device__ inline double bessel_k_large_scaled(double nu, double x,
+                                               double refine)
 {
     const double two_x = 2.0 * x;
     const double d = sqrt(two_x);
-    const double h = fmin(0.49, 2.0 * M_PI * d / (41.0 + two_x));
+    const double h = fmin(0.49, 2.0 * M_PI * d / (41.0 + two_x)) / refine;
     const double inv_d = 1.0 / d;
     double sum = 0.0;
-    for (int k = 0; k < 64; ++k) {
+    for (int k = 0; k < 256; ++k) {
         const double s = k * h;
         const double w = exp(-s * s);
         if (w < 1e-19) break;
@@ -163,7 +175,31 @@ __device__ inline double bessel_k_large(double nu, double x)
         const double g = 0.5 * (ap + 1.0 / ap) * 2.0 / sqrt(two_x + s * s);
         sum += (k == 0 ? 0.5 : 1.0) * w * g;
     }
-    return h * sum * exp(-x);
+    return h * sum;
+}
+
+__device__ inline double bessel_k_large(double nu, double x)
+{
+    return bessel_k_large_scaled(nu, x, 1.0) * exp(-x);
+}
+
+// x^nu e^x K_nu(x) for 2 <= x < 1024 from the problem's Chebyshev table:
+// x = 2^E m, m in [1, 2), lies in interval E - 1, at u = 2 m - 3 in
+// [-1, 1) (exact); Clenshaw's recurrence sums the series.
+__device__ __forceinline__ double matern_tab_eval(const double *tab, double x)
+{
+    const int E = (__double2hiint(x) >> 20) - 1023;
+    const double *c = tab + (size_t)(E - 1) * (kMaternTabDeg + 1);
+    const double u = x * __hiloint2double((1024 - E) << 20, 0) - 3.0;
+    const double u2 = 2.0 * u;
+    double b1 = 0.0, b2 = 0.0;
+    #pragma unroll
+    for (int k = kMaternTabDeg; k >= 1; --k) {
+        const double b0 = fma(u2, b1, c[k] - b2);
+        b2 = b1;
+        b1 = b0;
+    }
+    return fma(u, b1, c[0] - b2);
 }
 
 // K_nu(x), nu >= 0, x > 0.  Small arguments: Temme's series at
@@ -232,7 +268,13 @@ __device__ __forceinline__ double entry_fam(const DevKernel &K, double dist,
         case 1: return K.sigma * exp(-x);
         case 2: return K.sigma * ((1.0 + x) * exp(-x));
         case 3: return K.sigma * ((1.0 + x * (1.0 + x * (1.0 / 3.0))) * exp(-x));
-        default: return K.matern_coef * pow(x, K.nu) * bessel_knu(K.nu, x);
+        default:
+            if (K.matern_tab != nullptr && x >= 2.0) {
+                // e^-x underflows to zero long before 1024
+                if (!(x < 1024.0)) return 0.0;
+                return K.matern_coef * (exp(-x) * matern_tab_eval(K.matern_tab, x));
+            }
+            return K.matern_coef * pow(x, K.nu) * bessel_knu(K.nu, x);
         }
     } else if constexpr (FAM == FAM_COULOMB) {
         if (dist == 0.0) return K.zero_mode ? K.diag : 0.0;

@@ -26,7 +26,7 @@ namespace b200 {
 // ------------------------------------------------------------ layout
 
 size_t workspace_layout(Workspace &w, int m_max, int n_max, int k_max,
-                        bool store_d)
+                        bool store_d, bool proj_digits)
 {
     size_t o = 0;
     auto take = [&](size_t n) {
@@ -53,6 +53,13 @@ size_t workspace_layout(Workspace &w, int m_max, int n_max, int k_max,
     w.oNrm = take((size_t)((m_max + 63) / 64) * ((n_max + 63) / 64));
     w.oR = take((size_t)m_max * k_max);
     w.oRmx = take((size_t)m_max * ((n_max + 63) / 64));
+    w.oQd = w.oQe = w.oQf = 0;
+    if (proj_digits) {
+        // 7 byte slices x 64 basis columns x ldQd bytes; m ints; 64 ints
+        w.oQd = take((size_t)7 * 64 * ((m_max + 31) / 32 * 32) / 8);
+        w.oQe = take(((size_t)m_max + 1) / 2);
+        w.oQf = take(32);
+    }
     w.stride = o;
     return o;
 }
@@ -132,10 +139,11 @@ __device__ __forceinline__ double gen_entries_dim(
 
 __global__ void __launch_bounds__(256, 3)
 k_gen_tiles(const DevKernel *__restrict__ kernels,
-            const TileWork *__restrict__ tiles, Workspace ws)
+            const TileWork *__restrict__ tiles, Workspace ws, int need)
 {
     const TileWork tw = tiles[blockIdx.z];
     if (blockIdx.x * 64 >= tw.m || blockIdx.y * 64 >= tw.n) return;
+    if (need != 0 && (tw.status & need) == 0) return;
     __shared__ double rc[kStageDim][64], cc[kStageDim][64];
     __shared__ long long ri[64], ci[64];
     __shared__ double red[8];
@@ -213,10 +221,10 @@ k_gen_tiles(const DevKernel *__restrict__ kernels,
 }
 
 void launch_gen_tiles(const DevKernel *d_kernels, const TileWork *d_tiles,
-                      int ntiles, Workspace ws, cudaStream_t stream)
+                      int ntiles, Workspace ws, cudaStream_t stream, int need)
 {
     dim3 grid((ws.m_max + 63) / 64, (ws.n_max + 63) / 64, ntiles);
-    k_gen_tiles<<<grid, 256, 0, stream>>>(d_kernels, d_tiles, ws);
+    k_gen_tiles<<<grid, 256, 0, stream>>>(d_kernels, d_tiles, ws, need);
 }
 
 // ---------------------------------------------------- Gaussian sketch
@@ -422,6 +430,7 @@ __global__ void k_make_desc(GemmStep step, const TileWork *__restrict__ tiles,
         d.B = ws.D(s); d.ldb = ws.ldD();
         d.C = ws.B(s); d.ldc = ldk;
         d.M = tw.k1; d.N = tw.n; d.K = tw.m;
+        if (tw.status & TILE_PROJ_I8) d.M = 0;   // on the tensor cores
         break;
     case STEP_GRAM_B:   // NT: S = B B^T
         d.A = ws.B(s); d.lda = ldk;
@@ -1595,28 +1604,52 @@ void launch_select_w(const TileWork *d_tiles, int ntiles, Workspace ws,
     k_select_w<<<ntiles, 256, 0, stream>>>(d_tiles, ws);
 }
 
-// V(j, c) = C(ord[c], j): V is n x rank, leading dimension n.
-__global__ void k_write_v(const TileWork *__restrict__ tiles, Workspace ws,
-                          OutArena out)
+// V(j, c) = C(ord[c], j): V is n x rank, leading dimension n.  A CTA
+// transposes `cols` (8, 16 or 32) columns j of C at a time through shared
+// memory: it reads the k2 rows of those columns (contiguous in C) and
+// writes the rank selected rows as `cols` consecutive entries of each
+// column of V, so both sides are coalesced.
+__global__ void __launch_bounds__(256)
+k_write_v(const TileWork *__restrict__ tiles, Workspace ws, OutArena out,
+          int cols)
 {
+    extern __shared__ double wv_sm[];   // [cols][k2 + 1]
     const TileWork tw = tiles[blockIdx.x];
     if (tw.rank <= 0) return;
     const int s = tw.slot, ld = ws.ldK();
     const int *ord = ws.Ord(s);
     const double *C = ws.C(s);
     double *V = out.V + tw.off_v;
-    for (int c = blockIdx.y; c < tw.rank; c += gridDim.y) {
-        const int row = ord[c];
-        for (int j = threadIdx.x; j < tw.n; j += blockDim.x)
-            V[(size_t)c * tw.n + j] = C[(size_t)j * ld + row];
+    const int kr = tw.k2, ls = kr + 1;   // rows of C; ord[c] < k2
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    for (int j0 = blockIdx.y * cols; j0 < tw.n; j0 += gridDim.y * cols) {
+        const int nj = min(cols, tw.n - j0);
+        // warp w reads columns j0 + w, j0 + w + 8, ...: k2 contiguous rows
+        for (int jj = warp; jj < nj; jj += 8)
+            for (int i = lane; i < kr; i += 32)
+                wv_sm[jj * ls + i] = C[(size_t)(j0 + jj) * ld + i];
+        __syncthreads();
+        for (int c = warp; c < tw.rank; c += 8) {
+            const int row = ord[c];
+            if (lane < nj) V[(size_t)c * tw.n + j0 + lane] = wv_sm[lane * ls + row];
+        }
+        __syncthreads();
     }
 }
 
 void launch_write_v(const TileWork *d_tiles, int ntiles, Workspace ws,
                     OutArena out, cudaStream_t stream)
 {
+    // 32 columns per pass while the tile fits 96 KB, fewer for wide bases
+    int cols = 32;
+    while (cols > 8 && (size_t)cols * (ws.k_max + 1) * sizeof(double) > 96 * 1024)
+        cols /= 2;
+    const size_t smem = (size_t)cols * (ws.k_max + 1) * sizeof(double);
+    if (smem > 48 * 1024)
+        cudaFuncSetAttribute(k_write_v, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
     dim3 grid(ntiles, 8);
-    k_write_v<<<grid, 256, 0, stream>>>(d_tiles, ws, out);
+    k_write_v<<<grid, 256, smem, stream>>>(d_tiles, ws, out, cols);
 }
 
 }  // namespace b200

@@ -2,16 +2,22 @@
 // shared batches (continuous batching), each followed by its TLR-by-dense
 // products on the resident factors.
 //
-// A worker thread owns the GPU work.  Requests wait in FIFO order; whenever
-// the worker is free it admits, from the head of the queue, every request
-// whose estimated device footprint still fits in the budget next to the
-// results that are resident, and runs them as one starsh_b200_approximate_
-// batch() call: their tiles share every launch.  Requests that arrive while
-// a group is on the GPU are admitted with the next group, as memory allows.
-// After the group, each request's products B = M A run on the device and
-// the request completes (latency = submit to completion, host clock).
+// Worker threads (two by default, STARSH_B200_SERVER_WORKERS) own the GPU
+// work, each on its own engine context (streams and reusable buffers), so
+// that two groups are on the GPU at the same time and their launches
+// interleave.  Requests wait in FIFO order; a worker that becomes free
+// admits, from the head of the queue, every request whose estimated device
+// footprint still fits in the budget next to the results that are resident
+// and the groups other workers are running, and runs them as one
+// starsh_b200_approximate_batch() call: their tiles share every launch.
+// Requests that arrive while groups are on the GPU are admitted by the next
+// free worker, as memory allows.  After its group, each request's products
+// B = M A run on the device (same worker, same stream) and the request
+// completes (latency = submit to completion, host clock).
+#include <algorithm>
 #include <chrono>
 #include <condition_variable>
+#include <cstdlib>
 #include <deque>
 #include <mutex>
 #include <thread>
@@ -62,10 +68,11 @@ struct starsh_b200_server {
     std::unordered_map<const STARSH_blrm *, double> resident_of;
     double resident = 0.0;
     long long next_ticket = 1;
+    double inflight = 0.0;            // estimates of groups being run
     bool stop = false;
     bool paused = false;
     starsh_b200_server_stats stats{};
-    std::thread worker;
+    std::vector<std::thread> workers;
 };
 
 namespace b200 {
@@ -104,12 +111,21 @@ static void complete(starsh_b200_server *sv, Request *r, int status,
 
 static void worker_loop(starsh_b200_server *sv)
 {
+    // this worker's engine context (the shared one if it cannot be made)
+    Context *own = context_new_private();
+    set_thread_context(own);
     for (;;) {
         std::vector<Request *> group;
+        double group_estimate = 0.0;
         {
             std::unique_lock<std::mutex> lk(sv->mu);
             for (;;) {
-                if (sv->stop && sv->pending.empty()) return;
+                if (sv->stop && sv->pending.empty()) {
+                    lk.unlock();
+                    set_thread_context(nullptr);
+                    context_free_private(own);
+                    return;
+                }
                 // refuse requests larger than the whole budget
                 while (!sv->pending.empty() &&
                        sv->pending.front()->estimate > sv->budget) {
@@ -118,15 +134,19 @@ static void worker_loop(starsh_b200_server *sv)
                     complete(sv, r, STARSH_MALLOC_ERROR, nullptr);
                     sv->cv_done.notify_all();
                 }
-                double room = sv->budget - sv->resident;
+                double room = sv->budget - sv->resident - sv->inflight;
                 while (!sv->paused && !sv->pending.empty() &&
                        (int)group.size() < sv->max_group &&
                        sv->pending.front()->estimate <= room) {
                     room -= sv->pending.front()->estimate;
+                    group_estimate += sv->pending.front()->estimate;
                     group.push_back(sv->pending.front());
                     sv->pending.pop_front();
                 }
-                if (!group.empty()) break;
+                if (!group.empty()) {
+                    sv->inflight += group_estimate;
+                    break;
+                }
                 // nothing admissible: wait for a request or a release
                 sv->cv_work.wait(lk);
             }
@@ -158,6 +178,7 @@ static void worker_loop(starsh_b200_server *sv)
         }
         {
             std::lock_guard<std::mutex> lk(sv->mu);
+            sv->inflight -= group_estimate;
             if (info == STARSH_SUCCESS) sv->stats.entries += st.entries;
             for (int i = 0; i < np; ++i) {
                 Request *r = group[i];
@@ -180,6 +201,8 @@ static void worker_loop(starsh_b200_server *sv)
                                      std::chrono::steady_clock::now() - t0).count();
         }
         sv->cv_done.notify_all();
+        // memory came back: another worker may admit now
+        sv->cv_work.notify_all();
     }
 }
 
@@ -196,7 +219,10 @@ extern "C" int starsh_b200_server_new(starsh_b200_server **server,
     sv->budget = hbm_budget_bytes;
     sv->engine = engine;
     sv->max_group = max_group > 0 ? max_group : 1 << 30;
-    sv->worker = std::thread(worker_loop, sv);
+    int nw = 2;
+    if (const char *e = getenv("STARSH_B200_SERVER_WORKERS"))
+        nw = std::max(1, std::min(8, atoi(e)));
+    for (int w = 0; w < nw; ++w) sv->workers.emplace_back(worker_loop, sv);
     *server = sv;
     return STARSH_SUCCESS;
 }
@@ -304,7 +330,7 @@ extern "C" int starsh_b200_server_free(starsh_b200_server *server)
         server->paused = false;
     }
     server->cv_work.notify_all();
-    server->worker.join();
+    for (std::thread &w : server->workers) w.join();
     // requests nobody waited for
     for (auto &kv : server->requests) {
         if (kv.second->M) starsh_blrm_free(kv.second->M);

@@ -44,8 +44,8 @@
 #include <algorithm>
 #include <cstdint>
 #include <cuda.h>
-#include <cudaTypedefs.h>
 #include "engine.cuh"
+#include "tc_common.cuh"
 
 namespace b200 {
 
@@ -64,100 +64,12 @@ constexpr int kAbufBytes = kSlices * kSkRows * kSkChunk;                // 20 KB
 constexpr int kDStageBytes = kSkRows * kSkChunk * (int)sizeof(double);  // 32 KB
 constexpr int kOmSlotBytes = kSkChunk * kSkMaxN;                        // 2 KB
 
-// Shared-memory descriptor of a K-major operand without swizzle:
-// core matrices of 8 rows x 16 bytes (128 contiguous bytes), lbo = byte
-// distance between the two 16-byte K halves of one MMA, sbo = byte
-// distance between consecutive 8-row groups.
-__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo,
-                                              uint32_t sbo)
-{
-    uint64_t d = 0;
-    d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
-    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
-    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
-    d |= (uint64_t)1 << 46;            // descriptor version (sm_100)
-    return d;                          // base offset 0, no swizzle
-}
-
 // Instruction descriptor: int32 accumulator, int8 A (unsigned digits, or
 // the signed top digit), signed int8 B (Omega), both K-major, M = 128,
 // N = n.
 __host__ __device__ constexpr uint32_t idesc_i8(int n, bool a_signed)
 {
-    return (2u << 4) | ((a_signed ? 1u : 0u) << 7) | (1u << 10) |
-           ((uint32_t)(n >> 3) << 17) | ((uint32_t)(kSkRows >> 4) << 24);
-}
-
-__device__ __forceinline__ uint32_t smem_u32(const void *p)
-{
-    return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t da,
-                                       uint64_t db, uint32_t idesc,
-                                       int accumulate)
-{
-    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-                 "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}"
-                 :: "r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(accumulate));
-}
-
-// Arrives (once) on mbar when every MMA this thread issued so far is done.
-__device__ __forceinline__ void mma_commit(uint64_t *mbar)
-{
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
-                 :: "r"(smem_u32(mbar)));
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t *mbar, int count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;"
-                 :: "r"(smem_u32(mbar)), "r"(count));
-}
-
-__device__ __forceinline__ bool mbar_try(uint64_t *mbar, uint32_t parity)
-{
-    uint32_t ok;
-    asm volatile("{\n\t.reg .pred P1;\n\t"
-                 "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
-                 "selp.b32 %0, 1, 0, P1;\n\t}"
-                 : "=r"(ok) : "r"(smem_u32(mbar)), "r"(parity) : "memory");
-    return ok != 0;
-}
-
-// Waits for the completion of the phase of the given parity; gives up
-// after about two seconds, or as soon as *abort is set by another thread,
-// and returns false.
-__device__ __forceinline__ bool mbar_wait_or(uint64_t *mbar, uint32_t parity,
-                                             volatile int *abort)
-{
-    const long long t0 = clock64();
-    while (!mbar_try(mbar, parity)) {
-        if (*abort) return false;
-        if (clock64() - t0 > (1ll << 32)) return false;
-    }
-    return true;
-}
-
-__device__ __forceinline__ void mbar_arrive(uint64_t *mbar)
-{
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];"
-                 :: "r"(smem_u32(mbar)) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *mbar, uint32_t bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
-                 :: "r"(smem_u32(mbar)), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[8])
-{
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 "
-                 "{%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]),
-                   "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
-                 : "r"(taddr));
+    return idesc_i8_mn(kSkRows, n, a_signed);
 }
 
 // Digits of 8 entries x in (-1, 1), given as y = x 2^39 + 1.5 2^52 (one
@@ -192,17 +104,13 @@ __device__ __forceinline__ void digits8(const double (&y)[8],
     }
 }
 
-// TMA tile copy (this CTA only) of the 128 x 32 FP64 box at (row0, col0,
-// slot) of the workspace's D tensor; completes on mbar.
+// TMA tile copy of the 128 x 32 FP64 box at (row0, col0, slot) of the
+// workspace's D tensor; completes on mbar.
 __device__ __forceinline__ void tma_load_d(void *dst, const CUtensorMap *map,
                                            int row0, int col0, int slot,
                                            uint64_t *mbar)
 {
-    asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes "
-                 "[%0], [%1, {%2, %3, %4}], [%5];"
-                 :: "r"(smem_u32(dst)), "l"(map), "r"(row0), "r"(col0), "r"(slot),
-                    "r"(smem_u32(mbar))
-                 : "memory");
+    tma_load_3d(dst, map, row0, col0, slot, mbar);
 }
 
 // TMA tile copy of the 16 (rows k) x nc (columns c) byte box of Omega8 at
@@ -210,11 +118,7 @@ __device__ __forceinline__ void tma_load_d(void *dst, const CUtensorMap *map,
 __device__ __forceinline__ void tma_load_om(void *dst, const CUtensorMap *map,
                                             int k0, int c0, uint64_t *mbar)
 {
-    asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes "
-                 "[%0], [%1, {%2, %3}], [%4];"
-                 :: "r"(smem_u32(dst)), "l"(map), "r"(k0), "r"(c0),
-                    "r"(smem_u32(mbar))
-                 : "memory");
+    tma_load_2d(dst, map, k0, c0, mbar);
 }
 
 // Exponent e of the largest |D_ij| of row i over the tile's n columns
@@ -236,13 +140,21 @@ __device__ __forceinline__ int row_exponent(const Workspace &ws, int m,
 
 // The tile fields the kernel reads, loaded once per item.
 struct SkItem {
-    int m, n, bcur, slot, cols_done;
+    int m, n, bcur, slot, cols_done, status;
 };
 
 __device__ __forceinline__ SkItem sk_item(const TileWork *tiles, int tile)
 {
     const TileWork *w = tiles + tile;
-    return SkItem{w->m, w->n, w->bcur, w->slot, w->cols_done};
+    return SkItem{w->m, w->n, w->bcur, w->slot, w->cols_done, w->status};
+}
+
+// A tile takes part when its round is active and, if `need` is non-zero,
+// its status has one of the bits of `need` (tiles the fused generator
+// flagged for a re-sketch from the stored D).
+__device__ __forceinline__ bool sk_active(const SkItem &w, int need)
+{
+    return w.bcur > 0 && (need == 0 || (w.status & need) != 0);
 }
 
 // Y(:, 0:bcur) of every tile with an active round = D * Omega8(:, cols_done
@@ -252,7 +164,7 @@ __global__ void __launch_bounds__(kSkThreads, 1)
 k_sketch_i8(const __grid_constant__ CUtensorMap dmap,
             const __grid_constant__ CUtensorMap omap,
             const TileWork *__restrict__ tiles, int ntiles, Workspace ws,
-            int nc)
+            int nc, int need)
 {
     extern __shared__ __align__(1024) uint8_t sk_smem_raw[];
     __shared__ __align__(8) uint64_t full[kStages];    // chunk landed
@@ -285,7 +197,7 @@ k_sketch_i8(const __grid_constant__ CUtensorMap dmap,
             mbar_init(&empty[q], 1);
         }
         for (int b = 0; b < kAbufs; ++b) {
-            mbar_init(&afull[b], kConvThreads);
+            mbar_init(&afull[b], kConvThreads / 32);
             mbar_init(&afree[b], 1);
         }
         mbar_init(&accfull, 1);
@@ -319,11 +231,14 @@ k_sketch_i8(const __grid_constant__ CUtensorMap dmap,
             if (item + gridDim.x < nitems)   // the next item's fields, early
                 wn = sk_item(tiles, (int)((item + gridDim.x) / rpt));
             const int row0 = (int)(item % rpt) * kSkRows;
-            if (w.bcur <= 0 || row0 >= w.m) continue;
+            if (!sk_active(w, need) || row0 >= w.m) continue;
             const int nchunks = (w.n + kSkChunk - 1) / kSkChunk;
             const int i = row0 + r;
             // the item's row exponents, posted ahead by the epilogue warps
-            if (!mbar_wait_or(&expready[it & 1], (uint32_t)(it >> 1) & 1, &failed)) {
+            // (every decision below is warp-uniform: the loop has a
+            // __syncwarp)
+            const bool eok = mbar_wait_or(&expready[it & 1], (uint32_t)(it >> 1) & 1, &failed);
+            if (!__all_sync(0xffffffffu, eok ? 1 : 0)) {
                 fail_tile = tile;
                 failed = 1;
                 break;
@@ -338,7 +253,7 @@ k_sketch_i8(const __grid_constant__ CUtensorMap dmap,
                 bool ok = mbar_wait_or(&full[sg], (uint32_t)(gc / kStages) & 1, &failed);
                 ok = ok && (gc < kAbufs ||
                             mbar_wait_or(&afree[b], (uint32_t)((gc >> 1) - 1) & 1, &failed));
-                if (!ok) {
+                if (!__all_sync(0xffffffffu, ok ? 1 : 0)) {
                     fail_tile = tile;
                     failed = 1;
                     break;
@@ -361,8 +276,11 @@ k_sketch_i8(const __grid_constant__ CUtensorMap dmap,
                                                (qd >> 1) * 2048 + (r >> 3) * 128 +
                                                (r & 7) * 16 + (qd & 1) * 8) =
                         make_uint2(dg[s][0], dg[s][1]);
+                // each thread's digits visible to the tensor cores, then
+                // one arrival per warp
                 asm volatile("fence.proxy.async.shared::cta;");
-                mbar_arrive(&afull[b]);
+                __syncwarp();
+                if ((t & 31) == 0) mbar_arrive(&afull[b]);
             }
             if (failed) break;
             ++it;
@@ -380,7 +298,7 @@ k_sketch_i8(const __grid_constant__ CUtensorMap dmap,
                 if (item + gridDim.x < nitems)
                     wn = sk_item(tiles, (int)((item + gridDim.x) / rpt));
                 const int row0 = (int)(item % rpt) * kSkRows;
-                if (w.bcur <= 0 || row0 >= w.m) continue;
+                if (!sk_active(w, need) || row0 >= w.m) continue;
                 const int nchunks = (w.n + kSkChunk - 1) / kSkChunk;
                 for (int kc = 0; kc < nchunks; ++kc, ++gc) {
                     const int sg = (int)(gc % kStages);
@@ -421,7 +339,7 @@ k_sketch_i8(const __grid_constant__ CUtensorMap dmap,
                 if (item + gridDim.x < nitems)
                     wn = sk_item(tiles, (int)((item + gridDim.x) / rpt));
                 const int row0 = (int)(item % rpt) * kSkRows;
-                if (w.bcur <= 0 || row0 >= w.m) continue;
+                if (!sk_active(w, need) || row0 >= w.m) continue;
                 const int nchunks = (w.n + kSkChunk - 1) / kSkChunk;
                 // the previous item's accumulators have been read out
                 bool ok = it == 0 || mbar_wait_or(&accempty, (uint32_t)(it - 1) & 1, &failed);
@@ -472,7 +390,7 @@ k_sketch_i8(const __grid_constant__ CUtensorMap dmap,
         // (it + 1) & 1 last served item it - 1, whose conversion is over
         // once its accumulators were full.
         auto valid = [&](const SkItem &w, long long item) {
-            return w.bcur > 0 && (int)(item % rpt) * kSkRows < w.m;
+            return sk_active(w, need) && (int)(item % rpt) * kSkRows < w.m;
         };
         auto next_valid = [&](long long item, SkItem &w) {
             for (; item < nitems; item += gridDim.x) {
@@ -497,8 +415,11 @@ k_sketch_i8(const __grid_constant__ CUtensorMap dmap,
             const int row0 = (int)(item % rpt) * kSkRows;
             const int i = row0 + rr;
             const int e = rowexp[it & 1][rr];
-            if (!mbar_wait_or(&accfull, (uint32_t)it & 1, &failed)) {
-                fail_tile = tile;
+            // the TMEM loads below are warp-collective: every lane goes on
+            // or every lane stops
+            const bool ok = mbar_wait_or(&accfull, (uint32_t)it & 1, &failed);
+            if (!__all_sync(0xffffffffu, ok ? 1 : 0)) {
+                if (lane == 0) fail_tile = tile;
                 failed = 1;
                 break;
             }
@@ -554,7 +475,7 @@ bool sketch_i8_fits(int nc, int n_max)
            sketch_i8_smem() <= 227 * 1024;
 }
 
-static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
 {
     static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
     if (encode == nullptr) {
@@ -592,8 +513,8 @@ static bool d_tensor_map(CUtensorMap *map, const Workspace &ws, int nslots)
 
 // Tensor map of Omega8 (ld_om8 rows k, om8_cols columns c, column-major
 // bytes) with a 16 x nc box: columns past om8_cols read as zero.
-static bool om_tensor_map(CUtensorMap *map, const int8_t *om8, int ld_om8,
-                          int om8_cols, int nc)
+bool i8_colmajor_map(CUtensorMap *map, const int8_t *om8, int ld_om8,
+                     int om8_cols, int nc)
 {
     auto encode = tensor_map_encoder();
     if (encode == nullptr || ld_om8 % 16 != 0 || ((uintptr_t)om8 & 15u) != 0)
@@ -610,12 +531,12 @@ static bool om_tensor_map(CUtensorMap *map, const int8_t *om8, int ld_om8,
 
 bool launch_sketch_i8(const TileWork *d_tiles, int ntiles, Workspace ws,
                       const int8_t *om8, int ld_om8, int om8_cols, int ncols,
-                      cudaStream_t stream)
+                      cudaStream_t stream, int need)
 {
     const int nc = (ncols + 15) / 16 * 16;
     CUtensorMap dmap, omap;
     if (!d_tensor_map(&dmap, ws, ntiles) ||
-        !om_tensor_map(&omap, om8, ld_om8, om8_cols, nc))
+        !i8_colmajor_map(&omap, om8, ld_om8, om8_cols, nc))
         return false;
     static int sms = 0;
     if (sms == 0) {
@@ -630,7 +551,7 @@ bool launch_sketch_i8(const TileWork *d_tiles, int ntiles, Workspace ws,
     const int grid = (int)std::min<long long>(sms, items);
     if (grid <= 0) return true;
     k_sketch_i8<<<grid, kSkThreads, sketch_i8_smem(), stream>>>(
-        dmap, omap, d_tiles, ntiles, ws, nc);
+        dmap, omap, d_tiles, ntiles, ws, nc, need);
     return true;
 }
 

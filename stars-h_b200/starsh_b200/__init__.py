@@ -128,7 +128,9 @@ class Stats(Structure):
                 ("batches", c_longlong), ("sketch_launches", c_longlong),
                 ("gen_ms", c_double), ("basis_ms", c_double),
                 ("svd_ms", c_double), ("output_ms", c_double),
-                ("sketch_bytes", c_double), ("sketch_int8", c_int)]
+                ("sketch_bytes", c_double), ("sketch_int8", c_int),
+                ("fused_ms", c_double), ("fused_launches", c_longlong),
+                ("fused_bytes", c_double), ("resketch_tiles", c_longlong)]
 
 
 class ServerStats(Structure):
@@ -216,6 +218,10 @@ def _proto(lib):
         "starsh_blrm__dfe": (c_double, [P(Blrm)]),
         "starsh_b200_kernel_register": (c_int, [c_void_p, c_int, c_double]),
         "starsh_b200_kernel_family": (c_int, [c_void_p, P(c_int)]),
+        "starsh_b200_autotune_tile": (c_int, [P(Problem), c_int, P(c_int),
+                                              P(c_int), c_double, c_int,
+                                              P(c_int), P(c_double)]),
+        "starsh_b200_autotune_clear": (None, []),
         "starsh_b200_get_stats": (c_int, [P(Stats)]),
         "starsh_b200_set_device": (c_int, [c_int]),
         "starsh_b200_dense_rsvd_noalloc": (c_int, [c_void_p, c_int, c_int,

@@ -554,6 +554,15 @@ def run_c5(args, lib, clocks):
     reqs_p = [r for r in reqs if r["t"] < 10.0]
     lat_p, status_p, st_p, wall_p = serve(lib, reqs_p, sb.ENGINE_FP64, 1, A)
     ok = all(x == 0 for x in status)
+    # the single-request floor: one request alone on an idle server (2-D
+    # square exponential, tol 1e-4), per N
+    floor = {}
+    for nf in (4096, 16384, 65536):
+        sp = [dict(seed=99, n=nf, kernel="sqexp", tol=1e-4, ndim=2, t=0.0)]
+        one = build_mixed(lib, sp, handle, tune=args.tune)
+        serve(lib, one, sb.ENGINE_MIXED, 0, A)              # warm
+        lat1, st1, _, _ = serve(lib, one, sb.ENGINE_MIXED, 0, A)
+        floor[str(one[0]["n"])] = float(lat1[0])
 
     def pct(v):
         return {"p50": float(np.percentile(v, 50)),
@@ -574,6 +583,8 @@ def run_c5(args, lib, clocks):
                    "hbm_budget_bytes": C5["budget"], "engine": "mixed, continuous batching"},
         "latency_ms": pct(lat),
         "latency_ms_N_ge_32768": pct(lat[big]) if big.any() else None,
+        "single_request_floor_ms": floor,
+        "floor_what": "one 2-D square-exponential request (tol 1e-4, 32 matvecs) alone on an idle server, by N",
         "served_rps": len(reqs) / wall, "groups": int(st.groups),
         "failed": int(st.failed),
         "peak_resident_bytes": st.peak_resident_bytes,
@@ -764,6 +775,9 @@ def precision_study(lib, wl, prob, torch, ntiles=64, seed=7):
     nt = C.nblocks
     if wl["kind"] == "coulomb":
         fn = sb.kernel_symbol(lib, "starsh_esdata_block_coulomb_potential_kernel_3d")
+    elif wl["kind"] == "spatial":
+        name = {"exp": "exp", "sqexp": "sqrexp", "matern": "matern"}[wl["kernel"]]
+        fn = sb.kernel_symbol(lib, f"starsh_ssdata_block_{name}_kernel_{wl['ndim']}d")
     else:
         fn = sb.kernel_symbol(lib, "starsh_eddata_block_sin_kernel_3d")
     gen = sb.KERNEL(fn)
@@ -968,7 +982,7 @@ def main():
                     help="c4-batch / c5-serve: block sizes from the library's "
                          "autotuner (default) or the fixed rule by N")
     ap.add_argument("--precision-study", action="store_true",
-                    help="c3-*: add the sketch precision study to the line")
+                    help="c2-* / c3-*: add the sketch precision study to the line")
     ap.add_argument("--no-cpu", action="store_true",
                     help="skip the CPU baseline leg")
     ap.add_argument("--_cpu-run", type=int, default=0, dest="cpu_run")
@@ -1226,7 +1240,7 @@ def main():
     }
     if dmml:
         line["dmml"] = dmml
-    if args.precision_study and key.startswith("c3"):
+    if args.precision_study and (key.startswith("c3") or key.startswith("c2")):
         line["precision_study"] = precision_study(lib, wl, prob, torch)
     if world == 1 and not args.no_cpu:
         n = wl.get("cpu_n")

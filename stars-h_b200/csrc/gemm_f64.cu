@@ -6,6 +6,7 @@
 // double-buffered, the next K tile is fetched into registers while the
 // current one is multiplied.  Global loads are coalesced along whichever
 // dimension is contiguous for the given transpose flag.
+#include <cstdint>
 #include "gemm_f64.cuh"
 
 namespace b200 {
@@ -157,6 +158,130 @@ k_gemm_f64(const GemmDesc *__restrict__ descs, int tiles_n)
     }
 }
 
+// A^T B with 64 x 64 CTA tiles and a three-stage cp.async pipeline: the
+// transposed products of the basis rounds (Grams and projections onto the
+// basis) have outputs of at most a few 64 x 64 tiles and K = the tile
+// height, so one CTA walks a long K; the register-staged kernel above keeps
+// one K step in flight and waits on memory latency every step.  Operand
+// tiles land in shared memory directly (16-byte cp.async, k contiguous in
+// both operands), two steps ahead of the multiply (60 KB of shared memory,
+// three CTAs per SM as for the register-staged kernel).  Same per-element
+// accumulation order as k_gemm_f64 (K steps of 16 in order, the DMMA's
+// k-order inside a step), so results are identical to it.
+constexpr int kTnStages = 3;
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, bool pred)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    const int n = pred ? 16 : 0;   // zero-fill when outside the operand
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;"
+                 :: "r"(sa), "l"(gmem), "r"(n));
+}
+
+__global__ void __launch_bounds__(kGemmThreads)
+k_gemm_f64_tn_pipe(const GemmDesc *__restrict__ descs, int tiles_n)
+{
+    constexpr int BM = 64, BN = 64;
+    const GemmDesc d = descs[blockIdx.y];
+    const int tm = blockIdx.x / tiles_n, tn = blockIdx.x % tiles_n;
+    const int m0 = tm * BM, n0 = tn * BN;
+    if (m0 >= d.M || n0 >= d.N) return;
+    extern __shared__ double gemm_smem[];
+    // [stage][64 rows][kGemmLds] for A^T, then the same for B^T
+    double *As = gemm_smem;
+    double *Bs = gemm_smem + kTnStages * BM * kGemmLds;
+    const int t = threadIdx.x;
+    const int lane = t & 31, warp = t >> 5;
+    const int g = lane >> 2, tig = lane & 3;
+    const int wm = (warp % 2) * 32, wn = (warp / 2) * 16;
+    double acc[4][2][2];
+    #pragma unroll
+    for (int i = 0; i < 4; ++i)
+        #pragma unroll
+        for (int j = 0; j < 2; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+    // each operand tile is 64 rows x 16 k = 512 16-byte pieces: thread t
+    // copies pieces t and t + 256 of each (row = piece / 8, k pair = piece % 8)
+    const bool evenA = (d.lda & 1) == 0 && ((uintptr_t)d.A & 15) == 0;
+    const bool evenB = (d.ldb & 1) == 0 && ((uintptr_t)d.B & 15) == 0;
+    auto issue = [&](int kt) {
+        const int st = kt % kTnStages, k0 = kt * kGemmBK;
+        #pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            const int piece = t + kGemmThreads * r;
+            const int row = piece >> 3, kk = (piece & 7) * 2;
+            {
+                const int gm = m0 + row, gk = k0 + kk;
+                double *dst = As + (st * BM + row) * kGemmLds + kk;
+                if (evenA && gm < d.M && gk + 1 < d.K) {
+                    cp_async16(dst, d.A + (size_t)gm * d.lda + gk, true);
+                } else {
+                    dst[0] = (gm < d.M && gk < d.K) ? d.A[(size_t)gm * d.lda + gk] : 0.0;
+                    dst[1] = (gm < d.M && gk + 1 < d.K) ? d.A[(size_t)gm * d.lda + gk + 1] : 0.0;
+                }
+            }
+            {
+                const int gn = n0 + row, gk = k0 + kk;
+                double *dst = Bs + (st * BN + row) * kGemmLds + kk;
+                if (evenB && gn < d.N && gk + 1 < d.K) {
+                    cp_async16(dst, d.B + (size_t)gn * d.ldb + gk, true);
+                } else {
+                    dst[0] = (gn < d.N && gk < d.K) ? d.B[(size_t)gn * d.ldb + gk] : 0.0;
+                    dst[1] = (gn < d.N && gk + 1 < d.K) ? d.B[(size_t)gn * d.ldb + gk + 1] : 0.0;
+                }
+            }
+        }
+        asm volatile("cp.async.commit_group;");
+    };
+    const int ktiles = (d.K + kGemmBK - 1) / kGemmBK;
+    #pragma unroll
+    for (int p = 0; p < kTnStages - 1; ++p) {
+        if (p < ktiles) issue(p);
+        else asm volatile("cp.async.commit_group;");
+    }
+    for (int kt = 0; kt < ktiles; ++kt) {
+        // the group of step kt has landed (at most kTnStages - 2 newer ones
+        // still in flight)
+        asm volatile("cp.async.wait_group %0;" :: "n"(kTnStages - 2));
+        __syncthreads();
+        if (kt + kTnStages - 1 < ktiles) issue(kt + kTnStages - 1);
+        else asm volatile("cp.async.commit_group;");
+        const int st = kt % kTnStages;
+        const double *Ab = As + st * BM * kGemmLds;
+        const double *Bb = Bs + st * BN * kGemmLds;
+        #pragma unroll
+        for (int kk = 0; kk < kGemmBK; kk += 4) {
+            double af[4], bf[2];
+            #pragma unroll
+            for (int i = 0; i < 4; ++i) af[i] = Ab[(wm + i * 8 + g) * kGemmLds + kk + tig];
+            #pragma unroll
+            for (int j = 0; j < 2; ++j) bf[j] = Bb[(wn + j * 8 + g) * kGemmLds + kk + tig];
+            #pragma unroll
+            for (int i = 0; i < 4; ++i)
+                #pragma unroll
+                for (int j = 0; j < 2; ++j)
+                    dmma_8x8x4(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+        }
+    }
+    asm volatile("cp.async.wait_group 0;");
+    #pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int gm = m0 + wm + i * 8 + g;
+        if (gm >= d.M) continue;
+        #pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            #pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int gn = n0 + wn + j * 8 + 2 * tig + h;
+                if (gn >= d.N) continue;
+                double *c = d.C + (size_t)gn * d.ldc + gm;
+                double v = d.alpha * acc[i][j][h];
+                if (d.beta != 0.0) v += d.beta * *c;
+                *c = v;
+            }
+        }
+    }
+}
+
 template <int BM, int BN>
 static void launch_shape(bool ta, bool tb, const GemmDesc *dd, int nb,
                          int tiles_m, int tiles_n, cudaStream_t stream)
@@ -189,10 +314,23 @@ cudaError_t gemm_f64_batched(bool ta, bool tb, const GemmDesc *d_desc,
     else if (max_n <= 32 && max_m >= 128) { bm = 128; bn = 32; }
     const int tiles_m = (max_m + bm - 1) / bm;
     const int tiles_n = (max_n + bn - 1) / bn;
+    // transposed products with 64 x 64 tiles: the pipelined kernel
+    const bool pipe = ta && !tb && bm == 64 && bn == 64;
     for (int b0 = 0; b0 < batch; b0 += 65535) {
         const int nb = batch - b0 < 65535 ? batch - b0 : 65535;
         const GemmDesc *dd = d_desc + b0;
-        if (bm == 32) launch_shape<32, 128>(ta, tb, dd, nb, tiles_m, tiles_n, stream);
+        if (pipe) {
+            const size_t smem = (size_t)kTnStages * 2 * 64 * kGemmLds * sizeof(double);
+            static bool attr = false;
+            if (!attr) {
+                cudaFuncSetAttribute(k_gemm_f64_tn_pipe,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem);
+                attr = true;
+            }
+            dim3 grid(tiles_m * tiles_n, nb);
+            k_gemm_f64_tn_pipe<<<grid, kGemmThreads, smem, stream>>>(dd, tiles_n);
+        } else if (bm == 32) launch_shape<32, 128>(ta, tb, dd, nb, tiles_m, tiles_n, stream);
         else if (bm == 128) launch_shape<128, 32>(ta, tb, dd, nb, tiles_m, tiles_n, stream);
         else launch_shape<64, 64>(ta, tb, dd, nb, tiles_m, tiles_n, stream);
     }

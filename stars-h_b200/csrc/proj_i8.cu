@@ -1,43 +1,47 @@
 // Projection B = Q^T D of the adaptive engine on the tcgen05 tensor cores,
 // FP64-accurate through integer slices (the integer Ozaki scheme of
 // sketch_i8.cu); replaces the FP64 GEMM of the reference's
-// src/backends/sequential/dense/drsdd.c:69-70 for tiles with at most 64
+// src/backends/sequential/dense/drsdd.c:69-70 for tiles with at most 32
 // basis columns.
 //
 // Scaling.  The contraction runs over the tile rows i.  Row i of D is
 // scaled by 2^-e_i (e_i the exponent of its exact largest |D_ij|, from the
 // generator), x_ij = D_ij 2^-e_i in (-1, 1), and the factor moves to Q:
 // Q'_ic = Q_ic 2^e_i, so that B_cj = sum_i Q'_ic x_ij.  x is rounded to a
-// 56-bit integer (seven bytes, the top one signed) and Q' column c, scaled
-// by 2^-f_c (f_c the exponent of its largest entry), likewise:
+// 56-bit integer (seven bytes: six unsigned, the top one signed) and Q'
+// column c, scaled by 2^-f_c (f_c the exponent of its largest entry), to
+// a 54-bit integer in balanced base-256 digits (seven signed bytes):
 //     x_ij = 2^-55 sum_{s<7} 256^s a_s(i, j),
-//     Q'_ic = 2^(f_c - 55) sum_{t<7} 256^t b_t(i, c),
-// with a_6, b_6 signed and the others unsigned bytes.  Each a_s b_t is an
-// exact int8 x int8 -> int32 product (tcgen05.mma kind::i8); the products
-// of equal weight w = s + t share one TMEM accumulator, and only w >= 5 is
-// kept (the dropped terms are below 2^-59 of the largest product).  The
-// epilogue combines the eight accumulators in two exact int64 words and
-// converts once:
-//     B_cj = 2^(f_c - 70) (2^32 H + L),  H = sum_{w>=9} 256^(w-9) P_w,
+//     Q'_ic = 2^(f_c - 54) sum_{t<7} 256^t b_t(i, c).
+// Each a_s b_t is an exact int8 x int8 -> int32 product (tcgen05.mma
+// kind::i8); the products of equal weight w = s + t share one TMEM
+// accumulator block and only w >= 5 is kept (the dropped terms are below
+// 2^-57 of the largest product).  With the basis slices stacked in shared
+// memory between zero blocks, one MMA per D slice (N = 256) feeds all
+// eight weight blocks: seven MMAs per 32-row chunk.  The epilogue combines
+// the eight accumulators in two exact int64 words and converts once:
+//     B_cj = 2^(f_c - 69) (2^32 H + L),  H = sum_{w>=9} 256^(w-9) P_w,
 //                                        L = sum_{w<=8} 256^(w-5) P_w.
 // The representation error is 2^-56 of each row's largest entry of D and
-// of Q' column's largest entry: the level of the FP64 product it replaces.
-// Accumulators stay below 2^31 for m <= 4096 (seven products of weight w
-// per K step, each below 2^16); the kernel takes tiles of up to 2048 rows.
+// 2^-55 of each Q' column's largest entry: the level of the FP64 product
+// it replaces.  Accumulators stay below 2^31 for m <= 4096 (seven products
+// of weight w per K step, each below 2^15 in magnitude); the kernel takes
+// tiles of up to 2048 rows.
 //
-// k_proj_prep (one CTA per tile) computes e_i, f_c and the seven byte
-// slices of Q' (rows c < 64, zero beyond k1) into the slot's workspace and
+// k_proj_prep (one CTA per tile) computes e_i, f_c and the seven digit
+// slices of Q' (32 columns, zero beyond k1) into the slot's workspace and
 // flags the tile TILE_PROJ_I8; the FP64 projection skips flagged tiles.
 //
 // k_proj_i8 is persistent and warp-specialized like the sketch kernels:
-// one warp streams, per 32-row chunk of an item (tile, 128-column block),
-// the 32 x 128 FP64 block of D (two 128B-swizzled TMA boxes) into a
-// four-stage ring that the converters free as soon as they hold the values,
-// and the chunk's 14 KB of Q' slices (one bulk copy) into a two-stage ring
-// that the MMAs free; 16 converter warps write the seven digit slices of x
-// (each thread 8 rows of one column); one warp issues the 34 MMAs of the
-// chunk; four epilogue warps read the accumulators and write B.  Every wait is bounded; after a
-// timeout the tile is marked TILE_MMA_TIMEOUT and the call fails.
+// per 32-row chunk of an item (tile, 128-column block), one producer lane
+// streams the 32 x 128 FP64 block of D (two 128B-swizzled TMA boxes) into
+// a three-stage ring that the converters free as soon as they hold the
+// values, another the chunk's 7 KB of basis slices (two bulk copies) into
+// the stacks of a two-stage ring that the MMAs free; 16 converter warps
+// write the seven digit slices of x (each thread 8 rows of one column);
+// one warp issues the chunk's seven MMAs; four epilogue warps read the
+// accumulators and write B.  Every wait is bounded; after a timeout the
+// tile is marked TILE_MMA_TIMEOUT and the call fails.
 #include <algorithm>
 #include <cfloat>
 #include <cstdint>
@@ -49,10 +53,19 @@ namespace b200 {
 constexpr int kPjSlices = 7;
 constexpr int kPjCols = 128;          // columns of D per item (MMA M)
 constexpr int kPjChunk = 32;          // rows of D per chunk (MMA K)
-constexpr int kPjN = 64;              // basis columns (MMA N, padded)
+constexpr int kPjN = 32;              // basis columns per weight block
 constexpr int kPjMinW = 5;            // weights kept: 5 .. 12
 constexpr int kPjAcc = 2 * (kPjSlices - 1) - kPjMinW + 1;   // 8
-constexpr int kPjDStages = 4;         // D chunks in flight
+// The basis slices sit in shared memory as one stack of kPjBlocks blocks
+// of kPjN rows (per 16-byte K half, a "plane"): blocks 7 .. 13 hold slices
+// t = 0 .. 6, the others are zero.  The eight consecutive blocks starting
+// at block 12 - s are the B operand of D slice s: block w - 5 of that
+// window is slice w - s (zero outside 0 .. 6), so one MMA (N = 8 kPjN =
+// 256) adds a_s b_(w-s) into the accumulator of every weight w = 5 .. 12.
+constexpr int kPjBlocks = 20;
+constexpr int kPjPlane = kPjBlocks * kPjN * 16;                      // 10 KB
+constexpr int kPjQData = kPjSlices * kPjN * 16;                      // 3.5 KB
+constexpr int kPjDStages = 3;         // D chunks in flight
 constexpr int kPjQStages = 2;         // Q' chunks in flight
 constexpr int kPjConvThreads = 512;
 constexpr int kPjProducerWarp = 16;
@@ -62,12 +75,13 @@ constexpr int kPjThreads = 22 * 32;
 constexpr int kPjMaxRows = 2048;
 constexpr int kPjAbufBytes = kPjSlices * kPjCols * kPjChunk;          // 28 KB
 constexpr int kPjDBytes = kPjChunk * kPjCols * (int)sizeof(double);  // 32 KB
-constexpr int kPjQBytes = kPjSlices * 2 * kPjN * 16;                 // 14 KB
+constexpr int kPjQBytes = 2 * kPjQData;          // one chunk in global, 7 KB
+constexpr int kPjQStage = 2 * kPjPlane;          // one chunk's stack, 20 KB
 constexpr size_t kPjSmemBytes = (size_t)kPjDStages * kPjDBytes +
-                                (size_t)kPjQStages * kPjQBytes +
+                                (size_t)kPjQStages * kPjQStage +
                                 (size_t)2 * kPjAbufBytes + 1024;
 
-static_assert(kPjAcc * kPjN <= 512, "TMEM columns");
+static_assert(kPjAcc * kPjN <= 256, "TMEM columns");
 
 __host__ __device__ constexpr uint32_t idesc_i8_ab(int m, int n, bool a_signed,
                                                    bool b_signed)
@@ -139,10 +153,12 @@ k_proj_prep(TileWork *__restrict__ tiles, Workspace ws)
     for (int c = threadIdx.x; c < kPjN; c += blockDim.x)
         fe[c] = c < k1 && fmaxe[c] != INT32_MIN ? fmaxe[c] : 0;
     __syncthreads();
-    // slices, chunk-major (one bulk copy per 32-row chunk of the
-    // projection): byte (s, c, i) at ((i / 32 * 7 + s) * 2 + i % 32 / 16)
-    // * 1024 + c * 16 + i % 16; a thread writes one 16-byte row (c, 16 i)
-    // of every slice; rows c >= k1 and i >= m are zero
+    // slices in balanced base-256 digits (every byte signed, so one MMA
+    // can take all seven), chunk-major: per 32-row chunk, K half h, slice
+    // t, basis column c < 32, 16 bytes of rows i; byte (t, c, i) at
+    // i / 32 * kPjQBytes + (i % 32 / 16) * kPjQData + t * 512 + c * 16 +
+    // i % 16.  A thread writes one 16-byte row (c, 16 i) of every slice;
+    // columns c >= k1 and rows i >= m are zero.
     uint8_t *qd = ws.Qd(s);
     const int halves = ldq / 16;
     for (int e = threadIdx.x; e < kPjN * halves; e += blockDim.x) {
@@ -151,32 +167,34 @@ k_proj_prep(TileWork *__restrict__ tiles, Workspace ws)
         #pragma unroll
         for (int t = 0; t < kPjSlices; ++t)
             w[t][0] = w[t][1] = w[t][2] = w[t][3] = 0u;
-        const int fc = fmaxe[c] != INT32_MIN ? fmaxe[c] : 0;
+        const int fc = c < k1 && fmaxe[c] != INT32_MIN ? fmaxe[c] : 0;
         #pragma unroll
         for (int u = 0; u < 16; ++u) {
             const int i = i0 + u;
-            uint32_t lo = 0u, hi = 0u;
             if (c < k1 && i < m) {
                 const double q = Q[(size_t)c * ldm + i];
-                // X = Q_ic 2^(e_i - f_c + 55), |X| < 2^55, in exact steps
-                const int sh = re[i] - fc + 55;
+                // X = Q_ic 2^(e_i - f_c + 54), |X| < 2^54, in exact steps
+                const int sh = re[i] - fc + 54;
                 double X = q;
                 if (sh > 1000) X = ldexp(ldexp(X, 1000), sh - 1000);
                 else if (sh < -1000) X = ldexp(ldexp(X, -1000), sh + 1000);
                 else X = ldexp(X, sh);
+                uint32_t lo, hi;
                 bytes56(X, lo, hi);
+                long long v = ((long long)(int)hi << 32) | (long long)lo;
+                #pragma unroll
+                for (int t = 0; t < kPjSlices; ++t) {
+                    const int d = (int)(int8_t)(v & 0xFF);   // in [-128, 127]
+                    v = (v - d) >> 8;
+                    w[t][u >> 2] |= ((uint32_t)d & 0xFFu) << (8 * (u & 3));
+                }
             }
-            #pragma unroll
-            for (int t = 0; t < 4; ++t)
-                w[t][u >> 2] |= ((lo >> (8 * t)) & 0xFFu) << (8 * (u & 3));
-            #pragma unroll
-            for (int t = 0; t < 3; ++t)
-                w[4 + t][u >> 2] |= ((hi >> (8 * t)) & 0xFFu) << (8 * (u & 3));
         }
         #pragma unroll
         for (int t = 0; t < kPjSlices; ++t)
-            *reinterpret_cast<uint4 *>(qd + ((size_t)((hh >> 1) * kPjSlices + t) * 2 + (hh & 1)) * 1024 +
-                                       c * 16) = make_uint4(w[t][0], w[t][1], w[t][2], w[t][3]);
+            *reinterpret_cast<uint4 *>(qd + (size_t)(hh >> 1) * kPjQBytes +
+                                       (hh & 1) * kPjQData + t * (kPjN * 16) + c * 16) =
+                make_uint4(w[t][0], w[t][1], w[t][2], w[t][3]);
     }
     if (threadIdx.x == 0) tw.status |= TILE_PROJ_I8;
 }
@@ -213,9 +231,9 @@ k_proj_i8(const __grid_constant__ CUtensorMap dmap,
     __shared__ volatile int failed;
 
     uint8_t *base = pj_smem_raw + ((1024u - (smem_u32(pj_smem_raw) & 1023u)) & 1023u);
-    uint8_t *Dst = base;                                            // [4][32 KB]
-    uint8_t *Qst = base + (size_t)kPjDStages * kPjDBytes;           // [2][14 KB]
-    uint8_t *Abuf = Qst + (size_t)kPjQStages * kPjQBytes;           // [2][28 KB]
+    uint8_t *Dst = base;                                            // [3][32 KB]
+    uint8_t *Qst = base + (size_t)kPjDStages * kPjDBytes;           // [2][20 KB]
+    uint8_t *Abuf = Qst + (size_t)kPjQStages * kPjQStage;           // [2][28 KB]
 
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
     const int cpt = (ws.n_max + kPjCols - 1) / kPjCols;    // items per tile
@@ -241,9 +259,13 @@ k_proj_i8(const __grid_constant__ CUtensorMap dmap,
         mbar_init(&accempty, kPjCols);
         asm volatile("fence.mbarrier_init.release.cluster;");
     }
+    // the zero blocks of the basis stacks (the copies fill blocks 7 .. 13)
+    for (int q = t; q < kPjQStages * kPjQStage / 16; q += kPjThreads)
+        reinterpret_cast<uint4 *>(Qst)[q] = make_uint4(0u, 0u, 0u, 0u);
+    asm volatile("fence.proxy.async.shared::cta;");
     if (warp == kPjMmaWarp) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
-                     :: "r"(smem_u32(&tmem_base)), "r"(512));
+                     :: "r"(smem_u32(&tmem_base)), "r"(256));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     tc_fence_before();
@@ -401,11 +423,13 @@ k_proj_i8(const __grid_constant__ CUtensorMap dmap,
                         tma_load_3d(st + kPjCols * 128, &dmap, kc * kPjChunk + 16, j0,
                                     w.slot, &fullb[sg]);
                     } else {
-                        // the chunk's Q' slices: one contiguous 14 KB block
+                        // the chunk's basis slices, per K half one 3.5 KB
+                        // copy into blocks 7 .. 13 of that half's plane
                         mbar_expect_tx(&fullb[sg], kPjQBytes);
-                        bulk_load(Qst + (size_t)sg * kPjQBytes,
-                                  ws.Qd(w.slot) + (size_t)kc * kPjQBytes, kPjQBytes,
-                                  &fullb[sg]);
+                        const uint8_t *src = ws.Qd(w.slot) + (size_t)kc * kPjQBytes;
+                        uint8_t *dst = Qst + (size_t)sg * kPjQStage + 7 * kPjN * 16;
+                        bulk_load(dst, src, kPjQData, &fullb[sg]);
+                        bulk_load(dst + kPjPlane, src + kPjQData, kPjQData, &fullb[sg]);
                     }
                     issued = gc + 1;
                 }
@@ -430,7 +454,6 @@ k_proj_i8(const __grid_constant__ CUtensorMap dmap,
                 if (!item_valid(item, w)) continue;
                 const int tile = (int)(item / cpt);
                 const int nch = (w.m + kPjChunk - 1) / kPjChunk;
-                const int nn = (w.k1 + 15) / 16 * 16;
                 ok = it == 0 || mbar_wait_sleep(&accempty, (uint32_t)(it - 1) & 1, &failed, 32);
                 for (int kc = 0; ok && kc < nch; ++kc, ++gc) {
                     const int sq = (int)(gc % kPjQStages), b = (int)(gc & 1);
@@ -441,27 +464,18 @@ k_proj_i8(const __grid_constant__ CUtensorMap dmap,
                     }
                     tc_fence_after();
                     const uint8_t *A = Abuf + b * kPjAbufBytes;
-                    const uint8_t *qs = Qst + (size_t)sq * kPjQBytes;
+                    const uint8_t *qs = Qst + (size_t)sq * kPjQStage;
                     #pragma unroll
-                    for (int s = 0; s < kPjSlices; ++s) {
-                        const uint64_t da = umma_desc(smem_u32(A + s * (kPjCols * kPjChunk)),
+                    for (int sl = 0; sl < kPjSlices; ++sl) {
+                        const uint64_t da = umma_desc(smem_u32(A + sl * (kPjCols * kPjChunk)),
                                                       2048, 128);
-                        #pragma unroll
-                        for (int tq = 0; tq < kPjSlices; ++tq) {
-                            const int wgt = s + tq;
-                            if (wgt < kPjMinW) continue;
-                            const uint64_t db = umma_desc(
-                                smem_u32(qs + (2 * tq) * kPjN * 16), kPjN * 16, 128);
-                            // the first product of each weight in an item
-                            // (the smallest s, in this loop order) starts
-                            // its accumulator
-                            const bool first = kc == 0 &&
-                                s == (wgt > kPjSlices - 1 ? wgt - (kPjSlices - 1) : 0);
-                            mma_i8(tmem + (wgt - kPjMinW) * kPjN, da, db,
-                                   idesc_i8_ab(kPjCols, nn, s == kPjSlices - 1,
-                                               tq == kPjSlices - 1),
-                                   first ? 0 : 1);
-                        }
+                        // window of blocks 12 - sl .. 19 - sl: block w - 5
+                        // holds slice w - sl
+                        const uint64_t db = umma_desc(
+                            smem_u32(qs + (12 - sl) * kPjN * 16), kPjPlane, 128);
+                        mma_i8(tmem, da, db,
+                               idesc_i8_ab(kPjCols, kPjAcc * kPjN, sl == kPjSlices - 1, true),
+                               kc == 0 && sl == 0 ? 0 : 1);
                     }
                     mma_commit(&qempty[sq]);
                     mma_commit(&afree[b]);
@@ -518,7 +532,7 @@ k_proj_i8(const __grid_constant__ CUtensorMap dmap,
                         #pragma unroll
                         for (int a = 3; a >= 0; --a) L = L * 256 + (long long)(int)v[a][c8];
                         const double T = fma((double)H, 0x1p32, (double)L);
-                        Bm[(size_t)jj * ldk + c] = ldexp(T, fe[c] - 70);
+                        Bm[(size_t)jj * ldk + c] = ldexp(T, fe[c] - 69);
                     }
                 }
             }
@@ -534,7 +548,7 @@ k_proj_i8(const __grid_constant__ CUtensorMap dmap,
     if (fail_tile >= 0) atomicOr(&tiles[fail_tile].status, TILE_MMA_TIMEOUT);
     if (warp == kPjMmaWarp)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
-                     :: "r"(tmem), "r"(512));
+                     :: "r"(tmem), "r"(256));
 }
 
 void launch_proj_prep(TileWork *d_tiles, int ntiles, Workspace ws,

@@ -59,6 +59,15 @@ int starsh_blrm__dmml_b200(STARSH_blrm *matrix, int nrhs, double alpha,
  * (reference src/backends/sequential/blrm/dfe.c:16-134).  -1 on error. */
 double starsh_blrm__dfe_b200(STARSH_blrm *matrix);
 
+/* The two sums behind dfe: *diff2 = sum over far blocks of
+ * ||D_b - U_b V_b^T||_F^2 and *norm2 = sum over all blocks of ||D_b||_F^2
+ * (sqrt(2) weights of symmetric formats applied), so that a matrix split
+ * over processes has dfe = sqrt(sum diff2 / sum norm2) after one sum
+ * all-reduce of two doubles -- what the reference's MPI backend reduces
+ * (src/backends/mpi/blrm/dfe.c:140-149). */
+int starsh_b200_blrm_dfe_sums(STARSH_blrm *matrix, double *diff2,
+        double *norm2);
+
 /* ---------------------------------------------- device-resident results */
 
 /* Engine selectors for starsh_b200_approximate(). */

@@ -463,16 +463,20 @@ __global__ void k_dfe_sum(const double *__restrict__ part, int nslot,
     out[2 * j + 1] = b;
 }
 
-static double dfe_device(STARSH_blrm *M, Context &ctx)
+// The weighted sums sum ||D_b - U_b V_b^T||_F^2 (far blocks) and
+// sum ||D_b||_F^2 (all blocks) of M; returns STARSH_SUCCESS or an error.
+static int dfe_sums_device(STARSH_blrm *M, Context &ctx, double *diff2,
+                           double *norm2)
 {
+    *diff2 = *norm2 = 0.0;
     Record *rec = nullptr;
-    if (ensure_record(M, ctx, &rec)) return -1.0;
+    if (ensure_record(M, ctx, &rec)) return STARSH_UNKNOWN_ERROR;
     STARSH_blrf *F = M->format;
     STARSH_cluster *R = F->row_cluster, *C = F->col_cluster;
     cudaStream_t s = ctx.stream;
     const STARSH_int nf = F->nblocks_far, nn = F->nblocks_near;
     const size_t njobs = nf + nn;
-    if (njobs == 0) return 0.0;
+    if (njobs == 0) return STARSH_SUCCESS;
     std::vector<DfeJob> jobs(njobs);
     int mmax = 0, nmax = 0;
     for (STARSH_int b = 0; b < nf; ++b) {
@@ -500,8 +504,7 @@ static double dfe_device(STARSH_blrm *M, Context &ctx)
         pool_free(sums);
         pool_free(part);
         pool_free(dj);
-        cuda_fail(cudaErrorMemoryAllocation, "dfe buffers");
-        return -1.0;
+        return cuda_fail(cudaErrorMemoryAllocation, "dfe buffers");
     }
     cudaMemcpyAsync(dj, jobs.data(), njobs * sizeof(DfeJob),
                     cudaMemcpyHostToDevice, s);
@@ -522,10 +525,7 @@ static double dfe_device(STARSH_blrm *M, Context &ctx)
     pool_free(part);
     pool_free(dj);
     cudaError_t e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) {
-        cuda_fail(e, "dfe kernels");
-        return -1.0;
-    }
+    if (e != cudaSuccess) return cuda_fail(e, "dfe kernels");
     double diff = 0.0, norm = 0.0;
     const bool symm = F->symm == 'S';
     for (STARSH_int b = 0; b < nf; ++b) {
@@ -537,6 +537,15 @@ static double dfe_device(STARSH_blrm *M, Context &ctx)
         const double w = (symm && F->block_near[2 * b] != F->block_near[2 * b + 1]) ? 2.0 : 1.0;
         norm += w * h[2 * (nf + b)];
     }
+    *diff2 = diff;
+    *norm2 = norm;
+    return STARSH_SUCCESS;
+}
+
+static double dfe_device(STARSH_blrm *M, Context &ctx)
+{
+    double diff = 0.0, norm = 0.0;
+    if (dfe_sums_device(M, ctx, &diff, &norm) != STARSH_SUCCESS) return -1.0;
     return norm > 0.0 ? sqrt(diff) / sqrt(norm) : 0.0;
 }
 
@@ -611,4 +620,15 @@ extern "C" double starsh_blrm__dfe_b200(STARSH_blrm *matrix)
 extern "C" double starsh_blrm__dfe(STARSH_blrm *matrix)
 {
     return starsh_blrm__dfe_b200(matrix);
+}
+
+extern "C" int starsh_b200_blrm_dfe_sums(STARSH_blrm *matrix, double *diff2,
+                                         double *norm2)
+{
+    if (matrix == nullptr || diff2 == nullptr || norm2 == nullptr)
+        return STARSH_WRONG_PARAMETER;
+    Context *ctx = context();
+    if (!ctx) return STARSH_UNKNOWN_ERROR;
+    std::lock_guard<std::mutex> guard(ctx->lock);
+    return dfe_sums_device(matrix, *ctx, diff2, norm2);
 }

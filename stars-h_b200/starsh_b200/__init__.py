@@ -215,6 +215,8 @@ def _proto(lib):
         "starsh_blrm__dmml": (c_int, [P(Blrm), c_int, c_double, P(c_double),
                                       c_int, c_double, P(c_double), c_int]),
         "starsh_blrm__dfe_b200": (c_double, [P(Blrm)]),
+        "starsh_b200_blrm_dfe_sums": (c_int, [P(Blrm), P(c_double),
+                                              P(c_double)]),
         "starsh_blrm__dfe": (c_double, [P(Blrm)]),
         "starsh_b200_kernel_register": (c_int, [c_void_p, c_int, c_double]),
         "starsh_b200_kernel_family": (c_int, [c_void_p, P(c_int)]),

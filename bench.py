@@ -577,7 +577,8 @@ def run_c5(args, lib, clocks):
         "dtype": "f64", "data": "synthetic (seeded point generators)",
         "config": {"workload": f"serving-poisson-{rate:g}rps-{seconds:g}s",
                    "requests": len(reqs), "offered_rate_rps": rate,
-                   "workers": int(os.environ.get("STARSH_B200_SERVER_WORKERS", "2")),
+                   "workers": int(os.environ.get("STARSH_B200_SERVER_WORKERS", "3")),
+                   "group_entries_cap": float(os.environ.get("STARSH_B200_SERVER_GROUP_ENTRIES", "5e8")),
                    "N": "lognormal median 8192, sigma_log 0.5, clipped [2048, 65536]",
                    "tols": list(C5["tols"]), "nrhs": C5["nrhs"],
                    "hbm_budget_bytes": C5["budget"], "engine": "mixed, continuous batching"},

@@ -243,12 +243,14 @@ int starsh_b200_dense_rsvd_noalloc(const double *dD, int nrows, int ncols,
 
 /* A serving loop: approximation requests are admitted by an HBM budget and
  * run in shared batches, then each request's TLR-by-dense product runs on
- * the resident factors.  Continuous batching: worker threads (2 by
+ * the resident factors.  Continuous batching: worker threads (3 by
  * default, STARSH_B200_SERVER_WORKERS up to 8), each with its own CUDA
  * streams and buffers, take the next group whenever they are free, so
- * requests that arrive while a group is on the GPU are admitted by the
- * other worker as memory allows and the two groups' kernels overlap on the
- * device.  All calls are thread-safe. */
+ * requests that arrive while groups are on the GPU are admitted by a free
+ * worker as memory allows and the groups' kernels overlap on the device.
+ * A group takes requests in FIFO order up to 5e8 matrix entries of work
+ * (STARSH_B200_SERVER_GROUP_ENTRIES; its first request always goes in).
+ * All calls are thread-safe. */
 typedef struct starsh_b200_server starsh_b200_server;
 
 typedef struct starsh_b200_server_stats

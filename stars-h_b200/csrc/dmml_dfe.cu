@@ -49,7 +49,12 @@ __device__ __forceinline__ void dmma_884(double &c0, double &c1, double a,
 }
 
 // C += alpha * sum over segments of op(A_s) B_s.  CTA tile 64 x 64, same
-// fragment mapping as the batched GEMM (8 warps, 32 x 16 per warp).
+// fragment mapping as the batched GEMM (8 warps, 32 x 16 per warp).  The
+// K steps of 16 of all the CTA's segments form one sequence; operand tiles
+// are double-buffered in shared memory and the next step (possibly of the
+// next segment) is loaded into registers while the current one is
+// multiplied.  Each output element accumulates in the same order as a
+// plain loop over segments and steps.
 __global__ void __launch_bounds__(256)
 k_gemm_seg(const SegOut *__restrict__ outs, const Seg *__restrict__ segs,
            double alpha, int tiles_n)
@@ -57,50 +62,91 @@ k_gemm_seg(const SegOut *__restrict__ outs, const Seg *__restrict__ segs,
     const SegOut o = outs[blockIdx.y];
     const int m0 = (blockIdx.x / tiles_n) * 64, n0 = (blockIdx.x % tiles_n) * 64;
     if (m0 >= o.M || n0 >= o.N || o.seg0 >= o.seg1) return;
-    __shared__ double As[64 * 20];
-    __shared__ double Bs[64 * 20];
+    __shared__ double As[2][64 * 20];
+    __shared__ double Bs[2][64 * 20];
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const int g = lane >> 2, tig = lane & 3;
     const int wm = (warp & 1) * 32, wn = (warp >> 1) * 16;
     double acc[4][2][2] = {};
-    for (int sidx = o.seg0; sidx < o.seg1; ++sidx) {
-        const Seg sg = segs[sidx];
-        for (int k0 = 0; k0 < sg.K; k0 += 16) {
-            #pragma unroll
-            for (int r = 0; r < 4; ++r) {
-                int row, kk;
-                if (!sg.transA) { row = t & 63; kk = (t >> 6) + 4 * r; }
-                else { kk = t & 15; row = (t >> 4) + 16 * r; }
-                const int gm = m0 + row, gk = k0 + kk;
-                double v = 0.0;
-                if (gm < o.M && gk < sg.K)
-                    v = sg.transA ? sg.A[(size_t)gm * sg.lda + gk]
-                                  : sg.A[(size_t)gk * sg.lda + gm];
-                As[row * 20 + kk] = v;
-            }
-            #pragma unroll
-            for (int r = 0; r < 4; ++r) {
-                const int kk = t & 15, col = (t >> 4) + 16 * r;
-                const int gn = n0 + col, gk = k0 + kk;
-                Bs[col * 20 + kk] = (gn < o.N && gk < sg.K)
-                                        ? sg.B[(size_t)gn * sg.ldb + gk] : 0.0;
-            }
-            __syncthreads();
-            #pragma unroll
-            for (int kk = 0; kk < 16; kk += 4) {
-                double af[4], bf[2];
-                #pragma unroll
-                for (int i = 0; i < 4; ++i) af[i] = As[(wm + 8 * i + g) * 20 + kk + tig];
-                #pragma unroll
-                for (int j = 0; j < 2; ++j) bf[j] = Bs[(wn + 8 * j + g) * 20 + kk + tig];
-                #pragma unroll
-                for (int i = 0; i < 4; ++i)
-                    #pragma unroll
-                    for (int j = 0; j < 2; ++j)
-                        dmma_884(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
-            }
-            __syncthreads();
+    double ra[4], rb[4];
+    auto load = [&](const Seg &sg, int k0) {
+        #pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            int row, kk;
+            if (!sg.transA) { row = t & 63; kk = (t >> 6) + 4 * r; }
+            else { kk = t & 15; row = (t >> 4) + 16 * r; }
+            const int gm = m0 + row, gk = k0 + kk;
+            double v = 0.0;
+            if (gm < o.M && gk < sg.K)
+                v = sg.transA ? sg.A[(size_t)gm * sg.lda + gk]
+                              : sg.A[(size_t)gk * sg.lda + gm];
+            ra[r] = v;
         }
+        #pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const int kk = t & 15, col = (t >> 4) + 16 * r;
+            const int gn = n0 + col, gk = k0 + kk;
+            rb[r] = (gn < o.N && gk < sg.K) ? sg.B[(size_t)gn * sg.ldb + gk] : 0.0;
+        }
+    };
+    auto store = [&](const Seg &sg, int buf) {
+        #pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            int row, kk;
+            if (!sg.transA) { row = t & 63; kk = (t >> 6) + 4 * r; }
+            else { kk = t & 15; row = (t >> 4) + 16 * r; }
+            As[buf][row * 20 + kk] = ra[r];
+        }
+        #pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const int kk = t & 15, col = (t >> 4) + 16 * r;
+            Bs[buf][col * 20 + kk] = rb[r];
+        }
+    };
+    // the first step of a non-empty segment at or after s
+    auto first_from = [&](int s, Seg &sg) {
+        for (; s < o.seg1; ++s) {
+            sg = segs[s];
+            if (sg.K > 0) break;
+        }
+        return s;
+    };
+    Seg cur{};
+    int sidx = first_from(o.seg0, cur), k0 = 0, buf = 0;
+    if (sidx < o.seg1) {
+        load(cur, 0);
+        store(cur, 0);
+    }
+    __syncthreads();
+    while (sidx < o.seg1) {
+        // the next step: k0 + 16 of this segment, or the next segment's 0
+        Seg nxt = cur;
+        int nsidx = sidx, nk0 = k0 + 16;
+        if (nk0 >= cur.K) {
+            nsidx = first_from(sidx + 1, nxt);
+            nk0 = 0;
+        }
+        const bool more = nsidx < o.seg1;
+        if (more) load(nxt, nk0);
+        #pragma unroll
+        for (int kk = 0; kk < 16; kk += 4) {
+            double af[4], bf[2];
+            #pragma unroll
+            for (int i = 0; i < 4; ++i) af[i] = As[buf][(wm + 8 * i + g) * 20 + kk + tig];
+            #pragma unroll
+            for (int j = 0; j < 2; ++j) bf[j] = Bs[buf][(wn + 8 * j + g) * 20 + kk + tig];
+            #pragma unroll
+            for (int i = 0; i < 4; ++i)
+                #pragma unroll
+                for (int j = 0; j < 2; ++j)
+                    dmma_884(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+        }
+        if (more) store(nxt, buf ^ 1);
+        __syncthreads();
+        buf ^= 1;
+        sidx = nsidx;
+        k0 = nk0;
+        cur = nxt;
     }
     #pragma unroll
     for (int i = 0; i < 4; ++i) {

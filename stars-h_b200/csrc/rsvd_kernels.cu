@@ -75,6 +75,13 @@ size_t workspace_layout(Workspace &w, int m_max, int n_max, int k_max,
 // entries to Nrm(slot) (deterministic per-tile norms for the adaptive
 // sketch).
 constexpr int kStageDim = 4;
+#ifndef GEN_MIN_BLOCKS
+#define GEN_MIN_BLOCKS 3      // CTAs per SM the generator is compiled for
+#endif
+#ifndef GEN_UNROLL
+#define GEN_UNROLL 8          // entries of a thread evaluated together
+#endif
+constexpr int kGenUnroll = GEN_UNROLL;
 
 // The entries of one thread in a 64 x 64 block: rows ii, columns jj0,
 // jj0 + 4, ... below jn, written to Dcol[jj * ld] (Dcol points at row ii of
@@ -96,7 +103,7 @@ __device__ __forceinline__ double gen_entries(
     }
     double ss = 0.0;
     amax = 0.0;
-    #pragma unroll 4
+    #pragma unroll kGenUnroll
     for (int jj = jj0; jj < jn; jj += 4) {
         double dist = 0.0;
         if constexpr (NDIM > 0) {
@@ -137,7 +144,7 @@ __device__ __forceinline__ double gen_entries_dim(
     return gen_entries<FAM, 0>(K, staged, rc, cc, ri, ci, ii, jj0, jn, Dcol, ld, amax);
 }
 
-__global__ void __launch_bounds__(256, 3)
+__global__ void __launch_bounds__(256, GEN_MIN_BLOCKS)
 k_gen_tiles(const DevKernel *__restrict__ kernels,
             const TileWork *__restrict__ tiles, Workspace ws, int need)
 {

@@ -2,10 +2,11 @@
 // shared batches (continuous batching), each followed by its TLR-by-dense
 // products on the resident factors.
 //
-// Worker threads (two by default, STARSH_B200_SERVER_WORKERS) own the GPU
-// work, each on its own engine context (streams and reusable buffers), so
-// that two groups are on the GPU at the same time and their launches
-// interleave.  Requests wait in FIFO order; a worker that becomes free
+// Worker threads (three by default, STARSH_B200_SERVER_WORKERS) own the
+// GPU work, each on its own engine context (streams and reusable buffers),
+// so that several groups are on the GPU at the same time and their
+// launches interleave.  A group's work is capped (5e8 matrix entries,
+// STARSH_B200_SERVER_GROUP_ENTRIES; its first request always goes in).  Requests wait in FIFO order; a worker that becomes free
 // admits, from the head of the queue, every request whose estimated device
 // footprint still fits in the budget next to the results that are resident
 // and the groups other workers are running, and runs them as one
@@ -44,6 +45,7 @@ struct Request {
     int ldb;
     int keep;
     double estimate;          // admission estimate, bytes
+    double entries;           // matrix entries (the request's work)
     std::chrono::steady_clock::time_point t_submit;
     // results
     bool done = false;
@@ -60,6 +62,7 @@ struct starsh_b200_server {
     double budget;
     int engine;
     int max_group;
+    double group_entries;             // work cap of one group (entries)
     std::mutex mu;
     std::condition_variable cv_work;   // worker: new requests or releases
     std::condition_variable cv_done;   // waiters: completions
@@ -134,11 +137,19 @@ static void worker_loop(starsh_b200_server *sv)
                     complete(sv, r, STARSH_MALLOC_ERROR, nullptr);
                     sv->cv_done.notify_all();
                 }
+                // FIFO admission by memory, and by work: a group takes the
+                // head request and then requests while the group's entries
+                // stay within the cap, so one group's latency stays short
+                // while other workers take the next ones
                 double room = sv->budget - sv->resident - sv->inflight;
+                double work = 0.0;
                 while (!sv->paused && !sv->pending.empty() &&
                        (int)group.size() < sv->max_group &&
-                       sv->pending.front()->estimate <= room) {
+                       sv->pending.front()->estimate <= room &&
+                       (group.empty() ||
+                        work + sv->pending.front()->entries <= sv->group_entries)) {
                     room -= sv->pending.front()->estimate;
+                    work += sv->pending.front()->entries;
                     group_estimate += sv->pending.front()->estimate;
                     group.push_back(sv->pending.front());
                     sv->pending.pop_front();
@@ -219,7 +230,10 @@ extern "C" int starsh_b200_server_new(starsh_b200_server **server,
     sv->budget = hbm_budget_bytes;
     sv->engine = engine;
     sv->max_group = max_group > 0 ? max_group : 1 << 30;
-    int nw = 2;
+    sv->group_entries = 5e8;
+    if (const char *e = getenv("STARSH_B200_SERVER_GROUP_ENTRIES"))
+        sv->group_entries = std::max(1.0, atof(e));
+    int nw = 3;
     if (const char *e = getenv("STARSH_B200_SERVER_WORKERS"))
         nw = std::max(1, std::min(8, atoi(e)));
     for (int w = 0; w < nw; ++w) sv->workers.emplace_back(worker_loop, sv);
@@ -248,6 +262,7 @@ extern "C" int starsh_b200_server_submit(starsh_b200_server *server,
     r->ldb = ldb;
     r->keep = keep;
     r->estimate = estimate_bytes(format, maxrank);
+    r->entries = (double)format->row_cluster->ndata * (double)format->col_cluster->ndata;
     r->t_submit = std::chrono::steady_clock::now();
     {
         std::lock_guard<std::mutex> lk(server->mu);

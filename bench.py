@@ -587,6 +587,13 @@ def run_c5(args, lib, clocks):
         "single_request_floor_ms": floor,
         "floor_what": "one 2-D square-exponential request (tol 1e-4, 32 matvecs) alone on an idle server, by N",
         "served_rps": len(reqs) / wall, "groups": int(st.groups),
+        "server_means_ms": {
+            "queue_per_request": st.queue_ms / max(1, len(reqs)),
+            "approx_per_group": st.approx_ms / max(1, st.groups),
+            "products_per_group": st.products_ms / max(1, st.groups),
+            "requests_per_group": len(reqs) / max(1, st.groups),
+            "worker_busy_frac": st.busy_ms / 1e3 / wall / max(1, int(
+                os.environ.get("STARSH_B200_SERVER_WORKERS", "3")))},
         "failed": int(st.failed),
         "peak_resident_bytes": st.peak_resident_bytes,
         "plain_fp64_one_at_a_time": {

@@ -262,6 +262,10 @@ typedef struct starsh_b200_server_stats
                                      over the workers)                     */
     double resident_bytes;        /* results kept and not yet released     */
     double peak_resident_bytes;
+    double queue_ms;              /* sum over requests: submit to the start
+                                     of their group                        */
+    double approx_ms;             /* sum over groups: batched approximation */
+    double products_ms;           /* sum over groups: the requests' products */
 } starsh_b200_server_stats;
 
 /* hbm_budget_bytes bounds the device memory of admitted and kept results

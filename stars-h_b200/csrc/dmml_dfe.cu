@@ -1,9 +1,11 @@
 // TLR-by-dense product and Frobenius error on the device.
 //
 // dmml: B = alpha M A + beta B (reference src/backends/sequential/blrm/
-// dmml.c:16-145).  Per far block T = V^T A[cols] (one batched GEMM), then
-// every block row accumulates sum_b U_b T_b + sum_near D_b A[cols] in one
-// segmented GEMM whose K loop walks the blocks of that row, so no two CTAs
+// dmml.c:16-145: per far block T = V^T A[cols], B[rows] += U T, near
+// blocks dense).  Here every T of one input block column comes from one
+// GEMM over the concatenated right factors, and every block row
+// accumulates sum_b U_b T_b + sum_near D_b A[cols] in one GEMM whose K runs
+// over the row's concatenated left factors and near blocks, so no two CTAs
 // write the same rows and the sum order is fixed (deterministic).  For
 // symm == 'S' the transposed contribution of every off-diagonal block is
 // added to the mirrored block row, as the reference does (:78-87, :111-117).
@@ -15,6 +17,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "device_ctx.cuh"
@@ -23,20 +26,6 @@
 #include "starsh-b200.h"
 
 namespace b200 {
-
-// ------------------------------------------------------ segmented GEMM
-
-struct SegOut {
-    double *C;
-    int ldc, M, N;
-    int seg0, seg1;
-};
-
-struct Seg {
-    const double *A;   // M x K (or K x M if transA), column-major
-    const double *B;   // K x N
-    int lda, ldb, K, transA;
-};
 
 __device__ __forceinline__ void dmma_884(double &c0, double &c1, double a,
                                          double b)
@@ -48,117 +37,323 @@ __device__ __forceinline__ void dmma_884(double &c0, double &c1, double a,
         : "d"(a), "d"(b));
 }
 
-// C += alpha * sum over segments of op(A_s) B_s.  CTA tile 64 x 64, same
-// fragment mapping as the batched GEMM (8 warps, 32 x 16 per warp).  The
-// K steps of 16 of all the CTA's segments form one sequence; operand tiles
-// are double-buffered in shared memory and the next step (possibly of the
-// next segment) is loaded into registers while the current one is
-// multiplied.  Each output element accumulates in the same order as a
-// plain loop over segments and steps.
-__global__ void __launch_bounds__(256)
-k_gemm_seg(const SegOut *__restrict__ outs, const Seg *__restrict__ segs,
-           double alpha, int tiles_n)
+// ------------------------------------------------------ product kernels
+//
+// B = alpha M A as two long GEMMs instead of one small GEMM per block.
+// Phase 1, per input block column j: the rows of T are the columns of all
+// right factors V_p that multiply A_j (far block p, or its mirror in a
+// symmetric format), T(rho, :) = V_p(:, c)^T A_j -- M runs over the
+// concatenated factor columns, K over the block column's rows.  Phase 2,
+// per output block row i: B_i += [U_p1 U_p2 ...] [T_p1; T_p2; ...] +
+// sum_near op(D_b) A_j -- K runs over the concatenated left-factor columns
+// of the row, then over the near blocks' columns.  T is written by phase 1
+// straight into the row-ordered layout phase 2 reads: block row i's rows
+// of T form one column-major (S_i x nrhs) matrix, S_i = sum of the row's
+// ranks.  Each output element is written by one CTA, its sum in a fixed
+// order (deterministic).
+//
+// CTA tile 128 x BN (BN = 16 FN), 8 warps as 4 (m) x 2 (n), warp tile
+// 32 x 8 FN of FP64 mma.sync m8n8k4; K steps of 16 through a three-stage
+// cp.async pipeline.  Shared-memory layouts are chosen so that the
+// fragment reads and the copies are free of bank conflicts: B as [n][k]
+// (row stride 20 doubles); A as [m][k] (stride 20) in phase 1, whose
+// operand is contiguous along k in global memory, and as [k][m] (stride
+// 132) in phase 2, whose operand is contiguous along m.
+
+struct RowT {          // where phase 1 writes row rho of T
+    long long base;    // first T row of the output block row (P_i)
+    int kappa;         // row within the block row's T_i
+    int ld;            // rows of T_i (S_i)
+};
+
+struct Job1 {          // phase 1: up to 128 rows of T that share A_j
+    int rho0, rows;
+    int K;             // rows of A_j
+    long long in0;     // first row of A_j in A
+};
+
+struct NearPiece {
+    int block;         // near block (its D pointer is given per call)
+    int trans;         // 1: the mirrored block of a symmetric format
+    int K;             // columns of op(D)
+    int ld;            // leading dimension of D
+    long long in0;     // first row of the input block in A
+};
+
+struct Job2 {          // phase 2: up to 128 rows of one output block row
+    long long out0;    // first output row
+    int m0, rows;      // rows m0 .. m0 + rows - 1 of the block row
+    long long kap0;    // P_i (first concatenated column of the row)
+    int kfar;          // S_i
+    int near0, near1;  // the row's near pieces
+};
+
+constexpr int kPBM = 128, kPBK = 16, kPStages = 3;
+constexpr int kPAStage = 2560;   // >= 128 * 20 (phase 1), 16 * 132 (phase 2)
+
+template <int FN>
+constexpr int prod_stage_doubles() { return kPAStage + 20 * 16 * FN; }
+
+__device__ __forceinline__ void cp_async8(double *dst, const double *src,
+                                          bool ok)
 {
-    const SegOut o = outs[blockIdx.y];
-    const int m0 = (blockIdx.x / tiles_n) * 64, n0 = (blockIdx.x % tiles_n) * 64;
-    if (m0 >= o.M || n0 >= o.N || o.seg0 >= o.seg1) return;
-    __shared__ double As[2][64 * 20];
-    __shared__ double Bs[2][64 * 20];
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d),
+                 "l"(src), "r"(ok ? 8 : 0));
+}
+
+__device__ __forceinline__ void cp_async_commit()
+{
+    asm volatile("cp.async.commit_group;\n" ::);
+}
+
+__device__ __forceinline__ void cp_async_wait_stages()
+{
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(kPStages - 2));
+}
+
+// acc += A_stage B_stage for one K step (A_KMAJOR: A stored as [k][m]).
+template <int FN, bool A_KMAJOR>
+__device__ __forceinline__ void prod_step(const double *As, const double *Bs,
+                                          double (&acc)[4][FN][2], int wm,
+                                          int wn, int g, int tig)
+{
+    #pragma unroll
+    for (int kk = 0; kk < kPBK; kk += 4) {
+        double af[4], bf[FN];
+        #pragma unroll
+        for (int i = 0; i < 4; ++i)
+            af[i] = A_KMAJOR ? As[(kk + tig) * 132 + wm + 8 * i + g]
+                             : As[(wm + 8 * i + g) * 20 + kk + tig];
+        #pragma unroll
+        for (int j = 0; j < FN; ++j) bf[j] = Bs[(wn + 8 * j + g) * 20 + kk + tig];
+        #pragma unroll
+        for (int i = 0; i < 4; ++i)
+            #pragma unroll
+            for (int j = 0; j < FN; ++j)
+                dmma_884(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+    }
+}
+
+// Phase 1: T rows of one job (rows rho0 .. rho0 + rows - 1), columns
+// n0 .. n0 + BN - 1 of the right-hand sides.
+template <int FN>
+__global__ void __launch_bounds__(256, 2)
+k_prod_t(const Job1 *__restrict__ jobs, const double *const *__restrict__ vcol,
+         const RowT *__restrict__ rowt, const double *__restrict__ A, int lda,
+         double *__restrict__ T, int nrhs)
+{
+    constexpr int BN = 16 * FN;
+    constexpr int STAGE = prod_stage_doubles<FN>();
+    extern __shared__ double sm[];
+    __shared__ const double *rowp[kPBM];
+    const Job1 jb = jobs[blockIdx.x];
+    const int n0 = blockIdx.y * BN;
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const int g = lane >> 2, tig = lane & 3;
-    const int wm = (warp & 1) * 32, wn = (warp >> 1) * 16;
-    double acc[4][2][2] = {};
-    double ra[4], rb[4];
-    auto load = [&](const Seg &sg, int k0) {
-        #pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            int row, kk;
-            if (!sg.transA) { row = t & 63; kk = (t >> 6) + 4 * r; }
-            else { kk = t & 15; row = (t >> 4) + 16 * r; }
-            const int gm = m0 + row, gk = k0 + kk;
-            double v = 0.0;
-            if (gm < o.M && gk < sg.K)
-                v = sg.transA ? sg.A[(size_t)gm * sg.lda + gk]
-                              : sg.A[(size_t)gk * sg.lda + gm];
-            ra[r] = v;
-        }
-        #pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            const int kk = t & 15, col = (t >> 4) + 16 * r;
-            const int gn = n0 + col, gk = k0 + kk;
-            rb[r] = (gn < o.N && gk < sg.K) ? sg.B[(size_t)gn * sg.ldb + gk] : 0.0;
-        }
-    };
-    auto store = [&](const Seg &sg, int buf) {
-        #pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            int row, kk;
-            if (!sg.transA) { row = t & 63; kk = (t >> 6) + 4 * r; }
-            else { kk = t & 15; row = (t >> 4) + 16 * r; }
-            As[buf][row * 20 + kk] = ra[r];
-        }
-        #pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            const int kk = t & 15, col = (t >> 4) + 16 * r;
-            Bs[buf][col * 20 + kk] = rb[r];
-        }
-    };
-    // the first step of a non-empty segment at or after s
-    auto first_from = [&](int s, Seg &sg) {
-        for (; s < o.seg1; ++s) {
-            sg = segs[s];
-            if (sg.K > 0) break;
-        }
-        return s;
-    };
-    Seg cur{};
-    int sidx = first_from(o.seg0, cur), k0 = 0, buf = 0;
-    if (sidx < o.seg1) {
-        load(cur, 0);
-        store(cur, 0);
-    }
+    const int wm = (warp & 3) * 32, wn = (warp >> 2) * 8 * FN;
+    for (int r = t; r < kPBM; r += 256)
+        rowp[r] = r < jb.rows ? vcol[jb.rho0 + r] : nullptr;
     __syncthreads();
-    while (sidx < o.seg1) {
-        // the next step: k0 + 16 of this segment, or the next segment's 0
-        Seg nxt = cur;
-        int nsidx = sidx, nk0 = k0 + 16;
-        if (nk0 >= cur.K) {
-            nsidx = first_from(sidx + 1, nxt);
-            nk0 = 0;
-        }
-        const bool more = nsidx < o.seg1;
-        if (more) load(nxt, nk0);
+    const int lk = t & 15, lr = t >> 4;
+    const double *Aj = A + jb.in0;
+    const int steps = (jb.K + kPBK - 1) / kPBK;
+    auto issue = [&](int step, int st) {
+        double *As = sm + st * STAGE, *Bs = As + kPAStage;
+        const int k = step * kPBK + lk;
+        const bool kin = k < jb.K;
         #pragma unroll
-        for (int kk = 0; kk < 16; kk += 4) {
-            double af[4], bf[2];
-            #pragma unroll
-            for (int i = 0; i < 4; ++i) af[i] = As[buf][(wm + 8 * i + g) * 20 + kk + tig];
-            #pragma unroll
-            for (int j = 0; j < 2; ++j) bf[j] = Bs[buf][(wn + 8 * j + g) * 20 + kk + tig];
-            #pragma unroll
-            for (int i = 0; i < 4; ++i)
-                #pragma unroll
-                for (int j = 0; j < 2; ++j)
-                    dmma_884(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+        for (int q = 0; q < 8; ++q) {
+            const double *p = rowp[lr + 16 * q];
+            const bool ok = kin && p != nullptr;
+            cp_async8(As + (lr + 16 * q) * 20 + lk, ok ? p + k : A, ok);
         }
-        if (more) store(nxt, buf ^ 1);
+        #pragma unroll
+        for (int q = 0; q < FN; ++q) {
+            const int col = n0 + lr + 16 * q;
+            const bool ok = kin && col < nrhs;
+            cp_async8(Bs + (lr + 16 * q) * 20 + lk,
+                      ok ? Aj + k + (size_t)col * lda : A, ok);
+        }
+    };
+    double acc[4][FN][2] = {};
+    #pragma unroll
+    for (int s = 0; s < kPStages - 1; ++s) {
+        if (s < steps) issue(s, s);
+        cp_async_commit();
+    }
+    for (int s = 0; s < steps; ++s) {
+        cp_async_wait_stages();
         __syncthreads();
-        buf ^= 1;
-        sidx = nsidx;
-        k0 = nk0;
-        cur = nxt;
+        if (s + kPStages - 1 < steps)
+            issue(s + kPStages - 1, (s + kPStages - 1) % kPStages);
+        cp_async_commit();
+        const double *As = sm + (s % kPStages) * STAGE;
+        prod_step<FN, false>(As, As + kPAStage, acc, wm, wn, g, tig);
     }
     #pragma unroll
     for (int i = 0; i < 4; ++i) {
-        const int gm = m0 + wm + 8 * i + g;
-        if (gm >= o.M) continue;
+        const int r = wm + 8 * i + g;
+        if (r >= jb.rows) continue;
+        const RowT rt = rowt[jb.rho0 + r];
+        double *out = T + (size_t)nrhs * rt.base + rt.kappa;
         #pragma unroll
-        for (int j = 0; j < 2; ++j)
+        for (int j = 0; j < FN; ++j)
             #pragma unroll
             for (int h = 0; h < 2; ++h) {
-                const int gn = n0 + wn + 8 * j + 2 * tig + h;
-                if (gn < o.N) o.C[(size_t)gn * o.ldc + gm] += alpha * acc[i][j][h];
+                const int col = n0 + wn + 8 * j + 2 * tig + h;
+                if (col < nrhs) out[(size_t)col * rt.ld] = acc[i][j][h];
             }
+    }
+}
+
+// Phase 2: rows m0 .. m0 + rows - 1 of one output block row.
+template <int FN>
+__global__ void __launch_bounds__(256, 2)
+k_prod_b(const Job2 *__restrict__ jobs, const double *const *__restrict__ ucol,
+         const double *__restrict__ T, int nrhs,
+         const NearPiece *__restrict__ near, const double *const *__restrict__ nearD,
+         const double *__restrict__ A, int lda, double *__restrict__ B, int ldb,
+         double alpha)
+{
+    constexpr int BN = 16 * FN;
+    constexpr int STAGE = prod_stage_doubles<FN>();
+    extern __shared__ double sm[];
+    const Job2 jb = jobs[blockIdx.x];
+    const int n0 = blockIdx.y * BN;
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int g = lane >> 2, tig = lane & 3;
+    const int wm = (warp & 3) * 32, wn = (warp >> 2) * 8 * FN;
+    // A copies: rows am, am + 64 and columns ak + 4 q (q < 4) of the step;
+    // B copies: column lk of the step, right-hand sides lr + 16 q
+    const int am = t & 63, ak = t >> 6;
+    const int lk = t & 15, lr = t >> 4;
+    const double *Tf = T + (size_t)nrhs * jb.kap0;
+    int total = (jb.kfar + kPBK - 1) / kPBK;
+    for (int q = jb.near0; q < jb.near1; ++q) total += (near[q].K + kPBK - 1) / kPBK;
+    // issue position: piece (-1: the factors, else a near piece) and k0
+    int piece = jb.kfar > 0 ? -1 : jb.near0, k0 = 0;
+    const double *up[4];            // factor columns of the next far step
+    auto fetch_ptrs = [&]() {
+        #pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int kap = k0 + ak + 4 * q;
+            up[q] = piece < 0 && kap < jb.kfar ? ucol[jb.kap0 + kap] : nullptr;
+        }
+    };
+    auto advance = [&]() {
+        k0 += kPBK;
+        const int K = piece < 0 ? jb.kfar : near[piece].K;
+        if (k0 >= K) {
+            piece = piece < 0 ? jb.near0 : piece + 1;
+            k0 = 0;
+        }
+        fetch_ptrs();
+    };
+    auto issue = [&](int st) {
+        double *As = sm + st * STAGE, *Bs = As + kPAStage;
+        if (piece < 0) {
+            #pragma unroll
+            for (int q = 0; q < 4; ++q)
+                #pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int m = am + 64 * h;
+                    const bool ok = up[q] != nullptr && m < jb.rows;
+                    cp_async8(As + (ak + 4 * q) * 132 + m,
+                              ok ? up[q] + jb.m0 + m : A, ok);
+                }
+            #pragma unroll
+            for (int q = 0; q < FN; ++q) {
+                const int col = n0 + lr + 16 * q, kap = k0 + lk;
+                const bool ok = kap < jb.kfar && col < nrhs;
+                cp_async8(Bs + (lr + 16 * q) * 20 + lk,
+                          ok ? Tf + kap + (size_t)col * jb.kfar : A, ok);
+            }
+        } else {
+            const NearPiece np = near[piece];
+            const double *D = nearD[np.block];
+            #pragma unroll
+            for (int q = 0; q < 4; ++q)
+                #pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int m = am + 64 * h, kap = k0 + ak + 4 * q;
+                    const bool ok = kap < np.K && m < jb.rows;
+                    const size_t off = np.trans
+                        ? (size_t)kap + (size_t)(jb.m0 + m) * np.ld
+                        : (size_t)(jb.m0 + m) + (size_t)kap * np.ld;
+                    cp_async8(As + (ak + 4 * q) * 132 + m, ok ? D + off : A, ok);
+                }
+            #pragma unroll
+            for (int q = 0; q < FN; ++q) {
+                const int col = n0 + lr + 16 * q, kap = k0 + lk;
+                const bool ok = kap < np.K && col < nrhs;
+                cp_async8(Bs + (lr + 16 * q) * 20 + lk,
+                          ok ? A + np.in0 + kap + (size_t)col * lda : A, ok);
+            }
+        }
+    };
+    fetch_ptrs();
+    double acc[4][FN][2] = {};
+    #pragma unroll
+    for (int s = 0; s < kPStages - 1; ++s) {
+        if (s < total) {
+            issue(s);
+            advance();
+        }
+        cp_async_commit();
+    }
+    for (int s = 0; s < total; ++s) {
+        cp_async_wait_stages();
+        __syncthreads();
+        if (s + kPStages - 1 < total) {
+            issue((s + kPStages - 1) % kPStages);
+            advance();
+        }
+        cp_async_commit();
+        const double *As = sm + (s % kPStages) * STAGE;
+        prod_step<FN, true>(As, As + kPAStage, acc, wm, wn, g, tig);
+    }
+    #pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int m = wm + 8 * i + g;
+        if (m >= jb.rows) continue;
+        double *out = B + jb.out0 + m;
+        #pragma unroll
+        for (int j = 0; j < FN; ++j)
+            #pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int col = n0 + wn + 8 * j + 2 * tig + h;
+                if (col < nrhs) out[(size_t)col * ldb] += alpha * acc[i][j][h];
+            }
+    }
+}
+
+template <int FN>
+static void launch_products(const Job1 *j1, int n1, const double *const *vcol,
+                            const RowT *rowt, const Job2 *j2, int n2,
+                            const double *const *ucol, const NearPiece *near,
+                            const double *const *nearD, const double *A, int lda,
+                            double *T, double *B, int ldb, int nrhs, double alpha,
+                            cudaStream_t s)
+{
+    constexpr size_t smem = (size_t)kPStages * prod_stage_doubles<FN>() * sizeof(double);
+    static std::once_flag attr;
+    std::call_once(attr, [] {
+        cudaFuncSetAttribute(k_prod_t<FN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+        cudaFuncSetAttribute(k_prod_b<FN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+    });
+    const unsigned ny = (unsigned)((nrhs + 16 * FN - 1) / (16 * FN));
+    if (n1 > 0) {
+        k_prod_t<FN><<<dim3((unsigned)n1, ny), 256, smem, s>>>(j1, vcol, rowt, A,
+                                                              lda, T, nrhs);
+        count_launch();
+    }
+    if (n2 > 0) {
+        k_prod_b<FN><<<dim3((unsigned)n2, ny), 256, smem, s>>>(
+            j2, ucol, T, nrhs, near, nearD, A, lda, B, ldb, alpha);
+        count_launch();
     }
 }
 
@@ -244,6 +439,157 @@ static int ensure_record(STARSH_blrm *M, Context &ctx, Record **out)
 
 // ---------------------------------------------------------------- dmml
 
+// The product plan of a matrix (device arrays, built on its first product
+// and kept with its record): phase-1 jobs with their factor-column
+// pointers and T destinations, phase-2 jobs with the concatenated
+// left-factor columns of every block row and the near pieces.
+struct ProductPlan {
+    void *dev = nullptr;
+    const double **vcol = nullptr;
+    RowT *rowt = nullptr;
+    const double **ucol = nullptr;
+    Job1 *j1 = nullptr;
+    Job2 *j2 = nullptr;
+    NearPiece *near = nullptr;
+    int n1 = 0, n2 = 0, nnear = 0;
+    long long trows = 0;       // rows of T over all block rows
+    cudaEvent_t ready = nullptr;   // the upload has completed
+    ~ProductPlan()
+    {
+        if (ready) cudaEventDestroy(ready);
+        if (dev) pool_free(dev);
+    }
+};
+
+template <class T>
+static size_t put(std::vector<char> &buf, const std::vector<T> &v)
+{
+    const size_t off = (buf.size() + 255) / 256 * 256;
+    buf.resize(off + v.size() * sizeof(T));
+    if (!v.empty()) memcpy(buf.data() + off, v.data(), v.size() * sizeof(T));
+    return off;
+}
+
+static int build_plan(STARSH_blrm *M, const Record &rec, cudaStream_t s,
+                      ProductPlan **out)
+{
+    STARSH_blrf *F = M->format;
+    STARSH_cluster *R = F->row_cluster, *C = F->col_cluster;
+    const bool symm = F->symm == 'S';
+    // products: output block row, input block (of the column clustering,
+    // or of the row clustering for a mirrored block), factors, sizes
+    struct Prod { STARSH_int orow, icol; const double *U, *V; int m, n, r; long long in0; };
+    std::vector<Prod> prods;
+    for (STARSH_int b = 0; b < F->nblocks_far; ++b) {
+        const int r = M->far_rank[b];
+        if (r <= 0) continue;
+        const STARSH_int i = F->block_far[2 * b], j = F->block_far[2 * b + 1];
+        const int m = (int)R->size[i], n = (int)C->size[j];
+        prods.push_back({i, j, rec.dU[b], rec.dV[b], m, n, r, (long long)C->start[j]});
+        if (symm && i != j)
+            prods.push_back({j, i, rec.dV[b], rec.dU[b], n, m, r, (long long)R->start[i]});
+    }
+    const STARSH_int nbr = F->nbrows, nbc = std::max(F->nbrows, F->nbcols);
+    // phase 2 layout: per output row its products in list order
+    std::vector<long long> P(nbr + 1, 0);
+    std::vector<int> S(nbr, 0);
+    std::vector<int> kap(prods.size());
+    for (size_t p = 0; p < prods.size(); ++p) {
+        kap[p] = S[prods[p].orow];
+        S[prods[p].orow] += prods[p].r;
+    }
+    for (STARSH_int i = 0; i < nbr; ++i) P[i + 1] = P[i] + S[i];
+    const long long trows = P[nbr];
+    std::vector<const double *> ucol(trows);
+    for (size_t p = 0; p < prods.size(); ++p) {
+        const Prod &q = prods[p];
+        for (int c = 0; c < q.r; ++c)
+            ucol[P[q.orow] + kap[p] + c] = q.U + (size_t)c * q.m;
+    }
+    // phase 1: products grouped by input block, list order within a group
+    std::vector<std::vector<int>> bycol(nbc);
+    for (size_t p = 0; p < prods.size(); ++p) bycol[prods[p].icol].push_back((int)p);
+    std::vector<const double *> vcol;
+    std::vector<RowT> rowt;
+    std::vector<Job1> j1;
+    vcol.reserve(trows);
+    rowt.reserve(trows);
+    for (STARSH_int j = 0; j < nbc; ++j) {
+        if (bycol[j].empty()) continue;
+        const int rho0 = (int)vcol.size();
+        for (int p : bycol[j]) {
+            const Prod &q = prods[p];
+            for (int c = 0; c < q.r; ++c) {
+                vcol.push_back(q.V + (size_t)c * q.n);
+                rowt.push_back(RowT{P[q.orow], kap[p] + c, S[q.orow]});
+            }
+        }
+        const int cnt = (int)vcol.size() - rho0;
+        const Prod &q0 = prods[bycol[j][0]];
+        for (int r0 = 0; r0 < cnt; r0 += kPBM)
+            j1.push_back(Job1{rho0 + r0, std::min(kPBM, cnt - r0), q0.n, q0.in0});
+    }
+    // near pieces per output row, in near-block order
+    std::vector<std::vector<NearPiece>> rownear(nbr);
+    for (STARSH_int b = 0; b < F->nblocks_near; ++b) {
+        const STARSH_int i = F->block_near[2 * b], j = F->block_near[2 * b + 1];
+        const int m = (int)R->size[i], n = (int)C->size[j];
+        rownear[i].push_back(NearPiece{(int)b, 0, n, m, (long long)C->start[j]});
+        if (symm && i != j)
+            rownear[j].push_back(NearPiece{(int)b, 1, m, m, (long long)R->start[i]});
+    }
+    std::vector<NearPiece> near;
+    std::vector<Job2> j2;
+    for (STARSH_int i = 0; i < nbr; ++i) {
+        if (S[i] == 0 && rownear[i].empty()) continue;
+        const int near0 = (int)near.size();
+        near.insert(near.end(), rownear[i].begin(), rownear[i].end());
+        const int mi = (int)R->size[i];
+        for (int m0 = 0; m0 < mi; m0 += kPBM)
+            j2.push_back(Job2{(long long)R->start[i] + m0, m0, std::min(kPBM, mi - m0),
+                              P[i], S[i], near0, (int)near.size()});
+    }
+    // one device allocation for every array
+    std::vector<char> buf;
+    const size_t o_vcol = put(buf, vcol), o_rowt = put(buf, rowt),
+                 o_ucol = put(buf, ucol), o_j1 = put(buf, j1), o_j2 = put(buf, j2),
+                 o_near = put(buf, near);
+    auto *plan = new ProductPlan();
+    if (!buf.empty()) {
+        char *d = (char *)pool_alloc(buf.size(), s);
+        if (d == nullptr) {
+            delete plan;
+            return cuda_fail(cudaErrorMemoryAllocation, "product plan");
+        }
+        plan->dev = d;
+        const cudaError_t e = cudaMemcpyAsync(d, buf.data(), buf.size(),
+                                              cudaMemcpyHostToDevice, s);
+        if (e != cudaSuccess) {
+            delete plan;
+            return cuda_fail(e, "product plan upload");
+        }
+        plan->vcol = (const double **)(d + o_vcol);
+        plan->rowt = (RowT *)(d + o_rowt);
+        plan->ucol = (const double **)(d + o_ucol);
+        plan->j1 = (Job1 *)(d + o_j1);
+        plan->j2 = (Job2 *)(d + o_j2);
+        plan->near = (NearPiece *)(d + o_near);
+        // products on any stream wait for the upload
+        if (cudaEventCreateWithFlags(&plan->ready, cudaEventDisableTiming) !=
+                cudaSuccess ||
+            cudaEventRecord(plan->ready, s) != cudaSuccess) {
+            delete plan;
+            return cuda_fail(cudaGetLastError(), "product plan event");
+        }
+    }
+    plan->n1 = (int)j1.size();
+    plan->n2 = (int)j2.size();
+    plan->nnear = (int)near.size();
+    plan->trows = trows;
+    *out = plan;
+    return STARSH_SUCCESS;
+}
+
 int dmml_device(STARSH_blrm *M, int nrhs, double alpha,
                 const double *dA, int lda, double beta, double *dB,
                 int ldb, cudaStream_t user_stream, Context &ctx)
@@ -268,26 +614,29 @@ int dmml_device(STARSH_blrm *M, int nrhs, double alpha,
         cudaEventRecord(ev, user_stream);
         cudaStreamWaitEvent(s, ev, 0);
     }
+    ProductPlan *plan = nullptr;
+    {
+        std::lock_guard<std::mutex> g(rec->plan_lock);
+        if (!rec->plan) {
+            ProductPlan *built = nullptr;
+            if ((info = build_plan(M, *rec, s, &built))) {
+                cudaEventDestroy(ev);
+                return info;
+            }
+            rec->plan = std::shared_ptr<void>(built, [](void *q) {
+                delete (ProductPlan *)q;
+            });
+        }
+        plan = (ProductPlan *)rec->plan.get();
+    }
+    if (plan->ready) cudaStreamWaitEvent(s, plan->ready, 0);
     {
         const long long tot = (long long)nrows * nrhs;
         k_scale_cols<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(
             dB, ldb, (int)nrows, nrhs, beta);
         count_launch();
     }
-    const bool symm = F->symm == 'S';
-    // products: (output block row, U, V, m, n, r, input offset)
-    struct Prod { STARSH_int brow; const double *U, *V; int m, n, r; STARSH_int in0; };
-    std::vector<Prod> prods;
-    for (STARSH_int b = 0; b < F->nblocks_far; ++b) {
-        const int r = M->far_rank[b];
-        if (r <= 0) continue;
-        const STARSH_int i = F->block_far[2 * b], j = F->block_far[2 * b + 1];
-        const int m = (int)R->size[i], n = (int)C->size[j];
-        prods.push_back({i, rec->dU[b], rec->dV[b], m, n, r, C->start[j]});
-        if (symm && i != j)
-            prods.push_back({j, rec->dV[b], rec->dU[b], n, m, r, R->start[i]});
-    }
-    // near blocks: dense D (stored or regenerated when onfly)
+    // near blocks: dense D (stored, or regenerated when onfly)
     double *onfly_buf = nullptr;
     std::vector<const double *> nearD(F->nblocks_near, nullptr);
     if (F->nblocks_near > 0) {
@@ -296,9 +645,11 @@ int dmml_device(STARSH_blrm *M, int nrhs, double alpha,
             for (STARSH_int b = 0; b < F->nblocks_near; ++b)
                 tot += (size_t)R->size[F->block_near[2 * b]] *
                        C->size[F->block_near[2 * b + 1]];
-            cudaError_t e = cudaMallocAsync((void **)&onfly_buf,
-                                            tot * sizeof(double), s);
-            if (e != cudaSuccess) return cuda_fail(e, "cudaMallocAsync(onfly)");
+            onfly_buf = (double *)pool_alloc(tot * sizeof(double), s);
+            if (onfly_buf == nullptr) {
+                cudaEventDestroy(ev);
+                return cuda_fail(cudaErrorMemoryAllocation, "onfly blocks");
+            }
             std::vector<BlockJob> jobs;
             size_t off = 0;
             for (STARSH_int b = 0; b < F->nblocks_near; ++b) {
@@ -309,100 +660,45 @@ int dmml_device(STARSH_blrm *M, int nrhs, double alpha,
                 off += (size_t)jb.m * jb.n;
                 jobs.push_back(jb);
             }
-            if ((info = gen_blocks(rec->points->K, jobs, s))) return info;
+            if ((info = gen_blocks(rec->points->K, jobs, s))) {
+                pool_free(onfly_buf);
+                cudaEventDestroy(ev);
+                return info;
+            }
         } else {
             for (STARSH_int b = 0; b < F->nblocks_near; ++b) nearD[b] = rec->dD[b];
         }
     }
-    // T buffer: per product r x nrhs (ld r)
-    std::vector<size_t> toff(prods.size());
-    size_t ttot = 0;
-    for (size_t p = 0; p < prods.size(); ++p) {
-        toff[p] = ttot;
-        ttot += (size_t)prods[p].r * nrhs;
-    }
-    double *T = nullptr;
-    if (ttot) {
-        cudaError_t e = cudaMallocAsync((void **)&T, ttot * sizeof(double), s);
-        if (e != cudaSuccess) return cuda_fail(e, "cudaMallocAsync(T)");
-    }
-    // Phase 1: T_p = V_p^T A[in0:in0+n, :]
-    std::vector<GemmDesc> d1;
-    int max_r = 0;
-    for (size_t p = 0; p < prods.size(); ++p) {
-        const Prod &q = prods[p];
-        GemmDesc d;
-        d.A = q.V; d.lda = q.n;
-        d.B = dA + q.in0; d.ldb = lda;
-        d.C = T + toff[p]; d.ldc = q.r;
-        d.M = q.r; d.N = nrhs; d.K = q.n;
-        d.alpha = 1.0; d.beta = 0.0;
-        d1.push_back(d);
-        max_r = std::max(max_r, q.r);
-    }
-    // Phase 2: per block row, segments over its products and near blocks.
-    std::vector<std::vector<Seg>> rowsegs(F->nbrows);
-    for (size_t p = 0; p < prods.size(); ++p) {
-        const Prod &q = prods[p];
-        rowsegs[q.brow].push_back(Seg{q.U, T + toff[p], q.m, q.r, q.r, 0});
-    }
-    for (STARSH_int b = 0; b < F->nblocks_near; ++b) {
-        const STARSH_int i = F->block_near[2 * b], j = F->block_near[2 * b + 1];
-        const int m = (int)R->size[i], n = (int)C->size[j];
-        rowsegs[i].push_back(Seg{nearD[b], dA + C->start[j], m, lda, n, 0});
-        if (symm && i != j)
-            rowsegs[j].push_back(Seg{nearD[b], dA + R->start[i], m, lda, m, 1});
-    }
-    std::vector<SegOut> outs;
-    std::vector<Seg> segs;
-    int max_m = 0;
-    for (STARSH_int i = 0; i < F->nbrows; ++i) {
-        if (rowsegs[i].empty()) continue;
-        SegOut o;
-        o.C = dB + R->start[i];
-        o.ldc = ldb;
-        o.M = (int)R->size[i];
-        o.N = nrhs;
-        o.seg0 = (int)segs.size();
-        segs.insert(segs.end(), rowsegs[i].begin(), rowsegs[i].end());
-        o.seg1 = (int)segs.size();
-        outs.push_back(o);
-        max_m = std::max(max_m, o.M);
-    }
-    // Upload descriptor arrays in one allocation.
-    const size_t b1 = d1.size() * sizeof(GemmDesc);
-    const size_t b2 = outs.size() * sizeof(SegOut);
-    const size_t b3 = segs.size() * sizeof(Seg);
-    char *dbuf = nullptr;
-    if (b1 + b2 + b3) {
-        cudaError_t e = cudaMallocAsync((void **)&dbuf, b1 + b2 + b3 + 64, s);
-        if (e != cudaSuccess) return cuda_fail(e, "cudaMallocAsync(desc)");
-        std::vector<char> hbuf(b1 + b2 + b3);
-        memcpy(hbuf.data(), d1.data(), b1);
-        memcpy(hbuf.data() + b1, outs.data(), b2);
-        memcpy(hbuf.data() + b1 + b2, segs.data(), b3);
-        cudaMemcpyAsync(dbuf, hbuf.data(), hbuf.size(), cudaMemcpyHostToDevice, s);
-    }
-    if (!d1.empty()) {
-        gemm_f64_batched(true, false, (const GemmDesc *)dbuf, (int)d1.size(),
-                         max_r, nrhs, s);
-        count_launch();
-    }
-    if (!outs.empty()) {
-        const int tiles_n = (nrhs + 63) / 64;
-        const int tiles_m = (max_m + 63) / 64;
-        for (size_t o0 = 0; o0 < outs.size(); o0 += 65535) {
-            const unsigned no = (unsigned)std::min<size_t>(65535, outs.size() - o0);
-            dim3 grid(tiles_m * tiles_n, no);
-            k_gemm_seg<<<grid, 256, 0, s>>>(
-                (const SegOut *)(dbuf + b1) + o0, (const Seg *)(dbuf + b1 + b2),
-                alpha, tiles_n);
-            count_launch();
+    // per call: T (rows of every block row x nrhs) and the near pointers
+    const size_t tbytes = (size_t)plan->trows * nrhs * sizeof(double);
+    const size_t nbytes = nearD.size() * sizeof(double *);
+    char *scratch = nullptr;
+    if (tbytes + nbytes > 0) {
+        scratch = (char *)pool_alloc((tbytes + 255) / 256 * 256 + nbytes, s);
+        if (scratch == nullptr) {
+            if (onfly_buf) pool_free(onfly_buf);
+            cudaEventDestroy(ev);
+            return cuda_fail(cudaErrorMemoryAllocation, "product scratch");
         }
     }
-    if (dbuf) cudaFreeAsync(dbuf, s);
-    if (T) cudaFreeAsync(T, s);
-    if (onfly_buf) cudaFreeAsync(onfly_buf, s);
+    double *T = (double *)scratch;
+    const double **dnear = (const double **)(scratch + (tbytes + 255) / 256 * 256);
+    if (nbytes)
+        cudaMemcpyAsync(dnear, nearD.data(), nbytes, cudaMemcpyHostToDevice, s);
+    if (nrhs > 32)
+        launch_products<4>(plan->j1, plan->n1, plan->vcol, plan->rowt, plan->j2,
+                           plan->n2, plan->ucol, plan->near, dnear, dA, lda, T, dB,
+                           ldb, nrhs, alpha, s);
+    else if (nrhs > 16)
+        launch_products<2>(plan->j1, plan->n1, plan->vcol, plan->rowt, plan->j2,
+                           plan->n2, plan->ucol, plan->near, dnear, dA, lda, T, dB,
+                           ldb, nrhs, alpha, s);
+    else
+        launch_products<1>(plan->j1, plan->n1, plan->vcol, plan->rowt, plan->j2,
+                           plan->n2, plan->ucol, plan->near, dnear, dA, lda, T, dB,
+                           ldb, nrhs, alpha, s);
+    if (scratch) pool_free(scratch);
+    if (onfly_buf) pool_free(onfly_buf);
     cudaError_t e = cudaGetLastError();
     if (user_stream != s) {
         cudaEventRecord(ev, s);

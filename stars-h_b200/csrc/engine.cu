@@ -95,12 +95,19 @@ Context *context()
             set_error("cudaStreamCreate failed");
             return;
         }
-        // keep freed pool memory cached in the process
+        // keep freed pool memory cached in the process; a block freed on
+        // one stream is reused on another only once its free has
+        // completed, never by making the allocating stream wait for the
+        // freeing one (which would chain the serving workers' streams)
         cudaMemPool_t pool;
         if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
             uint64_t keep = UINT64_MAX;
             cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold,
                                     &keep);
+            int no = 0;
+            cudaMemPoolSetAttribute(pool,
+                                    cudaMemPoolReuseAllowInternalDependencies,
+                                    &no);
         }
         cudaGetLastError();
         g_ctx_ok = true;
@@ -1531,20 +1538,22 @@ extern "C" void b200_eval_block_host(STARSH_kernel *kernel, int nrows,
     if (!info) info = dp.upload(icol, ncols * sizeof(STARSH_int), &d, s);
     dp.K.col_piv = (const long long *)d;
     double *out = nullptr;
-    if (!info && cudaMalloc(&out, (size_t)nrows * ncols * sizeof(double)) !=
-                     cudaSuccess)
-        info = STARSH_MALLOC_ERROR;
+    if (!info) {
+        out = (double *)pool_alloc((size_t)nrows * ncols * sizeof(double), s);
+        if (out == nullptr) info = STARSH_MALLOC_ERROR;
+    }
     if (!info) {
         std::vector<BlockJob> jobs{BlockJob{0, 0, nrows, ncols, out}};
         info = gen_blocks(dp.K, jobs, s);
     }
-    if (!info)
-        info = cudaMemcpy2DAsync(result, (size_t)ld * sizeof(double), out,
-                                 (size_t)nrows * sizeof(double),
-                                 (size_t)nrows * sizeof(double), ncols,
-                                 cudaMemcpyDeviceToHost, s) == cudaSuccess
-                   ? cudaStreamSynchronize(s) : STARSH_UNKNOWN_ERROR;
-    if (out) cudaFree(out);
+    if (!info &&
+        (cudaMemcpy2DAsync(result, (size_t)ld * sizeof(double), out,
+                           (size_t)nrows * sizeof(double),
+                           (size_t)nrows * sizeof(double), ncols,
+                           cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+         cudaStreamSynchronize(s) != cudaSuccess))
+        info = STARSH_UNKNOWN_ERROR;
+    if (out) pool_free(out);
     if (info) {
         fprintf(stderr, "STARSH B200: block generation failed: %s\n",
                 t_error.c_str());

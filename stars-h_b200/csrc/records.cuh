@@ -4,6 +4,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <memory>
+#include <mutex>
 #include <vector>
 #include "device_ctx.cuh"
 #include "kernel_entry.cuh"
@@ -59,6 +60,9 @@ struct Record {
     size_t u_total = 0, v_total = 0, d_total = 0;
     bool host_filled = false;
     DevicePoints *points = nullptr;    // kept for onfly near blocks
+    // the TLR-product plan (dmml_dfe.cu), built on the first product
+    std::mutex plan_lock;
+    std::shared_ptr<void> plan;
     ~Record()
     {
         for (void *p : chunks) pool_free(p);

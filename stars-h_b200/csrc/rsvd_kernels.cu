@@ -1283,11 +1283,10 @@ k_jacobi(TileWork *__restrict__ tiles, Workspace ws)
 // cyclic order does, but every rotation reads shared memory instead of L2
 // and global traffic is a few copies of the factor per sweep.  Sweeps
 // repeat until one rotates nothing.
-template <int CLASS, int G, int E>
-__global__ void __launch_bounds__(512, 1)
+template <int CLASS, int G, int E, int THREADS>
+__global__ void __launch_bounds__(THREADS, 512 / THREADS)
 k_jacobi_block(TileWork *__restrict__ tiles, Workspace ws)
 {
-    constexpr int THREADS = 512;
     constexpr int B = THREADS / G;          // columns per block, pairs per step
     constexpr int P2 = 2 * B;               // columns in shared memory
     extern __shared__ double sm[];
@@ -1398,15 +1397,20 @@ k_jacobi_block(TileWork *__restrict__ tiles, Workspace ws)
     }
 }
 
+#ifndef JACOBI_BLOCK_THREADS
+#define JACOBI_BLOCK_THREADS 512
+#endif
+
 template <int CLASS, int G, int E>
 static void jacobi_block_launch(TileWork *d_tiles, int ntiles, Workspace ws,
                                 int max_rows, cudaStream_t stream)
 {
-    auto *fn = k_jacobi_block<CLASS, G, E>;
-    const size_t smem = (size_t)2 * (512 / G) * (max_rows | 1) * sizeof(double);
+    constexpr int THREADS = JACOBI_BLOCK_THREADS;
+    auto *fn = k_jacobi_block<CLASS, G, E, THREADS>;
+    const size_t smem = (size_t)2 * (THREADS / G) * (max_rows | 1) * sizeof(double);
     cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
-    fn<<<ntiles, 512, smem, stream>>>(d_tiles, ws);
+    fn<<<ntiles, THREADS, smem, stream>>>(d_tiles, ws);
 }
 
 template <int CLASS, int G, int E, int THREADS, bool SMEM>

@@ -156,6 +156,10 @@ static void worker_loop(starsh_b200_server *sv)
                 }
                 if (!group.empty()) {
                     sv->inflight += group_estimate;
+                    const auto now = std::chrono::steady_clock::now();
+                    for (const Request *r : group)
+                        sv->stats.queue_ms += std::chrono::duration<double, std::milli>(
+                                                  now - r->t_submit).count();
                     break;
                 }
                 // nothing admissible: wait for a request or a release
@@ -179,6 +183,7 @@ static void worker_loop(starsh_b200_server *sv)
                                                  sv->engine, 0);
         starsh_b200_stats st{};
         starsh_b200_get_stats(&st);
+        auto t1 = std::chrono::steady_clock::now();
         std::vector<int> status(np, info);
         for (int i = 0; i < np && info == STARSH_SUCCESS; ++i) {
             Request *r = group[i];
@@ -208,8 +213,10 @@ static void worker_loop(starsh_b200_server *sv)
                 complete(sv, r, status[i], M);
             }
             sv->stats.resident_bytes = sv->resident;
-            sv->stats.busy_ms += std::chrono::duration<double, std::milli>(
-                                     std::chrono::steady_clock::now() - t0).count();
+            const auto t2 = std::chrono::steady_clock::now();
+            sv->stats.busy_ms += std::chrono::duration<double, std::milli>(t2 - t0).count();
+            sv->stats.approx_ms += std::chrono::duration<double, std::milli>(t1 - t0).count();
+            sv->stats.products_ms += std::chrono::duration<double, std::milli>(t2 - t1).count();
         }
         sv->cv_done.notify_all();
         // memory came back: another worker may admit now

@@ -138,7 +138,9 @@ class ServerStats(Structure):
                 ("failed", c_longlong), ("groups", c_longlong),
                 ("entries", c_longlong), ("busy_ms", c_double),
                 ("resident_bytes", c_double),
-                ("peak_resident_bytes", c_double)]
+                ("peak_resident_bytes", c_double),
+                ("queue_ms", c_double), ("approx_ms", c_double),
+                ("products_ms", c_double)]
 
 
 def _proto(lib):

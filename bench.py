@@ -1145,9 +1145,14 @@ def main():
             i, j = Fc.block_near[2 * b], Fc.block_near[2 * b + 1]
             flops += 2.0 * R.size[i] * R.size[j] * nrhs
             byts += R.size[i] * R.size[j] * 8.0
+        dgemm = fp64_peak_tflops(torch)
         dmml = {"nrhs": nrhs, "ms": t * 1e3, "gflops": flops / t / 1e9,
                 "hbm_gbs": byts / t / 1e9,
-                "bound": "fp64 tensor" if flops / byts > 5 else "hbm"}
+                "bound": "fp64 tensor" if flops / byts > 5 else "hbm",
+                "dgemm_tflops_in_run": dgemm,
+                "frac_of_dgemm": flops / t / 1e12 / dgemm,
+                "kernels": "k_prod_t (T = V^T A per input block column) + "
+                           "k_prod_b (B += U T + D A per output block row)"}
         free(M, F)
 
     # e2e: the drop-in call with host buffers

@@ -1099,6 +1099,28 @@ __host__ __device__ inline int jacobi_class(int rows, int cols)
     return 10;                                    // streamed, global
 }
 
+// Most columns a factor of the class can have (columns <= rows).
+__host__ __device__ constexpr int jacobi_class_cols(int cls)
+{
+    return cls == 0 ? 32 : cls == 1 ? 64 : cls == 2 ? 128 : cls <= 4 ? 192
+         : cls <= 6 ? 256 : cls == 7 ? 288 : cls == 8 ? 320 : cls == 9 ? 512
+         : kMaxK;
+}
+
+// Convergence bookkeeping shared by the Jacobi kernels.  Every column
+// pair is checked once per sweep at a fixed step of the schedule (T steps
+// per sweep); lastrot[c] is the step at which column c was last rotated.
+// A pair whose previous check (T steps ago) found it orthogonal and whose
+// columns have not been rotated since is orthogonal still: it is skipped,
+// so late sweeps, and the final sweep that confirms convergence, only
+// look at the pairs that changed.  A sweep that rotates nothing ends the
+// iteration exactly as when every pair is checked.
+__device__ __forceinline__ bool jacobi_unchanged(const int *lastrot, int a,
+                                                 int b, int since)
+{
+    return lastrot[a] < since && lastrot[b] < since;
+}
+
 // Rotation of the column pair (ca, cb) by the G lanes of one group (gl =
 // lane within the group).  Every lane of the warp calls this (inactive
 // groups with valid = false) because the reductions shuffle across the
@@ -1191,10 +1213,12 @@ k_jacobi(TileWork *__restrict__ tiles, Workspace ws)
 {
     extern __shared__ double sm[];
     __shared__ int rotated[2];
+    __shared__ int lastrot[jacobi_class_cols(CLASS)];
     TileWork &tw = tiles[blockIdx.x];
     const int s = tw.slot;
     const int rows = tw.k1, cols = tw.k2;
     if (cols <= 0 || jacobi_class(rows, cols) != CLASS) return;   // uniform
+    for (int c = threadIdx.x; c < cols; c += THREADS) lastrot[c] = -1;
     // Relative orthogonality the rotations stop at: the rank cut needs the
     // left singular vectors orthonormal to well below tol (their overlap
     // enters the tail energies squared and the projector linearly): 1 % of
@@ -1220,10 +1244,12 @@ k_jacobi(TileWork *__restrict__ tiles, Workspace ws)
     const int gw = lane / G, gl = lane % G;
     const int nc = cols + (cols & 1);      // players, with a bye if odd
     const int npairs = nc / 2;
+    const int T = nc - 1;                  // steps per sweep
     int sweep = 0;
     for (; sweep < 40; ++sweep) {
         bool any = false;
         for (int step = 0; step < nc - 1; ++step) {
+            const int now = sweep * T + step;
             for (int base = warp * kGroupsPerWarp; base < npairs;
                  base += kWarps * kGroupsPerWarp) {
                 const int p = base + gw;
@@ -1238,12 +1264,17 @@ k_jacobi(TileWork *__restrict__ tiles, Workspace ws)
                     a = p == 0 ? 0 : 1 + x;
                     b = 1 + y;
                 }
-                const bool valid = p < npairs && a < cols && b < cols;
+                const bool valid = p < npairs && a < cols && b < cols &&
+                                   !jacobi_unchanged(lastrot, a, b, now - T);
+                if (!__any_sync(0xffffffffu, valid)) continue;   // warp-uniform
                 double *ca = A + (size_t)a * lda, *cb = A + (size_t)b * lda;
+                bool rot;
                 if constexpr (E > 0)
-                    any |= jacobi_rotate<G, E>(ca, cb, rows, gl, valid, eps2);
+                    rot = jacobi_rotate<G, E>(ca, cb, rows, gl, valid, eps2);
                 else
-                    any |= jacobi_rotate_stream(ca, cb, rows, lane, valid, eps2);
+                    rot = jacobi_rotate_stream(ca, cb, rows, lane, valid, eps2);
+                if (rot && gl == 0) lastrot[a] = lastrot[b] = now;
+                any |= rot;
             }
             __syncthreads();
         }
@@ -1291,6 +1322,7 @@ k_jacobi_block(TileWork *__restrict__ tiles, Workspace ws)
     constexpr int P2 = 2 * B;               // columns in shared memory
     extern __shared__ double sm[];
     __shared__ int rotated[2];
+    __shared__ int lastrot[jacobi_class_cols(CLASS)];
     TileWork &tw = tiles[blockIdx.x];
     const int s = tw.slot;
     const int rows = tw.k1, cols = tw.k2;
@@ -1303,30 +1335,60 @@ k_jacobi_block(TileWork *__restrict__ tiles, Workspace ws)
     const int nb = (cols + B - 1) / B;
     const int nbp = nb + (nb & 1);          // blocks, with a bye if odd
     const int gw = threadIdx.x / G, gl = threadIdx.x % G;
+    for (int c = threadIdx.x; c < cols; c += THREADS) lastrot[c] = -1;
     if (threadIdx.x == 0) rotated[0] = rotated[1] = 0;
     __syncthreads();
     auto column = [&](int q, int bi, int bj) {   // global column of slot q
         return q < B ? bi * B + q : bj * B + q - B;
     };
+    // the block pair of round rnd, meeting pr (circle method, as for
+    // columns); bye: one of the two is the empty block of an odd count
+    auto meeting = [&](int rnd, int pr, int &bi, int &bj) {
+        int x = pr - 1 + rnd, y = nbp - 2 - pr + rnd;
+        if (x >= nbp - 1) x -= nbp - 1;
+        if (y >= nbp - 1) y -= nbp - 1;
+        bi = pr == 0 ? 0 : 1 + x;
+        bj = 1 + y;
+        return bi >= nb || bj >= nb;
+    };
+    // steps of one sweep (the same schedule every sweep)
+    int T = 0;
+    for (int rnd = 0; rnd < nbp - 1; ++rnd)
+        for (int pr = 0; pr < nbp / 2; ++pr) {
+            int bi, bj;
+            const bool bye = meeting(rnd, pr, bi, bj);
+            if (bye && rnd > 0) continue;
+            T += (rnd == 0 ? B - 1 : 0) + (bye ? 0 : B);
+        }
     int sweep = 0;
     for (; sweep < 40; ++sweep) {
         bool any = false;
+        int now = sweep * T;                // step count, advanced per step
         for (int rnd = 0; rnd < nbp - 1; ++rnd) {
             for (int pr = 0; pr < nbp / 2; ++pr) {
-                // block pair pr of round rnd (circle method, as for columns)
-                int x = pr - 1 + rnd, y = nbp - 2 - pr + rnd;
-                if (x >= nbp - 1) x -= nbp - 1;
-                if (y >= nbp - 1) y -= nbp - 1;
-                const int bi = pr == 0 ? 0 : 1 + x, bj = 1 + y;
+                int bi, bj;
                 // Each block's own pairs are rotated once per sweep, in the
                 // first round (where every block meets exactly one other,
                 // or the bye); every meeting rotates the B^2 pairs across
                 // its two blocks.
-                const bool bye = bi >= nb || bj >= nb;
+                const bool bye = meeting(rnd, pr, bi, bj);
                 if (bye && rnd > 0) continue;                   // uniform
                 const int b0 = bye ? (bi < nb ? bi : bj) : bi;  // slots 0 .. B-1
                 const int b1 = bye ? nb : bj;                   // slots B .. 2B-1
                 const int nslots = bye ? B : P2;
+                const int msteps = (rnd == 0 ? B - 1 : 0) + (bye ? 0 : B);
+                // A meeting none of whose columns has been rotated since
+                // its previous occurrence (T steps ago, when all its pairs
+                // were found orthogonal) is skipped with its copies.
+                int hot = 0;
+                for (int q = threadIdx.x; q < nslots; q += THREADS) {
+                    const int c = column(q, b0, b1);
+                    if (c < cols && lastrot[c] >= now - T) hot = 1;
+                }
+                if (!__syncthreads_or(hot)) {
+                    now += msteps;
+                    continue;
+                }
                 for (int e = threadIdx.x; e < nslots * rows; e += THREADS) {
                     const int q = e / rows, i = e - q * rows;
                     const int c = column(q, b0, b1);
@@ -1343,25 +1405,37 @@ k_jacobi_block(TileWork *__restrict__ tiles, Workspace ws)
                         if (u >= B - 1) u -= B - 1;
                         if (v >= B - 1) v -= B - 1;
                         const int a = off + (q == 0 ? 0 : 1 + u), b = off + 1 + v;
-                        const bool valid = (off == 0 || !bye) &&
-                                           column(a, b0, b1) < cols &&
-                                           column(b, b0, b1) < cols;
-                        any |= jacobi_rotate<G, E>(sm + (size_t)a * lds,
-                                                   sm + (size_t)b * lds, rows, gl,
-                                                   valid, eps2);
+                        const int ca = column(a, b0, b1), cb = column(b, b0, b1);
+                        const bool valid = (off == 0 || !bye) && ca < cols &&
+                                           cb < cols &&
+                                           !jacobi_unchanged(lastrot, ca, cb, now - T);
+                        if (__any_sync(0xffffffffu, valid)) {
+                            const bool rot = jacobi_rotate<G, E>(
+                                sm + (size_t)a * lds, sm + (size_t)b * lds, rows,
+                                gl, valid, eps2);
+                            if (rot && gl == 0) lastrot[ca] = lastrot[cb] = now;
+                            any |= rot;
+                        }
                         __syncthreads();
+                        ++now;
                     }
                 }
                 if (!bye) {
                     // the cross pairs: slot gw with slot B + (gw + step) mod B
                     for (int step = 0; step < B; ++step) {
                         const int a = gw, b = B + (gw + step) % B;
-                        const bool valid = column(a, b0, b1) < cols &&
-                                           column(b, b0, b1) < cols;
-                        any |= jacobi_rotate<G, E>(sm + (size_t)a * lds,
-                                                   sm + (size_t)b * lds, rows, gl,
-                                                   valid, eps2);
+                        const int ca = column(a, b0, b1), cb = column(b, b0, b1);
+                        const bool valid = ca < cols && cb < cols &&
+                                           !jacobi_unchanged(lastrot, ca, cb, now - T);
+                        if (__any_sync(0xffffffffu, valid)) {
+                            const bool rot = jacobi_rotate<G, E>(
+                                sm + (size_t)a * lds, sm + (size_t)b * lds, rows,
+                                gl, valid, eps2);
+                            if (rot && gl == 0) lastrot[ca] = lastrot[cb] = now;
+                            any |= rot;
+                        }
                         __syncthreads();
+                        ++now;
                     }
                 }
                 for (int e = threadIdx.x; e < nslots * rows; e += THREADS) {

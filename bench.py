@@ -1159,6 +1159,11 @@ def main():
     entry = (lib.starsh_blrm__drsdd_b200_mp if chosen == sb.ENGINE_MIXED
              else lib.starsh_blrm__drsdd_b200)
     e2e_times, e2e_st = [], None
+    for _ in range(args.warmup):
+        # untimed, like the device-resident warm-up (first use of the
+        # library's page-locked host blocks)
+        M, F, *_ = step(chosen, 1, entry)
+        free(M, F)
     barrier()
     for _ in range(args.steps):
         M, F, dt, host, st = step(chosen, 1, entry)

@@ -21,6 +21,7 @@ struct Context {
     int device = -1;
     cudaStream_t stream = nullptr;
     cudaStream_t side = nullptr;   // second stream for overlapping launches
+    cudaStream_t copy = nullptr;   // device-to-host copies of finished batches
     DeviceBuffer workspace;    // per-slot scratch of the engine
     DeviceBuffer tiles;        // TileWork array of a batch
     DeviceBuffer descs;        // GemmDesc array of a batch
@@ -51,6 +52,13 @@ void set_thread_context(Context *c);
 // library stream.
 void *pool_alloc(size_t bytes, cudaStream_t s);
 void pool_free(void *p);
+
+// Page-locked host memory for host mirrors, kept after use (up to a cap)
+// so that repeated approximations copy straight into memory that is
+// already pinned.  host_pinned_free returns false for a pointer the pool
+// did not hand out.
+void *host_pinned_alloc(size_t bytes);
+bool host_pinned_free(void *p);
 
 // Records a CUDA error (with the call site) as the library's last error and
 // returns the matching STARSH error code.

@@ -20,6 +20,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <unordered_map>
 #include <vector>
 
@@ -90,6 +91,8 @@ Context *context()
         if (cudaStreamCreateWithFlags(&g_ctx.stream, cudaStreamNonBlocking)
                 != cudaSuccess ||
             cudaStreamCreateWithFlags(&g_ctx.side, cudaStreamNonBlocking)
+                != cudaSuccess ||
+            cudaStreamCreateWithFlags(&g_ctx.copy, cudaStreamNonBlocking)
                 != cudaSuccess) {
             cudaGetLastError();
             set_error("cudaStreamCreate failed");
@@ -134,7 +137,8 @@ Context *context_new_private()
     c->device = base->device;
     cudaSetDevice(c->device);
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->copy, cudaStreamNonBlocking) != cudaSuccess) {
         cudaGetLastError();
         delete c;
         return nullptr;
@@ -148,6 +152,7 @@ void context_free_private(Context *c)
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
     cudaStreamSynchronize(c->side);
+    cudaStreamSynchronize(c->copy);
     c->workspace.release();
     c->tiles.release();
     c->descs.release();
@@ -161,6 +166,7 @@ void context_free_private(Context *c)
     }
     cudaStreamDestroy(c->stream);
     cudaStreamDestroy(c->side);
+    cudaStreamDestroy(c->copy);
     delete c;
 }
 
@@ -181,6 +187,70 @@ void pool_free(void *p)
     // ordered on the calling thread's stream (its own work on p, if any,
     // precedes the free; matrices are freed after a device synchronisation)
     if (p) cudaFreeAsync(p, t_ctx != nullptr ? t_ctx->stream : g_ctx.stream);
+}
+
+// ------------------------------------------------- pinned host memory
+
+static std::mutex g_pin_mu;
+static std::multimap<size_t, void *> g_pin_idle;        // size -> block
+static std::unordered_map<void *, size_t> g_pin_owned;  // every block
+static size_t g_pin_idle_bytes = 0;
+
+static size_t pinned_cache_cap()
+{
+    static const size_t cap = [] {
+        size_t mb = 32768;   // idle pinned memory kept for reuse
+        if (const char *e = getenv("STARSH_B200_PINNED_CACHE_MB"))
+            mb = (size_t)std::max(0, atoi(e));
+        return mb << 20;
+    }();
+    return cap;
+}
+
+void *host_pinned_alloc(size_t bytes)
+{
+    bytes = std::max<size_t>(bytes, 1);
+    {
+        // an idle block at most a quarter larger than asked
+        std::lock_guard<std::mutex> g(g_pin_mu);
+        auto it = g_pin_idle.lower_bound(bytes);
+        if (it != g_pin_idle.end() && it->first <= bytes + bytes / 4) {
+            void *p = it->second;
+            g_pin_idle_bytes -= it->first;
+            g_pin_idle.erase(it);
+            return p;
+        }
+    }
+    void *p = nullptr;
+    if (cudaHostAlloc(&p, bytes, cudaHostAllocPortable) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> g(g_pin_mu);
+    g_pin_owned[p] = bytes;
+    return p;
+}
+
+bool host_pinned_free(void *p)
+{
+    std::vector<void *> drop;
+    {
+        std::lock_guard<std::mutex> g(g_pin_mu);
+        auto it = g_pin_owned.find(p);
+        if (it == g_pin_owned.end()) return false;
+        g_pin_idle.emplace(it->second, p);
+        g_pin_idle_bytes += it->second;
+        // above the cap: the largest idle blocks go back to the system
+        while (g_pin_idle_bytes > pinned_cache_cap() && !g_pin_idle.empty()) {
+            auto last = std::prev(g_pin_idle.end());
+            g_pin_idle_bytes -= last->first;
+            g_pin_owned.erase(last->second);
+            drop.push_back(last->second);
+            g_pin_idle.erase(last);
+        }
+    }
+    for (void *q : drop) cudaFreeHost(q);
+    return true;
 }
 
 void set_error(const std::string &msg)
@@ -390,6 +460,7 @@ struct EngineParams {
     int block;      // adaptive sketch: columns of the first round
     int block_next; // ... and of every later round
     int verify;     // unselected sample columns that finish a tile
+    bool mirror;    // host mirrors wanted: download each batch when done
 };
 
 // One problem of a batched approximation call.
@@ -437,6 +508,12 @@ static void cluster_boxes(const double *pts, long long count, int ndim,
 static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
                           const EngineParams &ep)
 {
+    // every return waits for the batch downloads still in flight (their
+    // device sources are freed with the records on failure)
+    struct CopyDrain {
+        cudaStream_t c;
+        ~CopyDrain() { cudaStreamSynchronize(c); }
+    } drain{ctx.copy};
     cudaStream_t s = ctx.stream;
     starsh_b200_stats &st = thread_stats();
     std::vector<TileWork> all;
@@ -921,10 +998,12 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
             rec->dU[owner[b0 + t].second] = base + w.off_u;
             rec->dV[owner[b0 + t].second] = base + w.off_v;
         }
+        std::vector<size_t> part_of(jobs.size(), 0);
         for (size_t p = 0; p < jobs.size(); ++p) {
             if (nu[p] + nv[p] == 0) continue;
             Record *rec = jobs[p].rec;
             rec->shared.push_back(chunk);
+            part_of[p] = rec->parts.size();
             rec->parts.push_back({base + u0[p], nu[p], base + v0[p], nv[p]});
             rec->u_total += nu[p];
             rec->v_total += nv[p];
@@ -941,6 +1020,24 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
             count_launch();
             cudaEventRecord(ev[8], s);
             output_pending = true;
+            if (ep.mirror) {
+                // each problem's factors of this batch go to page-locked
+                // host memory on the copy stream while later batches run
+                B200_CUDA(cudaStreamWaitEvent(ctx.copy, ev[8], 0), "mirror wait");
+                for (size_t p = 0; p < jobs.size(); ++p) {
+                    if (nu[p] + nv[p] == 0) continue;
+                    double *h = (double *)host_pinned_alloc(
+                        (nu[p] + nv[p]) * sizeof(double));
+                    if (h == nullptr) continue;   // mirrored later, staged
+                    B200_CUDA(cudaMemcpyAsync(h, base + u0[p],
+                                              (nu[p] + nv[p]) * sizeof(double),
+                                              cudaMemcpyDeviceToHost, ctx.copy),
+                              "mirror copy");
+                    Record::Part &pt = jobs[p].rec->parts[part_of[p]];
+                    pt.hU = h;
+                    pt.hV = h + nu[p];
+                }
+            }
         }
         if (const char *path = getenv("STARSH_B200_TILE_LOG")) {
             // diagnostics: one line per tile of the shape, basis and factor
@@ -1046,9 +1143,108 @@ static int staged_d2h(Context &ctx, const std::vector<D2HCopy> &jobs,
     return STARSH_SUCCESS;
 }
 
+// Host mirrors held in page-locked blocks of the pinned pool, by matrix.
+static std::mutex g_mirror_mu;
+static std::unordered_map<const STARSH_blrm *, std::vector<void *>> g_mirrors;
+
+// The host mirror from the parts downloaded batch by batch (the copies
+// have completed): far_U/far_V point into the parts' page-locked blocks,
+// the near blocks are copied into one more.
+static int map_early_mirror(STARSH_blrm *M, Record &rec, cudaStream_t s)
+{
+    STARSH_blrf *F = M->format;
+    starsh_b200_stats &st = thread_stats();
+    struct Span { const double *dev; size_t n; double *host; };
+    std::vector<Span> su, sv;
+    for (const Record::Part &pt : rec.parts) {
+        su.push_back({pt.U, pt.nu, pt.hU});
+        sv.push_back({pt.V, pt.nv, pt.hV});
+    }
+    auto by_dev = [](const Span &a, const Span &b) { return a.dev < b.dev; };
+    std::sort(su.begin(), su.end(), by_dev);
+    std::sort(sv.begin(), sv.end(), by_dev);
+    auto host_of = [](const std::vector<Span> &sp, const double *d) -> double * {
+        auto it = std::upper_bound(sp.begin(), sp.end(), Span{d, 0, nullptr},
+                                   [](const Span &a, const Span &b) {
+                                       return a.dev < b.dev;
+                                   });
+        if (it == sp.begin()) return nullptr;
+        --it;
+        if (d < it->dev || d >= it->dev + it->n) return nullptr;
+        return it->host + (d - it->dev);
+    };
+    for (STARSH_int b = 0; b < F->nblocks_far; ++b) {
+        // blocks without factors point at the first block, as in the
+        // single-allocation mirror
+        M->far_U[b]->data = rec.parts[0].hU;
+        M->far_V[b]->data = rec.parts[0].hV;
+        if (M->far_rank[b] <= 0) continue;
+        double *hu = host_of(su, rec.dU[b]), *hv = host_of(sv, rec.dV[b]);
+        if (hu == nullptr || hv == nullptr) {
+            set_error("host mirror: factor outside its chunks");
+            return STARSH_UNKNOWN_ERROR;
+        }
+        M->far_U[b]->data = hu;
+        M->far_V[b]->data = hv;
+    }
+    std::vector<void *> owned;
+    double *hD = nullptr;
+    bool d_pinned = false;
+    if (M->onfly == 0 && F->nblocks_near > 0) {
+        const size_t bytes = std::max<size_t>(rec.d_total, 1) * sizeof(double);
+        hD = (double *)host_pinned_alloc(bytes);
+        d_pinned = hD != nullptr;
+        if (!d_pinned) hD = (double *)malloc(bytes);
+        if (hD == nullptr) return STARSH_MALLOC_ERROR;
+        if (rec.d_total) {
+            // near blocks live in one contiguous device allocation
+            cudaError_t e = d_pinned
+                ? cudaMemcpyAsync(hD, rec.dD[0], rec.d_total * sizeof(double),
+                                  cudaMemcpyDeviceToHost, s)
+                : cudaSuccess;
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+            int info = e == cudaSuccess ? STARSH_SUCCESS : cuda_fail(e, "near mirror");
+            if (!info && !d_pinned)
+                info = staged_d2h(*context(),
+                                  {{(char *)hD, (const char *)rec.dD[0],
+                                    rec.d_total * sizeof(double)}}, s);
+            if (info) {
+                if (d_pinned) host_pinned_free(hD);
+                else free(hD);
+                return info;
+            }
+        }
+        size_t od = 0;
+        for (STARSH_int b = 0; b < F->nblocks_near; ++b) {
+            M->near_D[b]->data = hD + od;
+            od += M->near_D[b]->size;
+        }
+        if (d_pinned) owned.push_back(hD);
+    }
+    // the matrix owns the blocks from here on (the device record may be
+    // released before it)
+    for (Record::Part &pt : rec.parts) {
+        owned.push_back(pt.hU);
+        pt.hU = pt.hV = nullptr;
+    }
+    {
+        std::lock_guard<std::mutex> g(g_mirror_mu);
+        g_mirrors[M] = std::move(owned);
+    }
+    st.d2h_bytes += (long long)(rec.u_total + rec.v_total + rec.d_total) * 8;
+    M->alloc_U = nullptr;
+    M->alloc_V = nullptr;
+    M->alloc_D = d_pinned ? nullptr : hD;
+    rec.host_filled = true;
+    return STARSH_SUCCESS;
+}
+
 static int fill_host_mirror(STARSH_blrm *M, Record &rec, cudaStream_t s)
 {
     if (rec.host_filled) return STARSH_SUCCESS;
+    bool early = !rec.parts.empty();
+    for (const Record::Part &pt : rec.parts) early = early && pt.hU != nullptr;
+    if (early) return map_early_mirror(M, rec, s);
     STARSH_blrf *F = M->format;
     starsh_b200_stats &st = thread_stats();
     double *hU = (double *)malloc(std::max<size_t>(rec.u_total, 1) * sizeof(double));
@@ -1367,6 +1563,7 @@ static int approximate_batch(int np, STARSH_blrm **matrices,
     EngineParams ep{};
     ep.oversample = b200_oversample();
     ep.engine = engine;
+    ep.mirror = (flags & STARSH_B200_HOST_MIRROR) != 0;
     read_engine_env(ep);
     int info = compress_multi(*ctx, jobs, ep);
     int done = 0;
@@ -1466,6 +1663,19 @@ extern "C" void starsh_b200_blrm_release(STARSH_blrm *matrix)
     Context *ctx = context();
     if (ctx) cudaDeviceSynchronize();
     delete rec;
+}
+
+extern "C" void b200_host_mirror_free(const STARSH_blrm *matrix)
+{
+    std::vector<void *> owned;
+    {
+        std::lock_guard<std::mutex> g(g_mirror_mu);
+        auto it = g_mirrors.find(matrix);
+        if (it == g_mirrors.end()) return;
+        owned = std::move(it->second);
+        g_mirrors.erase(it);
+    }
+    for (void *p : owned) host_pinned_free(p);
 }
 
 extern "C" int starsh_b200_set_device(int device)

@@ -55,7 +55,12 @@ struct Record {
     std::vector<double *> dD;          // per near block (device, or null)
     // Factor chunks in far-block order: the host mirror of U (V) is the
     // concatenation of the chunks' U (V) parts.
-    struct Part { const double *U; size_t nu; const double *V; size_t nv; };
+    // hU (hV): the part's host copy when it was downloaded as soon as its
+    // batch finished (page-locked; U then V in one block), else null.
+    struct Part {
+        const double *U; size_t nu; const double *V; size_t nv;
+        double *hU = nullptr, *hV = nullptr;
+    };
     std::vector<Part> parts;
     size_t u_total = 0, v_total = 0, d_total = 0;
     bool host_filled = false;
@@ -65,6 +70,8 @@ struct Record {
     std::shared_ptr<void> plan;
     ~Record()
     {
+        for (Part &pt : parts)
+            if (pt.hU) host_pinned_free(pt.hU);
         for (void *p : chunks) pool_free(p);
         delete points;
     }

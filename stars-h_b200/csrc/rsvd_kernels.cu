@@ -19,6 +19,7 @@
 //     decides the rank is exact to FP64 rounding even where the Gram's
 //     eigenvalues are not.
 #include <cfloat>
+#include <cooperative_groups.h>
 #include "engine.cuh"
 
 namespace b200 {
@@ -1306,7 +1307,7 @@ k_jacobi(TileWork *__restrict__ tiles, Workspace ws)
 // Block one-sided Jacobi for the classes whose factor does not fit in
 // shared memory (k1 <= 512).  The k2 columns form blocks of B = 512 / G;
 // the blocks meet in a round-robin tournament, and each meeting brings the
-// block pair (2B columns, 131 KB at most) into shared memory, rotates the
+// block pair (2B columns, 164 KB at most) into shared memory, rotates the
 // B^2 column pairs across the two blocks there (B steps of B disjoint
 // pairs, one group of G lanes per pair, E rows per lane) and writes it
 // back; the pairs inside each block are rotated in the tournament's first
@@ -1314,128 +1315,133 @@ k_jacobi(TileWork *__restrict__ tiles, Workspace ws)
 // cyclic order does, but every rotation reads shared memory instead of L2
 // and global traffic is a few copies of the factor per sweep.  Sweeps
 // repeat until one rotates nothing.
-template <int CLASS, int G, int E, int THREADS>
-__global__ void __launch_bounds__(THREADS, 512 / THREADS)
+//
+// The meetings of one round touch disjoint blocks, so a tile is taken by a
+// cluster of kJacobiCluster CTAs that share each round's meetings and meet
+// at a cluster barrier between rounds (which also publishes the round's
+// columns in global memory): a tile's latency, which is what bounds the
+// batches that hold few such tiles, drops by up to that factor.  Times
+// (for the convergence bookkeeping) count the steps of a round once,
+// whichever CTA runs a meeting: round 0 takes steps [0, 2B - 1) (B - 1
+// within blocks, B across), round r > 0 the B steps from B - 1 + r B; a
+// column is only rotated by the one meeting of a round that holds it.
+// lastrot lives in the slot's Sig buffer during the iteration (the
+// normalisation overwrites it at the end), each meeting works on its own
+// copy of its columns' entries.  Data another CTA of the cluster wrote is
+// read past L1 (__ldcg).
+constexpr int kJacobiCluster = 4;
+
+template <int CLASS, int G, int E>
+__global__ void __launch_bounds__(512, 1)
 k_jacobi_block(TileWork *__restrict__ tiles, Workspace ws)
 {
+    constexpr int THREADS = 512;
     constexpr int B = THREADS / G;          // columns per block, pairs per step
     constexpr int P2 = 2 * B;               // columns in shared memory
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
+    const int crank = (int)cl.block_rank(), csize = (int)cl.num_blocks();
     extern __shared__ double sm[];
-    __shared__ int rotated[2];
-    __shared__ int lastrot[jacobi_class_cols(CLASS)];
-    TileWork &tw = tiles[blockIdx.x];
+    __shared__ int rotated[2];              // in the cluster's first CTA
+    __shared__ int lr[P2];                  // lastrot of the meeting's slots
+    TileWork &tw = tiles[blockIdx.x / csize];
     const int s = tw.slot;
     const int rows = tw.k1, cols = tw.k2;
-    if (cols <= 0 || jacobi_class(rows, cols) != CLASS) return;   // uniform
+    if (cols <= 0 || jacobi_class(rows, cols) != CLASS) return;   // cluster-uniform
     const double eps = fmax(1e-15, fmin(1e-7, 0.01 * tw.tol));
     const double eps2 = eps * eps;
     const int ldg = ws.ldK();
     double *Lg = ws.L(s);
+    int *lastrot = (int *)ws.Sig(s);
+    int *rot0 = cl.map_shared_rank(rotated, 0);
     const int lds = rows | 1;
     const int nb = (cols + B - 1) / B;
     const int nbp = nb + (nb & 1);          // blocks, with a bye if odd
     const int gw = threadIdx.x / G, gl = threadIdx.x % G;
-    for (int c = threadIdx.x; c < cols; c += THREADS) lastrot[c] = -1;
-    if (threadIdx.x == 0) rotated[0] = rotated[1] = 0;
-    __syncthreads();
+    for (int c = crank * THREADS + threadIdx.x; c < cols; c += csize * THREADS)
+        lastrot[c] = -1;
+    if (crank == 0 && threadIdx.x == 0) rotated[0] = rotated[1] = 0;
+    cl.sync();
     auto column = [&](int q, int bi, int bj) {   // global column of slot q
         return q < B ? bi * B + q : bj * B + q - B;
     };
-    // the block pair of round rnd, meeting pr (circle method, as for
-    // columns); bye: one of the two is the empty block of an odd count
-    auto meeting = [&](int rnd, int pr, int &bi, int &bj) {
-        int x = pr - 1 + rnd, y = nbp - 2 - pr + rnd;
-        if (x >= nbp - 1) x -= nbp - 1;
-        if (y >= nbp - 1) y -= nbp - 1;
-        bi = pr == 0 ? 0 : 1 + x;
-        bj = 1 + y;
-        return bi >= nb || bj >= nb;
-    };
-    // steps of one sweep (the same schedule every sweep)
-    int T = 0;
-    for (int rnd = 0; rnd < nbp - 1; ++rnd)
-        for (int pr = 0; pr < nbp / 2; ++pr) {
-            int bi, bj;
-            const bool bye = meeting(rnd, pr, bi, bj);
-            if (bye && rnd > 0) continue;
-            T += (rnd == 0 ? B - 1 : 0) + (bye ? 0 : B);
-        }
+    const int T = (B - 1) + (nbp - 1) * B;      // steps per sweep
     int sweep = 0;
     for (; sweep < 40; ++sweep) {
         bool any = false;
-        int now = sweep * T;                // step count, advanced per step
         for (int rnd = 0; rnd < nbp - 1; ++rnd) {
-            for (int pr = 0; pr < nbp / 2; ++pr) {
-                int bi, bj;
+            const int t0 = sweep * T + (rnd == 0 ? 0 : B - 1 + rnd * B);
+            for (int pr = crank; pr < nbp / 2; pr += csize) {
+                // block pair pr of round rnd (circle method, as for columns)
+                int x = pr - 1 + rnd, y = nbp - 2 - pr + rnd;
+                if (x >= nbp - 1) x -= nbp - 1;
+                if (y >= nbp - 1) y -= nbp - 1;
+                const int bi = pr == 0 ? 0 : 1 + x, bj = 1 + y;
                 // Each block's own pairs are rotated once per sweep, in the
                 // first round (where every block meets exactly one other,
                 // or the bye); every meeting rotates the B^2 pairs across
                 // its two blocks.
-                const bool bye = meeting(rnd, pr, bi, bj);
+                const bool bye = bi >= nb || bj >= nb;
                 if (bye && rnd > 0) continue;                   // uniform
                 const int b0 = bye ? (bi < nb ? bi : bj) : bi;  // slots 0 .. B-1
                 const int b1 = bye ? nb : bj;                   // slots B .. 2B-1
                 const int nslots = bye ? B : P2;
-                const int msteps = (rnd == 0 ? B - 1 : 0) + (bye ? 0 : B);
                 // A meeting none of whose columns has been rotated since
                 // its previous occurrence (T steps ago, when all its pairs
                 // were found orthogonal) is skipped with its copies.
                 int hot = 0;
-                for (int q = threadIdx.x; q < nslots; q += THREADS) {
-                    const int c = column(q, b0, b1);
-                    if (c < cols && lastrot[c] >= now - T) hot = 1;
+                for (int q = threadIdx.x; q < P2; q += THREADS) {
+                    const int c = q < nslots ? column(q, b0, b1) : cols;
+                    lr[q] = c < cols ? __ldcg(lastrot + c) : -1;
+                    if (c < cols && lr[q] >= t0 - T) hot = 1;
                 }
-                if (!__syncthreads_or(hot)) {
-                    now += msteps;
-                    continue;
-                }
+                if (!__syncthreads_or(hot)) continue;
                 for (int e = threadIdx.x; e < nslots * rows; e += THREADS) {
                     const int q = e / rows, i = e - q * rows;
                     const int c = column(q, b0, b1);
-                    sm[(size_t)q * lds + i] = c < cols ? Lg[(size_t)c * ldg + i] : 0.0;
+                    sm[(size_t)q * lds + i] = c < cols ? __ldcg(Lg + (size_t)c * ldg + i) : 0.0;
                 }
                 __syncthreads();
+                int now = t0;
                 if (rnd == 0) {
                     // round-robin over the B columns of each block, B / 2
                     // pairs per block and step (groups B / 2 .. B - 1 take
                     // block b1, idle at the bye)
                     const int q = gw % (B / 2), off = gw < B / 2 ? 0 : B;
-                    for (int step = 0; step < B - 1; ++step) {
+                    for (int step = 0; step < B - 1; ++step, ++now) {
                         int u = q - 1 + step, v = B - 2 - q + step;
                         if (u >= B - 1) u -= B - 1;
                         if (v >= B - 1) v -= B - 1;
                         const int a = off + (q == 0 ? 0 : 1 + u), b = off + 1 + v;
-                        const int ca = column(a, b0, b1), cb = column(b, b0, b1);
-                        const bool valid = (off == 0 || !bye) && ca < cols &&
-                                           cb < cols &&
-                                           !jacobi_unchanged(lastrot, ca, cb, now - T);
+                        const bool valid = (off == 0 || !bye) &&
+                                           column(a, b0, b1) < cols &&
+                                           column(b, b0, b1) < cols &&
+                                           !jacobi_unchanged(lr, a, b, now - T);
                         if (__any_sync(0xffffffffu, valid)) {
                             const bool rot = jacobi_rotate<G, E>(
                                 sm + (size_t)a * lds, sm + (size_t)b * lds, rows,
                                 gl, valid, eps2);
-                            if (rot && gl == 0) lastrot[ca] = lastrot[cb] = now;
+                            if (rot && gl == 0) lr[a] = lr[b] = now;
                             any |= rot;
                         }
                         __syncthreads();
-                        ++now;
                     }
                 }
                 if (!bye) {
                     // the cross pairs: slot gw with slot B + (gw + step) mod B
-                    for (int step = 0; step < B; ++step) {
+                    for (int step = 0; step < B; ++step, ++now) {
                         const int a = gw, b = B + (gw + step) % B;
-                        const int ca = column(a, b0, b1), cb = column(b, b0, b1);
-                        const bool valid = ca < cols && cb < cols &&
-                                           !jacobi_unchanged(lastrot, ca, cb, now - T);
+                        const bool valid = column(a, b0, b1) < cols &&
+                                           column(b, b0, b1) < cols &&
+                                           !jacobi_unchanged(lr, a, b, now - T);
                         if (__any_sync(0xffffffffu, valid)) {
                             const bool rot = jacobi_rotate<G, E>(
                                 sm + (size_t)a * lds, sm + (size_t)b * lds, rows,
                                 gl, valid, eps2);
-                            if (rot && gl == 0) lastrot[ca] = lastrot[cb] = now;
+                            if (rot && gl == 0) lr[a] = lr[b] = now;
                             any |= rot;
                         }
                         __syncthreads();
-                        ++now;
                     }
                 }
                 for (int e = threadIdx.x; e < nslots * rows; e += THREADS) {
@@ -1443,48 +1449,67 @@ k_jacobi_block(TileWork *__restrict__ tiles, Workspace ws)
                     const int c = column(q, b0, b1);
                     if (c < cols) Lg[(size_t)c * ldg + i] = sm[(size_t)q * lds + i];
                 }
+                for (int q = threadIdx.x; q < nslots; q += THREADS) {
+                    const int c = column(q, b0, b1);
+                    if (c < cols) lastrot[c] = lr[q];
+                }
                 __syncthreads();
             }
+            // the round's columns and times, visible to the whole cluster
+            cl.sync();
         }
-        if (any) rotated[sweep & 1] = 1;
-        if (threadIdx.x == 0) rotated[(sweep + 1) & 1] = 0;
-        __syncthreads();
-        if (!rotated[sweep & 1]) break;
+        if (any) rot0[sweep & 1] = 1;
+        if (crank == 0 && threadIdx.x == 0) rotated[(sweep + 1) & 1] = 0;
+        cl.sync();
+        if (!rot0[sweep & 1]) break;
     }
-    // Normalise into W = T(slot); squared norms into Sig.
+    // every CTA has read the first CTA's flag before any of them exits
+    cl.sync();
+    // Normalise into W = T(slot); squared norms into Sig (over lastrot).
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     double *W = ws.T(s);
     double *sig = ws.Sig(s);
-    for (int c = warp; c < cols; c += THREADS / 32) {
+    for (int c = crank * (THREADS / 32) + warp; c < cols;
+         c += csize * (THREADS / 32)) {
         const double *ca = Lg + (size_t)c * ldg;
         double nrm = 0.0;
-        for (int i = lane; i < rows; i += 32) nrm = fma(ca[i], ca[i], nrm);
+        for (int i = lane; i < rows; i += 32) {
+            const double x = __ldcg(ca + i);
+            nrm = fma(x, x, nrm);
+        }
         #pragma unroll
         for (int o = 16; o > 0; o >>= 1) nrm += __shfl_xor_sync(0xffffffffu, nrm, o);
         const double inv = nrm > 0.0 ? 1.0 / sqrt(nrm) : 0.0;
-        for (int i = lane; i < rows; i += 32) W[(size_t)c * ldg + i] = ca[i] * inv;
+        for (int i = lane; i < rows; i += 32) W[(size_t)c * ldg + i] = __ldcg(ca + i) * inv;
         if (lane == 0) sig[c] = nrm;
     }
-    if (threadIdx.x == 0) {
+    if (crank == 0 && threadIdx.x == 0) {
         tw.sweeps = sweep;
         if (sweep >= 40) tw.status |= TILE_JACOBI_SLOW;
     }
 }
 
-#ifndef JACOBI_BLOCK_THREADS
-#define JACOBI_BLOCK_THREADS 512
-#endif
-
 template <int CLASS, int G, int E>
 static void jacobi_block_launch(TileWork *d_tiles, int ntiles, Workspace ws,
                                 int max_rows, cudaStream_t stream)
 {
-    constexpr int THREADS = JACOBI_BLOCK_THREADS;
-    auto *fn = k_jacobi_block<CLASS, G, E, THREADS>;
-    const size_t smem = (size_t)2 * (THREADS / G) * (max_rows | 1) * sizeof(double);
+    auto *fn = k_jacobi_block<CLASS, G, E>;
+    const size_t smem = (size_t)2 * (512 / G) * (max_rows | 1) * sizeof(double);
     cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
-    fn<<<ntiles, THREADS, smem, stream>>>(d_tiles, ws);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)ntiles * kJacobiCluster);
+    cfg.blockDim = dim3(512);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = kJacobiCluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, fn, d_tiles, ws);
 }
 
 template <int CLASS, int G, int E, int THREADS, bool SMEM>

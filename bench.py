@@ -970,6 +970,58 @@ def reference_arm(args, key, wl, threads):
                 "d2h_bytes_per_step": 0}}))
 
 
+def run_single(args):
+    """One approximation (or one C4 batched call) with the chosen engine;
+    prints its phase times as one JSON line.  No warm-up, no comparison:
+    a program for launch lists and ncu captures."""
+    import starsh_b200 as sb
+    lib = sb.load()
+    engine = sb.ENGINE_FP64 if args.engine == "fp64" else sb.ENGINE_MIXED
+    if args.workload == "c4-batch":
+        handle = sb.KERNEL(lambda *a: None)
+        _keep.append(handle)
+        assert lib.starsh_b200_kernel_register(
+            c_void_p(ctypes.cast(handle, c_void_p).value), sb.FAMILY["coulomb"],
+            1.0) == 0
+        lib.starsh_set_oversample(str(C4["oversample"]).encode())
+        probs = build_mixed(lib, c4_specs(), handle, tune=args.tune)
+        n = len(probs)
+        ranks = (ctypes.c_int * n)(*[p["maxrank"] for p in probs])
+        tols = (ctypes.c_double * n)(*[p["tol"] for p in probs])
+        Fs = (POINTER(sb.Blrf) * n)(*[new_format(lib, p) for p in probs])
+        Ms = (POINTER(sb.Blrm) * n)()
+        assert lib.starsh_b200_approximate_batch(n, Ms, Fs, ranks, tols, None,
+                                                 engine, 0) == 0
+    else:
+        wl = dict(WORKLOADS[args.workload])
+        if args.n:
+            wl["N"] = args.n
+        lib.starsh_set_oversample(str(wl["oversample"]).encode())
+        prob = make_problem(lib, wl)
+        F = new_format(lib, prob)
+        M = POINTER(sb.Blrm)()
+        assert lib.starsh_b200_approximate(byref(M), F, wl["maxrank"], wl["tol"],
+                                           0, engine, 0) == 0
+        if args.products:
+            # TLR products B = M A on the device, nrhs of the workload (64
+            # when it names none)
+            import torch
+            nrhs = wl.get("dmml_nrhs", 64)
+            A = torch.randn(nrhs, wl["N"], dtype=torch.float64, device="cuda")
+            B = torch.zeros(nrhs, wl["N"], dtype=torch.float64, device="cuda")
+            for _ in range(args.products):
+                assert lib.starsh_b200_blrm_dmml_device(
+                    M, nrhs, 1.0, A.data_ptr(), wl["N"], 0.0, B.data_ptr(),
+                    wl["N"], None) == 0
+            torch.cuda.synchronize()
+    st = sb.stats(lib)
+    print(json.dumps({"workload": args.workload, "engine": args.engine,
+                      "total_ms": st.total_ms, "gen_ms": st.gen_ms,
+                      "basis_ms": st.basis_ms, "project_ms": st.project_ms,
+                      "svd_ms": st.svd_ms, "output_ms": st.output_ms,
+                      "launches": int(st.kernel_launches)}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -993,8 +1045,17 @@ def main():
                     help="c2-* / c3-*: add the sketch precision study to the line")
     ap.add_argument("--no-cpu", action="store_true",
                     help="skip the CPU baseline leg")
+    ap.add_argument("--single", action="store_true",
+                    help="one approximation of the workload (c4-batch: one "
+                         "batched call) and its phase times, nothing else: "
+                         "the program profiles are taken on")
+    ap.add_argument("--products", type=int, default=0,
+                    help="--single: then this many TLR products on the device")
     ap.add_argument("--_cpu-run", type=int, default=0, dest="cpu_run")
     args = ap.parse_args()
+    if args.single:
+        run_single(args)
+        return
     key = args.workload
     if args.cpu_run:
         if key in ("c4-batch", "c5-serve"):

@@ -1317,7 +1317,7 @@ k_jacobi(TileWork *__restrict__ tiles, Workspace ws)
 // repeat until one rotates nothing.
 //
 // The meetings of one round touch disjoint blocks, so a tile is taken by a
-// cluster of kJacobiCluster CTAs that share each round's meetings and meet
+// cluster of CTAs (jacobi_cluster()) that share each round's meetings and meet
 // at a cluster barrier between rounds (which also publishes the round's
 // columns in global memory): a tile's latency, which is what bounds the
 // batches that hold few such tiles, drops by up to that factor.  Times
@@ -1329,7 +1329,19 @@ k_jacobi(TileWork *__restrict__ tiles, Workspace ws)
 // normalisation overwrites it at the end), each meeting works on its own
 // copy of its columns' entries.  Data another CTA of the cluster wrote is
 // read past L1 (__ldcg).
-constexpr int kJacobiCluster = 4;
+constexpr int kJacobiClusterMax = 8;
+
+// CTAs per tile (STARSH_B200_JACOBI_CLUSTER, 1 .. 8, default 4).
+static int jacobi_cluster()
+{
+    static const int cs = [] {
+        int v = 4;
+        if (const char *e = getenv("STARSH_B200_JACOBI_CLUSTER"))
+            v = std::max(1, std::min(kJacobiClusterMax, atoi(e)));
+        return v;
+    }();
+    return cs;
+}
 
 template <int CLASS, int G, int E>
 __global__ void __launch_bounds__(512, 1)
@@ -1498,13 +1510,14 @@ static void jacobi_block_launch(TileWork *d_tiles, int ntiles, Workspace ws,
     cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)ntiles * kJacobiCluster);
+    const int cs = jacobi_cluster();
+    cfg.gridDim = dim3((unsigned)(ntiles * cs));
     cfg.blockDim = dim3(512);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = stream;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = kJacobiCluster;
+    attr[0].val.clusterDim.x = cs;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;

@@ -1317,7 +1317,7 @@ k_jacobi(TileWork *__restrict__ tiles, Workspace ws)
 // repeat until one rotates nothing.
 //
 // The meetings of one round touch disjoint blocks, so a tile is taken by a
-// cluster of CTAs (jacobi_cluster()) that share each round's meetings and meet
+// cluster of CTAs (jacobi_cluster) that share each round's meetings and meet
 // at a cluster barrier between rounds (which also publishes the round's
 // columns in global memory): a tile's latency, which is what bounds the
 // batches that hold few such tiles, drops by up to that factor.  Times
@@ -1331,16 +1331,19 @@ k_jacobi(TileWork *__restrict__ tiles, Workspace ws)
 // read past L1 (__ldcg).
 constexpr int kJacobiClusterMax = 8;
 
-// CTAs per tile (STARSH_B200_JACOBI_CLUSTER, 1 .. 8, default 4).
-static int jacobi_cluster()
+// CTAs per tile: 4 for the classes above 256 rows, 2 below (measured: a
+// cluster of 4 shortens the large classes most, the 193..256-row class
+// gains from 2 and loses SMs to the shared-memory classes beside it at 4);
+// STARSH_B200_JACOBI_CLUSTER (1 .. 8) sets one size for all.
+static int jacobi_cluster(int cls)
 {
-    static const int cs = [] {
-        int v = 4;
+    static const int forced = [] {
+        int v = 0;
         if (const char *e = getenv("STARSH_B200_JACOBI_CLUSTER"))
             v = std::max(1, std::min(kJacobiClusterMax, atoi(e)));
         return v;
     }();
-    return cs;
+    return forced ? forced : cls >= 7 ? 4 : 2;
 }
 
 template <int CLASS, int G, int E>
@@ -1510,7 +1513,7 @@ static void jacobi_block_launch(TileWork *d_tiles, int ntiles, Workspace ws,
     cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
     cudaLaunchConfig_t cfg = {};
-    const int cs = jacobi_cluster();
+    const int cs = jacobi_cluster(CLASS);
     cfg.gridDim = dim3((unsigned)(ntiles * cs));
     cfg.blockDim = dim3(512);
     cfg.dynamicSmemBytes = smem;

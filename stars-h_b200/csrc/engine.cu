@@ -123,8 +123,23 @@ Context *context()
     return &g_ctx;
 }
 
+// Private contexts of finished workers (streams and grown buffers), kept
+// for the next ones: a new server's workers start warm.
+static std::mutex g_idle_mu;
+static std::vector<Context *> g_idle_ctx;
+constexpr size_t kIdleContexts = 8;
+
 Context *context_new_private()
 {
+    {
+        std::lock_guard<std::mutex> g(g_idle_mu);
+        if (!g_idle_ctx.empty()) {
+            Context *c = g_idle_ctx.back();
+            g_idle_ctx.pop_back();
+            cudaSetDevice(c->device);
+            return c;
+        }
+    }
     Context *base = nullptr;
     {
         Context *saved = t_ctx;
@@ -153,6 +168,13 @@ void context_free_private(Context *c)
     cudaStreamSynchronize(c->stream);
     cudaStreamSynchronize(c->side);
     cudaStreamSynchronize(c->copy);
+    {
+        std::lock_guard<std::mutex> g(g_idle_mu);
+        if (g_idle_ctx.size() < kIdleContexts) {
+            g_idle_ctx.push_back(c);
+            return;
+        }
+    }
     c->workspace.release();
     c->tiles.release();
     c->descs.release();

@@ -104,7 +104,11 @@ __device__ __forceinline__ double gen_entries(
     }
     double ss = 0.0;
     amax = 0.0;
-    #pragma unroll kGenUnroll
+    // the Matern entry (series or table per entry) keeps the shorter
+    // unroll: eight of its bodies cost more registers than they save
+    constexpr int kUnroll =
+        FAM == FAM_MATERN || FAM == FAM_MATERN2 ? 4 : kGenUnroll;
+    #pragma unroll kUnroll
     for (int jj = jj0; jj < jn; jj += 4) {
         double dist = 0.0;
         if constexpr (NDIM > 0) {

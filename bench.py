@@ -1352,6 +1352,26 @@ def main():
     }
     if dmml:
         line["dmml"] = dmml
+    # the other large kernels of the step, each against its own bound:
+    # the generator writes D once (8 B per entry; its limit is FP64 issue),
+    # the projection B = Q^T D is an FP64 DMMA contraction
+    if chosen == sb.ENGINE_MIXED and last.gen_ms > 0 and last.project_ms > 0:
+        dgemm = dmml["dgemm_tflops_in_run"] if dmml else fp64_peak_tflops(torch)
+        hbm_peak, hbm_src = measured_hbm_gbs()
+        gen_entries = float(last.entries)
+        line["rooflines_other"] = {
+            "generation (k_gen_tiles)": {
+                "bound": "fp64 issue (an exp or Bessel evaluation per entry)",
+                "entries_per_s": gen_entries / (last.gen_ms / 1e3),
+                "d_write_gbs": 8.0 * gen_entries / (last.gen_ms / 1e3) / 1e9,
+                "frac_of_hbm": 8.0 * gen_entries / (last.gen_ms / 1e3) / 1e9 / hbm_peak,
+                "hbm_peak_source": hbm_src},
+            "projection (k_gemm_f64 TN, B = Q^T D)": {
+                "bound": "tensor (FP64 DMMA)",
+                "achieved_tflops": last.project_flops / (last.project_ms / 1e3) / 1e12,
+                "peak_tflops": dgemm,
+                "frac": last.project_flops / (last.project_ms / 1e3) / 1e12 / dgemm,
+                "peak_source": "cuBLAS DGEMM 4096^3 measured in this run"}}
     if args.precision_study and (key.startswith("c3") or key.startswith("c2")):
         line["precision_study"] = precision_study(lib, wl, prob, torch)
     if world == 1 and not args.no_cpu:

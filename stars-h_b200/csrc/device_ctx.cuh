@@ -12,8 +12,11 @@ namespace b200 {
 struct DeviceBuffer {
     void *ptr = nullptr;
     size_t bytes = 0;
-    // Ensures capacity; contents are not preserved.  Returns false on OOM.
-    bool reserve(size_t need);
+    cudaStream_t stream = nullptr;   // the stream it was allocated on
+    // Ensures capacity, stream-ordered on s (from the device's cached
+    // pool: growing never synchronises the device); contents are not
+    // preserved.  Returns false on OOM.
+    bool reserve(size_t need, cudaStream_t s);
     void release();
 };
 

@@ -34,23 +34,25 @@ namespace b200 {
 
 // --------------------------------------------------------------- context
 
-bool DeviceBuffer::reserve(size_t need)
+bool DeviceBuffer::reserve(size_t need, cudaStream_t s)
 {
     if (need <= bytes) return true;
-    release();
-    if (cudaMalloc(&ptr, need) != cudaSuccess) {
+    if (ptr) cudaFreeAsync(ptr, s);
+    ptr = nullptr;
+    bytes = 0;
+    if (cudaMallocAsync(&ptr, need, s) != cudaSuccess) {
         cudaGetLastError();
         ptr = nullptr;
-        bytes = 0;
         return false;
     }
     bytes = need;
+    stream = s;
     return true;
 }
 
 void DeviceBuffer::release()
 {
-    if (ptr) cudaFree(ptr);
+    if (ptr) cudaFreeAsync(ptr, stream);
     ptr = nullptr;
     bytes = 0;
 }
@@ -601,7 +603,7 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
         set_error("maxrank + oversample above 1024 is not supported");
         return STARSH_WRONG_PARAMETER;
     }
-    if (!ctx.kernels.reserve(kernels.size() * sizeof(DevKernel)))
+    if (!ctx.kernels.reserve(kernels.size() * sizeof(DevKernel), s))
         return cuda_fail(cudaErrorMemoryAllocation, "kernel table");
     B200_CUDA(cudaMemcpyAsync(ctx.kernels.ptr, kernels.data(),
                               kernels.size() * sizeof(DevKernel),
@@ -610,7 +612,7 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
     // Gaussian sketch, shared by every tile (as the reference reuses the
     // same iseed for every block): n_max x k_max, ld n_max.
     if (ctx.omega_rows != n_max || ctx.omega_cols != k_max) {
-        if (!ctx.omega.reserve((size_t)n_max * k_max * sizeof(double)))
+        if (!ctx.omega.reserve((size_t)n_max * k_max * sizeof(double), s))
             return cuda_fail(cudaErrorMemoryAllocation, "omega");
         launch_gaussian((double *)ctx.omega.ptr, n_max, k_max, n_max,
                         kOmegaSeed, s);
@@ -627,7 +629,7 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
     const int ld_om8 = (n_max + 63) / 64 * 64;
     if (use_i8 && (ctx.omega8_rows != n_max || ctx.omega8_cols != k_max ||
                    ctx.omega8_ld != ld_om8)) {
-        if (!ctx.omega8.reserve((size_t)ld_om8 * k_max))
+        if (!ctx.omega8.reserve((size_t)ld_om8 * k_max, s))
             return cuda_fail(cudaErrorMemoryAllocation, "omega8");
         launch_gaussian_i8((int8_t *)ctx.omega8.ptr, n_max, k_max, ld_om8,
                            kOmegaSeed, s);
@@ -710,11 +712,11 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
         max_slots = std::max<long long>(max_slots, nt);
         b0 += nt;
     }
-    if (!ctx.workspace.reserve(ws_need))
+    if (!ctx.workspace.reserve(ws_need, s))
         return cuda_fail(cudaErrorMemoryAllocation, "workspace");
-    if (!ctx.tiles.reserve((size_t)max_slots * sizeof(TileWork)) ||
-        !ctx.descs.reserve((size_t)max_slots * sizeof(GemmDesc)) ||
-        !ctx.flag.reserve(256))
+    if (!ctx.tiles.reserve((size_t)max_slots * sizeof(TileWork), s) ||
+        !ctx.descs.reserve((size_t)max_slots * sizeof(GemmDesc), s) ||
+        !ctx.flag.reserve(256, s))
         return cuda_fail(cudaErrorMemoryAllocation, "batch arrays");
     Workspace ws{};
     TileWork *dt = (TileWork *)ctx.tiles.ptr;
@@ -933,9 +935,8 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
         if ((info = gemm(STEP_PROJECT, true, false, nt, k_max, plan[pi].n, none))) break;
         cudaEventRecord(ev[3], s);
         if ((info = gemm(STEP_GRAM_B, false, true, nt, k_max, k_max, none))) break;
-        launch_pivchol(2, dt, dt, nt, ws, s);
-        launch_jacobi(dt, nt, ws, s, ctx.side);
-        count_launch(2);
+        count_launch(launch_pivchol(2, dt, dt, nt, ws, s));
+        count_launch(launch_jacobi(dt, nt, ws, s, ctx.side));
         if ((info = gemm(STEP_ROTATE, true, false, nt, k_max, plan[pi].n, none))) break;
         launch_rank_cut(dt, nt, ws, s);
         count_launch();

@@ -148,14 +148,15 @@ void make_gemm_descs(GemmStep step, const TileWork *d_tiles, int ntiles,
 void launch_gen_tiles(const DevKernel *d_kernels, const TileWork *d_tiles,
                       int ntiles, Workspace ws, cudaStream_t stream,
                       int need = 0);
-void launch_pivchol(int phase, const TileWork *d_tiles, TileWork *d_tiles_rw,
-                    int ntiles, Workspace ws, cudaStream_t s);
+// launch_pivchol and launch_jacobi return the number of kernels launched.
+int launch_pivchol(int phase, const TileWork *d_tiles, TileWork *d_tiles_rw,
+                   int ntiles, Workspace ws, cudaStream_t s);
 void launch_gather_cols(int phase, const TileWork *d_tiles, int ntiles,
                         Workspace ws, cudaStream_t stream);
 void launch_chol_inv(int phase, TileWork *d_tiles, int ntiles, Workspace ws,
                      cudaStream_t stream);
-void launch_jacobi(TileWork *d_tiles, int ntiles, Workspace ws,
-                   cudaStream_t stream, cudaStream_t side);
+int launch_jacobi(TileWork *d_tiles, int ntiles, Workspace ws,
+                  cudaStream_t stream, cudaStream_t side);
 void launch_rank_cut(TileWork *d_tiles, int ntiles, Workspace ws,
                      cudaStream_t stream);
 void launch_merge_basis(TileWork *d_tiles, int ntiles, cudaStream_t stream);

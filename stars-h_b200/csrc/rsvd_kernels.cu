@@ -19,6 +19,7 @@
 //     decides the rank is exact to FP64 rounding even where the Gram's
 //     eigenvalues are not.
 #include <cfloat>
+#include <climits>
 #include <cooperative_groups.h>
 #include "engine.cuh"
 
@@ -672,6 +673,11 @@ __device__ double block_sum(double x, double *red)
 enum : int { PH_A = 0, PH_B = 1, PH_H = 2, PH_R = 3, PH_R2 = 4 };
 
 constexpr int kSmallThreads = 256;
+#ifndef PIVCHOL_H_LANES
+#define PIVCHOL_H_LANES 4
+#endif
+constexpr int kPivcholLanes = PIVCHOL_H_LANES;   // lanes per row, large phase-H factors
+constexpr int kPivcholSplit = 128;               // "large": more rows than this
 constexpr int kMaxK = 1024;   // largest sketch width handled by one CTA
 
 // Left-looking pivoted Cholesky of the Gram in S(slot) (dimension nn):
@@ -679,8 +685,15 @@ constexpr int kMaxK = 1024;   // largest sketch width handled by one CTA
 // (column j holds the multipliers of pivot j).  Stops when the largest
 // remaining diagonal entry is <= thr.  For the basis phases (A, B) the
 // pivot block R11 = L[piv, :]^T is inverted into T(slot).
-__global__ void __launch_bounds__(kSmallThreads)
-k_pivchol(TileWork *__restrict__ tiles, Workspace ws, int phase)
+//
+// LPR lanes share a row's update (the left-looking product with the
+// previous columns, read from L2): more loads in flight for the large
+// factors of phase H, whose few tiles per batch bound the launch.  Tiles
+// with nn outside [nn_lo, nn_hi] are left to another launch.
+template <int LPR>
+__global__ void __launch_bounds__(kSmallThreads * LPR)
+k_pivchol(TileWork *__restrict__ tiles, Workspace ws, int phase, int nn_lo,
+          int nn_hi)
 {
     TileWork &tw = tiles[blockIdx.x];
     const int s = tw.slot;
@@ -696,6 +709,7 @@ k_pivchol(TileWork *__restrict__ tiles, Workspace ws, int phase)
     else if (phase == PH_R) nn = tw.bcur;
     else if (phase == PH_R2) nn = tw.need_pass_b ? tw.bcur : 0;
     else nn = tw.k;
+    if (nn < nn_lo || nn > nn_hi) return;   // another launch's tile
     if ((phase == PH_B && !tw.need_pass_b) ||
         ((phase == PH_R || phase == PH_R2) && nn <= 0)) {
         if (threadIdx.x == 0) {
@@ -808,6 +822,7 @@ k_pivchol(TileWork *__restrict__ tiles, Workspace ws, int phase)
             piv[j] = p;
             used[p] = 1;
         }
+        if constexpr (LPR == 1) {
         for (int i = threadIdx.x; i < nn; i += blockDim.x) {
             double v;
             if (i == p) {
@@ -831,6 +846,40 @@ k_pivchol(TileWork *__restrict__ tiles, Workspace ws, int phase)
                 dg[i] -= v * v;
             }
             L[(size_t)j * ld + i] = v;
+        }
+        } else {
+        // lane q of a row's group sums l = q, q + LPR, ... (two chains);
+        // the block-uniform row loop keeps every lane in the shuffles
+        const int q = threadIdx.x % LPR;
+        for (int i0 = 0; i0 < nn; i0 += blockDim.x / LPR) {
+            const int i = i0 + threadIdx.x / LPR;
+            const bool live = i < nn && i != p && !used[i];
+            double a0 = 0.0, a1 = 0.0;
+            if (live) {
+                int l = q;
+                for (; l + LPR < j; l += 2 * LPR) {
+                    a0 = fma(L[(size_t)l * ld + i], lp[l], a0);
+                    a1 = fma(L[(size_t)(l + LPR) * ld + i], lp[l + LPR], a1);
+                }
+                for (; l < j; l += LPR) a0 = fma(L[(size_t)l * ld + i], lp[l], a0);
+            }
+            double part = a0 + a1;
+            #pragma unroll
+            for (int o = LPR / 2; o > 0; o >>= 1)
+                part += __shfl_xor_sync(0xffffffffu, part, o);
+            if (i < nn && q == 0) {
+                double v;
+                if (i == p) {
+                    v = sp;
+                } else if (used[i]) {
+                    v = 0.0;
+                } else {
+                    v = (G[(size_t)p * ld + i] - part) / sp;
+                    dg[i] -= v * v;
+                }
+                L[(size_t)j * ld + i] = v;
+            }
+        }
         }
         __syncthreads();
     }
@@ -870,8 +919,8 @@ k_pivchol(TileWork *__restrict__ tiles, Workspace ws, int phase)
 void launch_round_pivchol(TileWork *d_tiles, int ntiles, Workspace ws,
                           int repeat, cudaStream_t stream)
 {
-    k_pivchol<<<ntiles, kSmallThreads, 0, stream>>>(d_tiles, ws,
-                                                    repeat ? PH_R2 : PH_R);
+    k_pivchol<1><<<ntiles, kSmallThreads, 0, stream>>>(
+        d_tiles, ws, repeat ? PH_R2 : PH_R, 0, INT_MAX);
 }
 
 // ||D||_F^2 of every block from the generator's per-CTA partial sums, in a
@@ -958,10 +1007,21 @@ void launch_round_end(TileWork *d_tiles, int ntiles, int verify,
                                                           verify);
 }
 
-void launch_pivchol(int phase, const TileWork *, TileWork *d_tiles_rw,
+int launch_pivchol(int phase, const TileWork *, TileWork *d_tiles_rw,
                     int ntiles, Workspace ws, cudaStream_t s)
 {
-    k_pivchol<<<ntiles, kSmallThreads, 0, s>>>(d_tiles_rw, ws, phase);
+    if (phase == PH_H && kPivcholLanes > 1) {
+        // small factors one lane per row, large ones kPivcholLanes
+        k_pivchol<1><<<ntiles, kSmallThreads, 0, s>>>(d_tiles_rw, ws, phase, 0,
+                                                      kPivcholSplit);
+        k_pivchol<kPivcholLanes><<<ntiles, kSmallThreads * kPivcholLanes, 0, s>>>(
+            d_tiles_rw, ws, phase, kPivcholSplit + 1, INT_MAX);
+        return 2;
+    } else {
+        k_pivchol<1><<<ntiles, kSmallThreads, 0, s>>>(d_tiles_rw, ws, phase, 0,
+                                                      INT_MAX);
+        return 1;
+    }
 }
 
 // Gathers the pivot columns of Y into the Q buffer (phase A) or the Q1
@@ -1543,8 +1603,8 @@ static void jacobi_class_launch(TileWork *d_tiles, int ntiles, Workspace ws,
     fn<<<ntiles, THREADS, SMEM ? smem : 0, stream>>>(d_tiles, ws);
 }
 
-void launch_jacobi(TileWork *d_tiles, int ntiles, Workspace ws,
-                   cudaStream_t stream, cudaStream_t side)
+int launch_jacobi(TileWork *d_tiles, int ntiles, Workspace ws,
+                  cudaStream_t stream, cudaStream_t side)
 {
     // Classes a batch can reach, from the largest factor it may hold
     // (k1, k2 <= k_max).  Shared memory is sized for the class's largest
@@ -1606,6 +1666,8 @@ void launch_jacobi(TileWork *d_tiles, int ntiles, Workspace ws,
         cudaEventDestroy(fork);
         cudaEventDestroy(join);
     }
+    return 1 + (kmax > 32) + (kmax > 64) + 2 * (kmax > 128) + 2 * (kmax > 192) +
+           (kmax > 256) + (kmax > 288) + (kmax > 320) + (kmax > 512);
 }
 
 // Appends the residual-pass columns to the basis: k1 += kb.

@@ -36,6 +36,7 @@ struct Context {
     DeviceBuffer omega8;       // int8 sketch matrix of the adaptive engine
     int omega8_rows = 0, omega8_cols = 0, omega8_ld = 0;
     int omega_rows = 0, omega_cols = 0;   // shape Omega was generated for
+    size_t workspace_cap = (size_t)-1;    // most workspace one batch may use
     std::mutex lock;           // one approximation / dmml at a time
 };
 

@@ -152,6 +152,13 @@ Context *context_new_private()
     if (base == nullptr) return nullptr;
     Context *c = new Context();
     c->device = base->device;
+    // a serving worker's batches stay at most this large (several workers
+    // share the device; batches of this size already fill it), so its
+    // workspace is reserved once, at the start
+    size_t cap_mb = 8192;
+    if (const char *e = getenv("STARSH_B200_SERVER_WORKSPACE_MB"))
+        cap_mb = (size_t)std::max(64LL, atoll(e));
+    c->workspace_cap = cap_mb << 20;
     cudaSetDevice(c->device);
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess ||
@@ -679,6 +686,7 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
     size_t budget = std::min<size_t>(free_b / 2, (size_t)24 << 30);
     if (const char *e = getenv("STARSH_B200_WORKSPACE_MB"))
         budget = std::min<size_t>(budget, (size_t)atoll(e) << 20);
+    budget = std::min(budget, ctx.workspace_cap);
     // Batch plan: each batch takes as many tiles as fit the budget with
     // the layout of its largest dimensions (at most 4096).
     struct BatchPlan { long long b0; int nt; int m, n, k; size_t stride; };

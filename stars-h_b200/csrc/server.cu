@@ -117,6 +117,15 @@ static void worker_loop(starsh_b200_server *sv)
     // this worker's engine context (the shared one if it cannot be made)
     Context *own = context_new_private();
     set_thread_context(own);
+    // the worker's batch workspace, once, before it serves (growing it
+    // while serving would map new memory in the middle of requests)
+    if (own != nullptr && own->workspace_cap != (size_t)-1) {
+        size_t free_b = 0, total_b = 0;
+        cudaMemGetInfo(&free_b, &total_b);
+        const size_t want = std::min(own->workspace_cap, free_b / 4);
+        if (own->workspace.reserve(want, own->stream))
+            cudaStreamSynchronize(own->stream);
+    }
     for (;;) {
         std::vector<Request *> group;
         double group_estimate = 0.0;

@@ -617,6 +617,12 @@ def run_c5(args, lib, clocks):
                    "hbm_budget_bytes": C5["budget"], "engine": "mixed, continuous batching"},
         "latency_ms": pct(lat),
         "latency_ms_N_ge_32768": pct(lat[big]) if big.any() else None,
+        "slowest_requests": [
+            {"n": int(reqs[i]["n"]), "nb": int(reqs[i]["nb"]),
+             "kernel": reqs[i]["kernel"],
+             "ndim": int(reqs[i]["ndim"]), "tol": reqs[i]["tol"],
+             "arrival_s": float(reqs[i]["t"]), "latency_ms": float(lat[i])}
+            for i in np.argsort(lat)[::-1][:8]],
         "single_request_floor_ms": floor,
         "floor_what": "one 2-D square-exponential request (tol 1e-4, 32 matvecs) alone on an idle one-worker server that served it before (best of 3 after a first), by N",
         "served_rps": len(reqs) / wall, "groups": int(st.groups),

@@ -334,22 +334,27 @@ void fill_kernel(DevKernel &K, const b200_kspec &sp)
 }
 
 // Chebyshev coefficients of G(x) = x^nu e^x K_nu(x) on each interval
-// [2^(q+1), 2^(q+2)] (one CTA per interval): G at the kMaternTabDeg + 1
-// Chebyshev points of the first kind u_j = cos(pi (j + 1/2) / (deg + 1)),
-// x_j = 2^q (u_j + 3), then c_k = 2 / (deg + 1) sum_j G(x_j)
-// cos(pi k (j + 1/2) / (deg + 1)), c_0 halved (the discrete cosine
-// transform of Chebyshev interpolation).  The interpolant is accurate to
-// a few units of 1e-15 relative on every interval (G is analytic in the
-// right half-plane, the nearest singularity is at x = 0).
+// [2^E, 2^(E+1)], E = q + kMaternTabEmin (one CTA per interval q): G at
+// the kMaternTabDeg + 1 Chebyshev points of the first kind u_j = cos(pi
+// (j + 1/2) / (deg + 1)), x_j = 2^(E-1) (u_j + 3), then c_k = 2 / (deg + 1)
+// sum_j G(x_j) cos(pi k (j + 1/2) / (deg + 1)), c_0 halved (the discrete
+// cosine transform of Chebyshev interpolation).  Node values come from the
+// trapezoidal integral for x >= 2 and from Temme's series below.  The
+// interpolant is accurate to a few units of 1e-15 relative on every
+// interval (G is analytic in the right half-plane, the nearest
+// singularity is at x = 0).
 __global__ void k_matern_table(double nu, double *tab)
 {
     constexpr int N1 = kMaternTabDeg + 1;
     __shared__ double g[N1];
     const int q = blockIdx.x, j = threadIdx.x;
     if (j < N1) {
+        // node j of interval [2^E, 2^(E+1)), E = q + kMaternTabEmin
         const double u = cospi((j + 0.5) / N1);
-        const double x = ldexp(u + 3.0, q);
-        g[j] = exp(nu * log(x)) * bessel_k_large_scaled(nu, x, 2.0);
+        const double x = ldexp(u + 3.0, q + kMaternTabEmin - 1);
+        g[j] = x >= 2.0
+            ? exp(nu * log(x)) * bessel_k_large_scaled(nu, x, 2.0)
+            : exp(nu * log(x) + x) * bessel_knu(nu, x);
     }
     __syncthreads();
     if (j < N1) {

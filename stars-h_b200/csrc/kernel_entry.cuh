@@ -35,7 +35,8 @@ struct DevKernel {
     double matern_coef, matern_scale;
     int matern_half;          // 1, 2, 3 for nu = 1/2, 3/2, 5/2; else 0
     // Matérn with other nu: Chebyshev coefficients of x^nu e^x K_nu(x) on
-    // [2^(q+1), 2^(q+2)], q < kMaternTabIntervals (device, or null)
+    // [2^E, 2^(E+1)), kMaternTabEmin <= E < kMaternTabEmin +
+    // kMaternTabIntervals (device, or null)
     const double *matern_tab;
     double inv_neg_beta;      // -1/beta (exp)
     double inv_neg_2beta2;    // 1/((-2 beta) beta) (square exponential)
@@ -48,10 +49,15 @@ struct DevKernel {
     const long long *col_piv;
 };
 
-// Matérn table: kMaternTabIntervals dyadic intervals covering [2, 1024),
-// each with kMaternTabDeg + 1 Chebyshev coefficients.
+// Matérn table: kMaternTabIntervals dyadic intervals covering
+// [2^-10, 1024), each with kMaternTabDeg + 1 Chebyshev coefficients.  On
+// every interval [a, 2a) the function is analytic except at x = 0, which
+// lies at u = -3 of the interval's [-1, 1): the same Bernstein ellipse
+// (rho = 3 + 2 sqrt 2) at every scale, so one degree serves all of them.
 constexpr int kMaternTabDeg = 18;
-constexpr int kMaternTabIntervals = 9;
+constexpr int kMaternTabEmin = -10;
+constexpr int kMaternTabIntervals = 20;
+constexpr double kMaternTabLo = 0.0009765625;   // 2^kMaternTabEmin
 
 // Taylor coefficients of 1/Gamma(1+z) about z = 0 (a_0 = 1, a_1 = Euler's
 // gamma, ...), computed with mpmath at 50 digits by
@@ -183,13 +189,13 @@ __device__ inline double bessel_k_large(double nu, double x)
     return bessel_k_large_scaled(nu, x, 1.0) * exp(-x);
 }
 
-// x^nu e^x K_nu(x) for 2 <= x < 1024 from the problem's Chebyshev table:
-// x = 2^E m, m in [1, 2), lies in interval E - 1, at u = 2 m - 3 in
-// [-1, 1) (exact); Clenshaw's recurrence sums the series.
+// x^nu e^x K_nu(x) for 2^-10 <= x < 1024 from the problem's Chebyshev
+// table: x = 2^E m, m in [1, 2), lies in interval E - kMaternTabEmin, at
+// u = 2 m - 3 in [-1, 1) (exact); Clenshaw's recurrence sums the series.
 __device__ __forceinline__ double matern_tab_eval(const double *tab, double x)
 {
     const int E = (__double2hiint(x) >> 20) - 1023;
-    const double *c = tab + (size_t)(E - 1) * (kMaternTabDeg + 1);
+    const double *c = tab + (size_t)(E - kMaternTabEmin) * (kMaternTabDeg + 1);
     const double u = x * __hiloint2double((1024 - E) << 20, 0) - 3.0;
     const double u2 = 2.0 * u;
     double b1 = 0.0, b2 = 0.0;
@@ -269,7 +275,7 @@ __device__ __forceinline__ double entry_fam(const DevKernel &K, double dist,
         case 2: return K.sigma * ((1.0 + x) * exp(-x));
         case 3: return K.sigma * ((1.0 + x * (1.0 + x * (1.0 / 3.0))) * exp(-x));
         default:
-            if (K.matern_tab != nullptr && x >= 2.0) {
+            if (K.matern_tab != nullptr && x >= kMaternTabLo) {
                 // e^-x underflows to zero long before 1024
                 if (!(x < 1024.0)) return 0.0;
                 return K.matern_coef * (exp(-x) * matern_tab_eval(K.matern_tab, x));

@@ -81,7 +81,10 @@ enum STARSH_B200_ENGINE
 enum STARSH_B200_FLAGS
 {
     /* Copy factors and dense blocks to host memory before returning
-     * (the drop-in entry points always set it). */
+     * (the drop-in entry points always set it).  Each batch's factors are
+     * copied while later batches compute, into page-locked host blocks
+     * that the matrix owns; starsh_blrm_free returns them to the
+     * library's pool (STARSH_B200_PINNED_CACHE_MB of idle blocks kept). */
     STARSH_B200_HOST_MIRROR = 1,
 };
 

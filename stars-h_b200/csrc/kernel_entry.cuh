@@ -49,48 +49,6 @@ struct DevKernel {
     const long long *col_piv;
 };
 
-// e^v for the non-positive arguments of the decaying kernels, by the
-// reduction of W. J. Cody and W. Waite ("Software Manual for the
-// Elementary Functions", 1980): v = n ln2 + r, n = rint(v / ln2), |r| <=
-// ln2 / 2, r computed with ln2 split into a 32-bit head (n ln2_hi is exact
-// for |n| < 2^21) and its remainder; e^r by the Taylor series of degree 13
-// (truncation below 5e-18 relative on that interval) in Horner form, and
-// 2^n added to the exponent field.  Arguments below -708 (where 2^n would
-// leave the normal range) take CUDA's exp.  The split and the
-// coefficients 1/k! were computed with mpmath at 50 digits.
-#ifndef B200_OWN_EXP
-#define B200_OWN_EXP 0
-#endif
-__device__ __forceinline__ double exp_nonpos(double v)
-{
-#if B200_OWN_EXP
-    if (!(v >= -708.0)) return exp(v);
-    const double shift = 0x1.8p52;                    // 1.5 2^52
-    const double t = fma(v, 0x1.71547652b82fep+0, shift);
-    const int n = __double2loint(t);                   // rint(v log2 e)
-    const double dn = t - shift;
-    double r = fma(dn, -0x1.62e42ff000000p-1, v);
-    r = fma(dn, 0x1.718432a1b0e26p-35, r);
-    double p = 0x1.6124613a86d09p-33;
-    p = fma(p, r, 0x1.1eed8eff8d898p-29);
-    p = fma(p, r, 0x1.ae64567f544e4p-26);
-    p = fma(p, r, 0x1.27e4fb7789f5cp-22);
-    p = fma(p, r, 0x1.71de3a556c734p-19);
-    p = fma(p, r, 0x1.a01a01a01a01ap-16);
-    p = fma(p, r, 0x1.a01a01a01a01ap-13);
-    p = fma(p, r, 0x1.6c16c16c16c17p-10);
-    p = fma(p, r, 0x1.1111111111111p-7);
-    p = fma(p, r, 0x1.5555555555555p-5);
-    p = fma(p, r, 0x1.5555555555555p-3);
-    p = fma(p, r, 0.5);
-    p = fma(p, r, 1.0);
-    p = fma(p, r, 1.0);
-    return __hiloint2double(__double2hiint(p) + (n << 20), __double2loint(p));
-#else
-    return exp(v);
-#endif
-}
-
 // Matérn table: kMaternTabIntervals dyadic intervals covering
 // [2^-10, 1024), each with kMaternTabDeg + 1 Chebyshev coefficients.  On
 // every interval [a, 2a) the function is analytic except at x = 0, which
@@ -303,24 +261,24 @@ __device__ __forceinline__ double entry_fam(const DevKernel &K, double dist,
 {
     if constexpr (FAM == FAM_EXP) {
         const double v = sqrt(dist) * K.inv_neg_beta;
-        return v == 0.0 ? K.sigma + K.noise : K.sigma * exp_nonpos(v);
+        return v == 0.0 ? K.sigma + K.noise : K.sigma * exp(v);
     } else if constexpr (FAM == FAM_SQREXP) {
         const double v = dist * K.inv_neg_2beta2;
-        return v == 0.0 ? K.sigma + K.noise : K.sigma * exp_nonpos(v);
+        return v == 0.0 ? K.sigma + K.noise : K.sigma * exp(v);
     } else if constexpr (FAM == FAM_MATERN || FAM == FAM_MATERN2) {
         const double x = sqrt(dist) * K.matern_scale;
         if (x == 0.0) return K.sigma + K.noise;
         // nu = 1/2, 3/2, 5/2: 2^(1-nu)/Gamma(nu) x^nu K_nu(x) is
         // exp(-x) times 1, 1 + x, 1 + x + x^2/3 (K_{n+1/2} is elementary)
         switch (K.matern_half) {
-        case 1: return K.sigma * exp_nonpos(-x);
-        case 2: return K.sigma * ((1.0 + x) * exp_nonpos(-x));
-        case 3: return K.sigma * ((1.0 + x * (1.0 + x * (1.0 / 3.0))) * exp_nonpos(-x));
+        case 1: return K.sigma * exp(-x);
+        case 2: return K.sigma * ((1.0 + x) * exp(-x));
+        case 3: return K.sigma * ((1.0 + x * (1.0 + x * (1.0 / 3.0))) * exp(-x));
         default:
             if (K.matern_tab != nullptr && x >= kMaternTabLo) {
                 // e^-x underflows to zero long before 1024
                 if (!(x < 1024.0)) return 0.0;
-                return K.matern_coef * (exp_nonpos(-x) * matern_tab_eval(K.matern_tab, x));
+                return K.matern_coef * (exp(-x) * matern_tab_eval(K.matern_tab, x));
             }
             return K.matern_coef * pow(x, K.nu) * bessel_knu(K.nu, x);
         }

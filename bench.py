@@ -1347,7 +1347,11 @@ def main():
         "e2e": {"value": e2e_value, "unit": "Mentries/s",
                 "h2d_bytes_per_step": int(e2e_st.h2d_bytes),
                 "d2h_bytes_per_step": int(e2e_st.d2h_bytes),
-                "ms_per_step": t_e2e * 1e3},
+                "ms_per_step": t_e2e * 1e3,
+                "last_step_host_ms": {
+                    "whole_call": e2e_st.total_ms,
+                    "waiting_for_batch_downloads": e2e_st.mirror_wait_ms,
+                    "after_last_batch": e2e_st.finish_ms}},
         "gpu_launches": int(sum(s.kernel_launches for s in sts)),
         "phases_ms": {"generation": last.gen_ms, "fused_gen_sketch": last.fused_ms,
                       "sketch": last.sketch_ms, "basis": last.basis_ms,

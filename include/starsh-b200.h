@@ -355,6 +355,11 @@ typedef struct starsh_b200_stats
     double fused_bytes;       /* algorithmic HBM bytes of the fused
                                  kernel: D and the round-0 Y written     */
     long long resketch_tiles; /* tiles re-sketched from the stored D    */
+    double mirror_wait_ms;    /* host mirror: host time waiting, after the
+                                 last batch, for the batch downloads     */
+    double finish_ms;         /* host time from the last batch to return
+                                 (demotion, near blocks, host structure,
+                                 mirror mapping and near-block copy)    */
 } starsh_b200_stats;
 int starsh_b200_get_stats(starsh_b200_stats *stats);
 

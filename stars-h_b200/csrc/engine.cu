@@ -548,7 +548,13 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
     // device sources are freed with the records on failure)
     struct CopyDrain {
         cudaStream_t c;
-        ~CopyDrain() { cudaStreamSynchronize(c); }
+        ~CopyDrain()
+        {
+            const auto t0 = std::chrono::steady_clock::now();
+            cudaStreamSynchronize(c);
+            thread_stats().mirror_wait_ms += std::chrono::duration<double, std::milli>(
+                std::chrono::steady_clock::now() - t0).count();
+        }
     } drain{ctx.copy};
     cudaStream_t s = ctx.stream;
     starsh_b200_stats &st = thread_stats();
@@ -1602,9 +1608,12 @@ static int approximate_batch(int np, STARSH_blrm **matrices,
     ep.mirror = (flags & STARSH_B200_HOST_MIRROR) != 0;
     read_engine_env(ep);
     int info = compress_multi(*ctx, jobs, ep);
+    const auto t_finish = std::chrono::steady_clock::now();
     int done = 0;
     for (; done < np && info == STARSH_SUCCESS; ++done)
         info = finish_problem(jobs[done], flags, s, &matrices[done]);
+    st.finish_ms = std::chrono::duration<double, std::milli>(
+                       std::chrono::steady_clock::now() - t_finish).count();
     if (info) {
         // the problems finished before the failure are released too
         for (int q = 0; q + 1 < done; ++q) {

@@ -130,7 +130,8 @@ class Stats(Structure):
                 ("svd_ms", c_double), ("output_ms", c_double),
                 ("sketch_bytes", c_double), ("sketch_int8", c_int),
                 ("fused_ms", c_double), ("fused_launches", c_longlong),
-                ("fused_bytes", c_double), ("resketch_tiles", c_longlong)]
+                ("fused_bytes", c_double), ("resketch_tiles", c_longlong),
+                ("mirror_wait_ms", c_double), ("finish_ms", c_double)]
 
 
 class ServerStats(Structure):

@@ -37,6 +37,10 @@ struct Context {
     int omega8_rows = 0, omega8_cols = 0, omega8_ld = 0;
     int omega_rows = 0, omega_cols = 0;   // shape Omega was generated for
     size_t workspace_cap = (size_t)-1;    // most workspace one batch may use
+    // page-locked staging of a batch's tile records (two, used in turn, so
+    // that their uploads do not wait for the stream)
+    void *tiles_pin[2] = {nullptr, nullptr};
+    size_t tiles_pin_bytes = 0;
     std::mutex lock;           // one approximation / dmml at a time
 };
 

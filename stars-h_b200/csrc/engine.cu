@@ -194,6 +194,7 @@ void context_free_private(Context *c)
     for (int i = 0; i < 2; ++i) {
         if (c->stage[i]) cudaFreeHost(c->stage[i]);
         if (c->stage_ev[i]) cudaEventDestroy(c->stage_ev[i]);
+        if (c->tiles_pin[i]) host_pinned_free(c->tiles_pin[i]);
     }
     cudaStreamDestroy(c->stream);
     cudaStreamDestroy(c->side);
@@ -737,6 +738,30 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
         !ctx.descs.reserve((size_t)max_slots * sizeof(GemmDesc), s) ||
         !ctx.flag.reserve(256, s))
         return cuda_fail(cudaErrorMemoryAllocation, "batch arrays");
+    const size_t pin_need = (size_t)max_slots * sizeof(TileWork);
+    if (ctx.tiles_pin_bytes < pin_need) {
+        B200_CUDA(cudaStreamSynchronize(s), "tile staging");
+        for (void *&q : ctx.tiles_pin) {
+            if (q) host_pinned_free(q);
+            q = host_pinned_alloc(pin_need);
+        }
+        ctx.tiles_pin_bytes = ctx.tiles_pin[0] && ctx.tiles_pin[1] ? pin_need : 0;
+    }
+    // Uploads a batch's tile records through page-locked staging when there
+    // is some (a copy from pageable memory would first wait for the whole
+    // stream); `which` alternates between the two buffers.  The buffer is
+    // free again once the stream has passed the previous upload from it:
+    // every batch ends with a stream synchronisation.
+    auto upload_tiles = [&](long long b0, int nt, int which) {
+        const size_t bytes = (size_t)nt * sizeof(TileWork);
+        if (ctx.tiles_pin_bytes >= bytes) {
+            memcpy(ctx.tiles_pin[which], &all[b0], bytes);
+            return cudaMemcpyAsync(ctx.tiles.ptr, ctx.tiles_pin[which], bytes,
+                                   cudaMemcpyHostToDevice, s);
+        }
+        return cudaMemcpyAsync(ctx.tiles.ptr, &all[b0], bytes,
+                               cudaMemcpyHostToDevice, s);
+    };
     Workspace ws{};
     TileWork *dt = (TileWork *)ctx.tiles.ptr;
     GemmDesc *dd = (GemmDesc *)ctx.descs.ptr;
@@ -790,8 +815,7 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
                     any_separate = true;
                 }
             }
-        cudaMemcpyAsync(dt, &all[b0], nt * sizeof(TileWork),
-                        cudaMemcpyHostToDevice, s);
+        upload_tiles(b0, nt, 0);
         cudaEventRecord(ev[4], s);
         if (fused) {
             launch_round_setup(dt, nt, ep.block, (int *)ctx.flag.ptr, s);
@@ -1052,8 +1076,7 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
         }
         if (total > 0) {
             OutArena out{base, base};
-            cudaMemcpyAsync(dt, &all[b0], nt * sizeof(TileWork),
-                            cudaMemcpyHostToDevice, s);
+            upload_tiles(b0, nt, 1);
             cudaEventRecord(ev[7], s);
             launch_select_w(dt, nt, ws, s);
             count_launch();

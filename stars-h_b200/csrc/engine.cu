@@ -885,6 +885,8 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
         // N. Halko, P.-G. Martinsson, J. A. Tropp, SIAM Review 53 (2011)
         // sec. 4.3), when a round adds none, or after k columns.
         int *d_active = (int *)ctx.flag.ptr;
+        bool any_width = false;
+        for (int t = 0; t < nt && !any_width; ++t) any_width = all[b0 + t].k > 0;
         auto append = [&](int bmax) -> int {
             // orthonormalise the selected residual columns (kb of them)
             // against the basis and append them: CholQR of R_J, one more
@@ -910,11 +912,16 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
             if (!pre_sketched) {
             launch_round_setup(dt, nt, block, d_active, s);
             count_launch();
-            int active = 0;
-            B200_CUDA(cudaMemcpyAsync(&active, d_active, sizeof(int),
-                                      cudaMemcpyDeviceToHost, s), "round flag");
-            B200_CUDA(cudaStreamSynchronize(s), "round flag");
-            if (!active) break;
+            // round 0 samples every tile with a sketch width (known on
+            // the host): the round is enqueued behind the generation
+            // without waiting for the flag
+            if (round > 0 || !any_width) {
+                int active = 0;
+                B200_CUDA(cudaMemcpyAsync(&active, d_active, sizeof(int),
+                                          cudaMemcpyDeviceToHost, s), "round flag");
+                B200_CUDA(cudaStreamSynchronize(s), "round flag");
+                if (!active) break;
+            }
             }
             cudaEventRecord(ev[0], s);
             if (pre_sketched) {

@@ -116,6 +116,14 @@ int starsh_b200_blrm_download(STARSH_blrm *matrix);
  * it as well; call this one when M is freed by the reference library. */
 void starsh_b200_blrm_release(STARSH_blrm *matrix);
 
+/* Returns the page-locked host blocks of M's host mirror (when its factors
+ * were downloaded batch by batch, STARSH_B200_HOST_MIRROR) to the
+ * library's pool; M's far_U/far_V/near_D data must not be used after it.
+ * starsh_blrm_free() of this library does it as well; call this one, with
+ * starsh_b200_blrm_release(), when M is freed by the reference library.
+ * No-op for other matrices. */
+void starsh_b200_blrm_host_release(const STARSH_blrm *matrix);
+
 /* dmml with device pointers dA (lda) and dB (ldb) on `stream`
  * (a cudaStream_t, NULL for the default stream).  Asynchronous. */
 int starsh_b200_blrm_dmml_device(STARSH_blrm *matrix, int nrhs,

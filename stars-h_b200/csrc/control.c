@@ -651,7 +651,7 @@ void starsh_blrm_free(STARSH_blrm *matrix)
     if(M == NULL)
         return;
     starsh_b200_blrm_release(M);
-    b200_host_mirror_free(M);
+    starsh_b200_blrm_host_release(M);
     STARSH_blrf *F = M->format;
     if(F->nblocks_far > 0)
     {

@@ -1740,7 +1740,7 @@ extern "C" void starsh_b200_blrm_release(STARSH_blrm *matrix)
     delete rec;
 }
 
-extern "C" void b200_host_mirror_free(const STARSH_blrm *matrix)
+extern "C" void starsh_b200_blrm_host_release(const STARSH_blrm *matrix)
 {
     std::vector<void *> owned;
     {

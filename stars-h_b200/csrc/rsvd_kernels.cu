@@ -1395,11 +1395,13 @@ k_jacobi(TileWork *__restrict__ tiles, Workspace ws)
 // read past L1 (__ldcg).
 constexpr int kJacobiClusterMax = 8;
 
-// CTAs per tile: 4 for the classes above 256 rows, 2 below (measured: a
-// cluster of 4 shortens the large classes most, the 193..256-row class
-// gains from 2 and loses SMs to the shared-memory classes beside it at 4);
+// CTAs per tile: 4 for the classes above 256 rows and for every block
+// class of a batch that holds such factors (kmax > 256: its large tiles
+// bound the batch), 2 otherwise (measured: on batches whose factors stay
+// below 257 rows, 4 CTAs per tile take SMs from the shared-memory classes
+// beside them and lose, on batches with larger factors they win);
 // STARSH_B200_JACOBI_CLUSTER (1 .. 8) sets one size for all.
-static int jacobi_cluster(int cls)
+static int jacobi_cluster(int cls, int kmax)
 {
     static const int forced = [] {
         int v = 0;
@@ -1407,7 +1409,7 @@ static int jacobi_cluster(int cls)
             v = std::max(1, std::min(kJacobiClusterMax, atoi(e)));
         return v;
     }();
-    return forced ? forced : cls >= 7 ? 4 : 2;
+    return forced ? forced : (cls >= 7 || kmax > 256) ? 4 : 2;
 }
 
 template <int CLASS, int G, int E>
@@ -1572,12 +1574,13 @@ template <int CLASS, int G, int E>
 static void jacobi_block_launch(TileWork *d_tiles, int ntiles, Workspace ws,
                                 int max_rows, cudaStream_t stream)
 {
+    const int kmax = ws.k_max;
     auto *fn = k_jacobi_block<CLASS, G, E>;
     const size_t smem = (size_t)2 * (512 / G) * (max_rows | 1) * sizeof(double);
     cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
     cudaLaunchConfig_t cfg = {};
-    const int cs = jacobi_cluster(CLASS);
+    const int cs = jacobi_cluster(CLASS, kmax);
     cfg.gridDim = dim3((unsigned)(ntiles * cs));
     cfg.blockDim = dim3(512);
     cfg.dynamicSmemBytes = smem;

@@ -49,11 +49,6 @@ void b200_eval_block_host(STARSH_kernel *kernel, int nrows, int ncols,
 /* Oversampling of the randomized engines (starsh_params.oversample). */
 int b200_oversample(void);
 
-/* Returns the page-locked host blocks that hold the host mirror of
- * `matrix` (when its factors were downloaded batch by batch) to the
- * library's pinned pool; no-op for other matrices. */
-void b200_host_mirror_free(const STARSH_blrm *matrix);
-
 #ifdef __cplusplus
 }
 #endif

@@ -779,11 +779,17 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
     OutArena none{nullptr, nullptr};
     int info = STARSH_SUCCESS;
 
+    // round_count >= 0: the steps of an adaptive round whose sampling
+    // tiles (round_count of them, known from the round flag) have compact
+    // descriptors; -1: one descriptor per tile of the batch
+    int round_count = -1;
     auto gemm = [&](GemmStep step, bool ta, bool tb, int nt, int mm, int nn,
                     OutArena out) -> int {
-        make_gemm_descs(step, dt, nt, ws, omega, n_max, out, dd, s);
+        const bool compact = round_count >= 0;
+        make_gemm_descs(step, dt, nt, ws, omega, n_max, out, dd, s, compact);
         count_launch(2);
-        return gemm_f64_batched(ta, tb, dd, nt, mm, nn, s) == cudaSuccess
+        return gemm_f64_batched(ta, tb, dd, compact ? round_count : nt, mm, nn,
+                                s) == cudaSuccess
                    ? STARSH_SUCCESS
                    : cuda_fail(cudaGetLastError(), "gemm_f64_batched");
     };
@@ -909,18 +915,21 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
             const int block = round == 0 ? ep.block : ep.block_next;
             const int bmax = std::min(block, k_max);
             const bool pre_sketched = fused && round == 0;
+            round_count = -1;
             if (!pre_sketched) {
             launch_round_setup(dt, nt, block, d_active, s);
             count_launch();
             // round 0 samples every tile with a sketch width (known on
             // the host): the round is enqueued behind the generation
-            // without waiting for the flag
+            // without waiting for the flag; later rounds read how many
+            // tiles sample and run their GEMMs over those alone
             if (round > 0 || !any_width) {
                 int active = 0;
                 B200_CUDA(cudaMemcpyAsync(&active, d_active, sizeof(int),
                                           cudaMemcpyDeviceToHost, s), "round flag");
                 B200_CUDA(cudaStreamSynchronize(s), "round flag");
                 if (!active) break;
+                round_count = active;
             }
             }
             cudaEventRecord(ev[0], s);
@@ -968,6 +977,7 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
                 st.sketch_launches += 1;
             }
         }
+        round_count = -1;
         if (info) break;
         }
         // projection (tiles with at most 64 basis columns on the tensor

@@ -40,6 +40,8 @@ struct TileWork {
     double dnorm2;          // ||D||_F^2 of the block, exact (FP64)
     int cols_done;          // sketch columns consumed so far
     int bcur;               // columns of the current round (0: inactive)
+    int round_slot;         // its place among the round's sampling tiles,
+                            // or -1 (compacted GEMM descriptors)
     int done;               // sampling finished (converged or capped)
     int kround;             // directions the current round's sample added
     int k1_round;           // basis columns when the current round began
@@ -139,7 +141,8 @@ struct OutArena {
 // Builds the descriptors of `step` for every tile of the batch.
 void make_gemm_descs(GemmStep step, const TileWork *d_tiles, int ntiles,
                      Workspace ws, const double *d_omega, int ld_omega,
-                     OutArena out, GemmDesc *d_desc, cudaStream_t stream);
+                     OutArena out, GemmDesc *d_desc, cudaStream_t stream,
+                     bool compact = false);
 
 // Per-tile kernels (one CTA per tile).
 // Thresholds come from each tile's tol and maxrank; the generator reads

@@ -332,14 +332,20 @@ void launch_gaussian_i8(int8_t *d_om8, int rows, int cols, int ld,
 
 // ------------------------------------------------- GEMM descriptors
 
+// With `compact`, only the tiles sampling in the current round write a
+// descriptor, at their round slot: the GEMM then runs over that many
+// descriptors instead of the whole batch (every adaptive-round step is
+// empty for the other tiles).
 __global__ void k_make_desc(GemmStep step, const TileWork *__restrict__ tiles,
                             int ntiles, Workspace ws,
                             const double *__restrict__ omega, int ld_omega,
-                            OutArena out, GemmDesc *__restrict__ desc)
+                            OutArena out, GemmDesc *__restrict__ desc,
+                            int compact)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= ntiles) return;
     const TileWork tw = tiles[t];
+    if (compact && tw.round_slot < 0) return;
     const int s = tw.slot;
     GemmDesc d;
     d.alpha = 1.0;
@@ -552,15 +558,17 @@ __global__ void k_make_desc(GemmStep step, const TileWork *__restrict__ tiles,
         d.M = tw.m; d.N = tw.rank; d.K = tw.k1;
         break;
     }
-    desc[t] = d;
+    desc[compact ? tw.round_slot : t] = d;
 }
 
 void make_gemm_descs(GemmStep step, const TileWork *d_tiles, int ntiles,
                      Workspace ws, const double *d_omega, int ld_omega,
-                     OutArena out, GemmDesc *d_desc, cudaStream_t stream)
+                     OutArena out, GemmDesc *d_desc, cudaStream_t stream,
+                     bool compact)
 {
     k_make_desc<<<(ntiles + 127) / 128, 128, 0, stream>>>(
-        step, d_tiles, ntiles, ws, d_omega, ld_omega, out, d_desc);
+        step, d_tiles, ntiles, ws, d_omega, ld_omega, out, d_desc,
+        compact ? 1 : 0);
 }
 
 // ------------------------------------------------- block reductions
@@ -952,7 +960,8 @@ void launch_block_norms(const TileWork *, TileWork *d_rw, int ntiles,
 }
 
 // Start of a sampling round: tiles not done sample min(block, k - cols)
-// more columns; *active becomes 1 if any tile samples.
+// more columns; *active counts them (each takes the next round slot, in
+// any order: a slot only places the tile's GEMM descriptors).
 __global__ void k_round_setup(TileWork *__restrict__ tiles, int ntiles,
                               int block, int *active)
 {
@@ -962,12 +971,13 @@ __global__ void k_round_setup(TileWork *__restrict__ tiles, int ntiles,
     if (tw.done || tw.cols_done >= tw.k) {
         tw.bcur = 0;
         tw.done = 1;
+        tw.round_slot = -1;
         return;
     }
     tw.bcur = min(block, tw.k - tw.cols_done);
     tw.k1_round = tw.k1;
     tw.trunc_round = 0;
-    atomicOr(active, 1);
+    tw.round_slot = atomicAdd(active, 1);
 }
 
 void launch_round_setup(TileWork *d_tiles, int ntiles, int block,

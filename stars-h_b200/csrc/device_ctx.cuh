@@ -30,6 +30,7 @@ struct Context {
     DeviceBuffer descs;        // GemmDesc array of a batch
     DeviceBuffer omega;        // Gaussian sketch matrix
     DeviceBuffer flag;         // round flag of the adaptive sketch
+    DeviceBuffer act;          // a round's sampling tiles, by round slot
     void *stage[2] = {nullptr, nullptr};     // pinned D2H staging buffers
     cudaEvent_t stage_ev[2] = {nullptr, nullptr};
     DeviceBuffer kernels;      // DevKernel table of a batch's problems

@@ -189,6 +189,7 @@ void context_free_private(Context *c)
     c->descs.release();
     c->omega.release();
     c->flag.release();
+    c->act.release();
     c->kernels.release();
     c->omega8.release();
     for (int i = 0; i < 2; ++i) {
@@ -736,7 +737,8 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
         return cuda_fail(cudaErrorMemoryAllocation, "workspace");
     if (!ctx.tiles.reserve((size_t)max_slots * sizeof(TileWork), s) ||
         !ctx.descs.reserve((size_t)max_slots * sizeof(GemmDesc), s) ||
-        !ctx.flag.reserve(256, s))
+        !ctx.flag.reserve(256, s) ||
+        !ctx.act.reserve((size_t)max_slots * sizeof(int), s))
         return cuda_fail(cudaErrorMemoryAllocation, "batch arrays");
     const size_t pin_need = (size_t)max_slots * sizeof(TileWork);
     if (ctx.tiles_pin_bytes < pin_need) {
@@ -824,7 +826,8 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
         upload_tiles(b0, nt, 0);
         cudaEventRecord(ev[4], s);
         if (fused) {
-            launch_round_setup(dt, nt, ep.block, (int *)ctx.flag.ptr, s);
+            launch_round_setup(dt, nt, ep.block, (int *)ctx.flag.ptr,
+                               (int *)ctx.act.ptr, s);
             if (any_separate) {
                 launch_gen_tiles(d_kernels, dt, nt, ws, s, TILE_GEN_SEPARATE);
                 count_launch();
@@ -893,18 +896,23 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
         int *d_active = (int *)ctx.flag.ptr;
         bool any_width = false;
         for (int t = 0; t < nt && !any_width; ++t) any_width = all[b0 + t].k > 0;
+        // the per-tile kernels of a round: over its sampling tiles alone
+        // when their count is known (round_count), else the whole batch
+        const int *act = (const int *)ctx.act.ptr;
+        auto rcount = [&]() { return round_count >= 0 ? round_count : nt; };
+        auto ract = [&]() { return round_count >= 0 ? act : nullptr; };
         auto append = [&](int bmax) -> int {
             // orthonormalise the selected residual columns (kb of them)
             // against the basis and append them: CholQR of R_J, one more
             // projection, CholQR again (CGS2)
             int e;
-            launch_gather_cols(1, dt, nt, ws, s);
+            launch_gather_cols(1, dt, rcount(), ws, s, ract());
             count_launch();
             if ((e = gemm(STEP_A_Q1B, false, false, nt, m_max, bmax, none))) return e;
             if ((e = gemm(STEP_A_ORTH_Z, true, false, nt, k_max, bmax, none))) return e;
             if ((e = gemm(STEP_A_ORTH_R, false, false, nt, m_max, bmax, none))) return e;
             if ((e = gemm(STEP_A_GRAM_R, true, false, nt, bmax, bmax, none))) return e;
-            launch_chol_inv(1, dt, nt, ws, s);
+            launch_chol_inv(1, dt, rcount(), ws, s, ract());
             count_launch();
             if ((e = gemm(STEP_A_QB, false, false, nt, m_max, bmax, none))) return e;
             launch_merge_basis(dt, nt, s);
@@ -917,7 +925,7 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
             const bool pre_sketched = fused && round == 0;
             round_count = -1;
             if (!pre_sketched) {
-            launch_round_setup(dt, nt, block, d_active, s);
+            launch_round_setup(dt, nt, block, d_active, (int *)ctx.act.ptr, s);
             count_launch();
             // round 0 samples every tile with a sketch width (known on
             // the host): the round is enqueued behind the generation
@@ -955,7 +963,7 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
                 if ((info = gemm(STEP_A_RES_Y, false, false, nt, m_max, bmax, none))) break;
             }
             if ((info = gemm(STEP_A_GRAM, true, false, nt, bmax, bmax, none))) break;
-            launch_round_pivchol(dt, nt, ws, 0, s);
+            launch_round_pivchol(dt, rcount(), ws, 0, s, ract());
             count_launch();
             if ((info = append(bmax))) break;
             if (may_repeat) {
@@ -963,7 +971,7 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
                 if ((info = gemm(STEP_A_RES_Z2, true, false, nt, k_max, bmax, none))) break;
                 if ((info = gemm(STEP_A_RES_Y2, false, false, nt, m_max, bmax, none))) break;
                 if ((info = gemm(STEP_A_GRAM2, true, false, nt, bmax, bmax, none))) break;
-                launch_round_pivchol(dt, nt, ws, 1, s);
+                launch_round_pivchol(dt, rcount(), ws, 1, s, ract());
                 count_launch();
                 if ((info = append(bmax))) break;
             }

@@ -154,10 +154,13 @@ void launch_gen_tiles(const DevKernel *d_kernels, const TileWork *d_tiles,
 // launch_pivchol and launch_jacobi return the number of kernels launched.
 int launch_pivchol(int phase, const TileWork *d_tiles, TileWork *d_tiles_rw,
                    int ntiles, Workspace ws, cudaStream_t s);
+// `act` (optional): the launch covers the `ntiles` tiles listed there (a
+// round's sampling tiles) instead of the first `ntiles` of the batch.
 void launch_gather_cols(int phase, const TileWork *d_tiles, int ntiles,
-                        Workspace ws, cudaStream_t stream);
+                        Workspace ws, cudaStream_t stream,
+                        const int *act = nullptr);
 void launch_chol_inv(int phase, TileWork *d_tiles, int ntiles, Workspace ws,
-                     cudaStream_t stream);
+                     cudaStream_t stream, const int *act = nullptr);
 int launch_jacobi(TileWork *d_tiles, int ntiles, Workspace ws,
                   cudaStream_t stream, cudaStream_t side);
 void launch_rank_cut(TileWork *d_tiles, int ntiles, Workspace ws,
@@ -169,11 +172,12 @@ void launch_merge_basis(TileWork *d_tiles, int ntiles, cudaStream_t stream);
 void launch_block_norms(const TileWork *d_tiles, TileWork *d_rw, int ntiles,
                         Workspace ws, cudaStream_t stream);
 void launch_round_setup(TileWork *d_tiles, int ntiles, int block,
-                        int *d_active, cudaStream_t stream);
+                        int *d_active, int *d_act, cudaStream_t stream);
 void launch_round_end(TileWork *d_tiles, int ntiles, int verify,
                       cudaStream_t stream);
 void launch_round_pivchol(TileWork *d_tiles, int ntiles, Workspace ws,
-                          int repeat, cudaStream_t stream);
+                          int repeat, cudaStream_t stream,
+                          const int *act = nullptr);
 void launch_select_w(const TileWork *d_tiles, int ntiles, Workspace ws,
                      cudaStream_t stream);
 // Tensor-core projection B = Q^T D (proj_i8.cu) of the tiles with at most

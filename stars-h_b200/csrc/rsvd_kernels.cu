@@ -701,9 +701,9 @@ constexpr int kMaxK = 1024;   // largest sketch width handled by one CTA
 template <int LPR>
 __global__ void __launch_bounds__(kSmallThreads * LPR)
 k_pivchol(TileWork *__restrict__ tiles, Workspace ws, int phase, int nn_lo,
-          int nn_hi)
+          int nn_hi, const int *__restrict__ act)
 {
-    TileWork &tw = tiles[blockIdx.x];
+    TileWork &tw = tiles[act ? act[blockIdx.x] : blockIdx.x];
     const int s = tw.slot;
     const double tol = tw.tol;
     __shared__ double dg[kMaxK];
@@ -925,10 +925,10 @@ k_pivchol(TileWork *__restrict__ tiles, Workspace ws, int phase, int nn_lo,
 }
 
 void launch_round_pivchol(TileWork *d_tiles, int ntiles, Workspace ws,
-                          int repeat, cudaStream_t stream)
+                          int repeat, cudaStream_t stream, const int *act)
 {
     k_pivchol<1><<<ntiles, kSmallThreads, 0, stream>>>(
-        d_tiles, ws, repeat ? PH_R2 : PH_R, 0, INT_MAX);
+        d_tiles, ws, repeat ? PH_R2 : PH_R, 0, INT_MAX, act);
 }
 
 // ||D||_F^2 of every block from the generator's per-CTA partial sums, in a
@@ -963,7 +963,7 @@ void launch_block_norms(const TileWork *, TileWork *d_rw, int ntiles,
 // more columns; *active counts them (each takes the next round slot, in
 // any order: a slot only places the tile's GEMM descriptors).
 __global__ void k_round_setup(TileWork *__restrict__ tiles, int ntiles,
-                              int block, int *active)
+                              int block, int *active, int *act)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= ntiles) return;
@@ -978,14 +978,16 @@ __global__ void k_round_setup(TileWork *__restrict__ tiles, int ntiles,
     tw.k1_round = tw.k1;
     tw.trunc_round = 0;
     tw.round_slot = atomicAdd(active, 1);
+    act[tw.round_slot] = t;
 }
 
 void launch_round_setup(TileWork *d_tiles, int ntiles, int block,
-                        int *d_active, cudaStream_t stream)
+                        int *d_active, int *d_act, cudaStream_t stream)
 {
     cudaMemsetAsync(d_active, 0, sizeof(int), stream);
     k_round_setup<<<(ntiles + 127) / 128, 128, 0, stream>>>(d_tiles, ntiles,
-                                                            block, d_active);
+                                                            block, d_active,
+                                                            d_act);
 }
 
 // End of a round: the new orthonormal columns join the basis.  The tile is
@@ -1023,13 +1025,13 @@ int launch_pivchol(int phase, const TileWork *, TileWork *d_tiles_rw,
     if (phase == PH_H && kPivcholLanes > 1) {
         // small factors one lane per row, large ones kPivcholLanes
         k_pivchol<1><<<ntiles, kSmallThreads, 0, s>>>(d_tiles_rw, ws, phase, 0,
-                                                      kPivcholSplit);
+                                                      kPivcholSplit, nullptr);
         k_pivchol<kPivcholLanes><<<ntiles, kSmallThreads * kPivcholLanes, 0, s>>>(
-            d_tiles_rw, ws, phase, kPivcholSplit + 1, INT_MAX);
+            d_tiles_rw, ws, phase, kPivcholSplit + 1, INT_MAX, nullptr);
         return 2;
     } else {
         k_pivchol<1><<<ntiles, kSmallThreads, 0, s>>>(d_tiles_rw, ws, phase, 0,
-                                                      INT_MAX);
+                                                      INT_MAX, nullptr);
         return 1;
     }
 }
@@ -1037,9 +1039,10 @@ int launch_pivchol(int phase, const TileWork *, TileWork *d_tiles_rw,
 // Gathers the pivot columns of Y into the Q buffer (phase A) or the Q1
 // buffer (phase B).
 __global__ void k_gather_cols(const TileWork *__restrict__ tiles,
-                              Workspace ws, int phase)
+                              Workspace ws, int phase,
+                              const int *__restrict__ act)
 {
-    const TileWork tw = tiles[blockIdx.x];
+    const TileWork tw = tiles[act ? act[blockIdx.x] : blockIdx.x];
     const int s = tw.slot;
     const int cnt = phase == PH_A ? tw.k1 : tw.kb;
     if (cnt <= 0) return;
@@ -1055,10 +1058,10 @@ __global__ void k_gather_cols(const TileWork *__restrict__ tiles,
 }
 
 void launch_gather_cols(int phase, const TileWork *d_tiles, int ntiles,
-                        Workspace ws, cudaStream_t stream)
+                        Workspace ws, cudaStream_t stream, const int *act)
 {
     dim3 grid(ntiles, 16);
-    k_gather_cols<<<grid, 256, 0, stream>>>(d_tiles, ws, phase);
+    k_gather_cols<<<grid, 256, 0, stream>>>(d_tiles, ws, phase, act);
 }
 
 // Cholesky G = R^T R of the re-orthogonalisation Gram in S(slot)
@@ -1066,9 +1069,10 @@ void launch_gather_cols(int phase, const TileWork *d_tiles, int ntiles,
 // T(slot) = R^{-1}.  For phase B the new columns are appended to the basis
 // afterwards by the caller's merge step.
 __global__ void __launch_bounds__(kSmallThreads)
-k_chol_inv(TileWork *__restrict__ tiles, Workspace ws, int phase)
+k_chol_inv(TileWork *__restrict__ tiles, Workspace ws, int phase,
+           const int *__restrict__ act)
 {
-    TileWork &tw = tiles[blockIdx.x];
+    TileWork &tw = tiles[act ? act[blockIdx.x] : blockIdx.x];
     const int s = tw.slot;
     const int nn = phase == PH_A ? tw.k1 : tw.kb;
     if (nn <= 0) return;
@@ -1127,9 +1131,9 @@ k_chol_inv(TileWork *__restrict__ tiles, Workspace ws, int phase)
 }
 
 void launch_chol_inv(int phase, TileWork *d_tiles, int ntiles, Workspace ws,
-                     cudaStream_t stream)
+                     cudaStream_t stream, const int *act)
 {
-    k_chol_inv<<<ntiles, kSmallThreads, 0, stream>>>(d_tiles, ws, phase);
+    k_chol_inv<<<ntiles, kSmallThreads, 0, stream>>>(d_tiles, ws, phase, act);
 }
 
 // -------------------------------------------------- one-sided Jacobi

@@ -7,6 +7,7 @@
 // current one is multiplied.  Global loads are coalesced along whichever
 // dimension is contiguous for the given transpose flag.
 #include <cstdint>
+#include <mutex>
 #include "gemm_f64.cuh"
 
 namespace b200 {
@@ -158,14 +159,15 @@ k_gemm_f64(const GemmDesc *__restrict__ descs, int tiles_n)
     }
 }
 
-// A^T B with 64 x 64 CTA tiles and a three-stage cp.async pipeline: the
-// transposed products of the basis rounds (Grams and projections onto the
-// basis) have outputs of at most a few 64 x 64 tiles and K = the tile
+// A^T B with 64 x 64 or 32 x 128 CTA tiles and a three-stage cp.async
+// pipeline: the transposed products (Grams and projections onto the basis
+// in the rounds; the projection B = Q^T D and rotation C = W^T B of the
+// small SVD, 32 x 128) have outputs of a few tiles and K = the tile
 // height, so one CTA walks a long K; the register-staged kernel above keeps
 // one K step in flight and waits on memory latency every step.  Operand
 // tiles land in shared memory directly (16-byte cp.async, k contiguous in
-// both operands), two steps ahead of the multiply (60 KB of shared memory,
-// three CTAs per SM as for the register-staged kernel).  Same per-element
+// both operands), two steps ahead of the multiply (60 or 75 KB of shared
+// memory).  Same per-element
 // accumulation order as k_gemm_f64 (K steps of 16 in order, the DMMA's
 // k-order inside a step), so results are identical to it.
 constexpr int kTnStages = 3;
@@ -178,10 +180,14 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem, bool pr
                  :: "r"(sa), "l"(gmem), "r"(n));
 }
 
+template <int BM, int BN>
 __global__ void __launch_bounds__(kGemmThreads)
 k_gemm_f64_tn_pipe(const GemmDesc *__restrict__ descs, int tiles_n)
 {
-    constexpr int BM = 64, BN = 64;
+    constexpr int WARPS_M = BM / 32;
+    static_assert(WARPS_M * (BN / 16) == kGemmThreads / 32, "warp grid");
+    // 16-byte pieces of the two operand tiles (BM and BN rows of 16 k)
+    constexpr int PA = BM * kGemmBK / 2, PIECES = (BM + BN) * kGemmBK / 2;
     const GemmDesc d = descs[blockIdx.y];
     const int tm = blockIdx.x / tiles_n, tn = blockIdx.x % tiles_n;
     const int m0 = tm * BM, n0 = tn * BN;
@@ -193,23 +199,24 @@ k_gemm_f64_tn_pipe(const GemmDesc *__restrict__ descs, int tiles_n)
     const int t = threadIdx.x;
     const int lane = t & 31, warp = t >> 5;
     const int g = lane >> 2, tig = lane & 3;
-    const int wm = (warp % 2) * 32, wn = (warp / 2) * 16;
+    const int wm = (warp % WARPS_M) * 32, wn = (warp / WARPS_M) * 16;
     double acc[4][2][2];
     #pragma unroll
     for (int i = 0; i < 4; ++i)
         #pragma unroll
         for (int j = 0; j < 2; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-    // each operand tile is 64 rows x 16 k = 512 16-byte pieces: thread t
-    // copies pieces t and t + 256 of each (row = piece / 8, k pair = piece % 8)
+    // the A tile (BM rows x 16 k) is pieces 0 .. PA - 1, the B tile (BN
+    // rows) the rest; thread t copies pieces t, t + 256, ... (row = piece
+    // / 8 within its tile, k pair = piece % 8)
     const bool evenA = (d.lda & 1) == 0 && ((uintptr_t)d.A & 15) == 0;
     const bool evenB = (d.ldb & 1) == 0 && ((uintptr_t)d.B & 15) == 0;
     auto issue = [&](int kt) {
         const int st = kt % kTnStages, k0 = kt * kGemmBK;
         #pragma unroll
-        for (int r = 0; r < 2; ++r) {
+        for (int r = 0; r < PIECES / kGemmThreads; ++r) {
             const int piece = t + kGemmThreads * r;
-            const int row = piece >> 3, kk = (piece & 7) * 2;
-            {
+            if (piece < PA) {
+                const int row = piece >> 3, kk = (piece & 7) * 2;
                 const int gm = m0 + row, gk = k0 + kk;
                 double *dst = As + (st * BM + row) * kGemmLds + kk;
                 if (evenA && gm < d.M && gk + 1 < d.K) {
@@ -218,8 +225,9 @@ k_gemm_f64_tn_pipe(const GemmDesc *__restrict__ descs, int tiles_n)
                     dst[0] = (gm < d.M && gk < d.K) ? d.A[(size_t)gm * d.lda + gk] : 0.0;
                     dst[1] = (gm < d.M && gk + 1 < d.K) ? d.A[(size_t)gm * d.lda + gk + 1] : 0.0;
                 }
-            }
-            {
+            } else {
+                const int q = piece - PA;
+                const int row = q >> 3, kk = (q & 7) * 2;
                 const int gn = n0 + row, gk = k0 + kk;
                 double *dst = Bs + (st * BN + row) * kGemmLds + kk;
                 if (evenB && gn < d.N && gk + 1 < d.K) {
@@ -314,22 +322,28 @@ cudaError_t gemm_f64_batched(bool ta, bool tb, const GemmDesc *d_desc,
     else if (max_n <= 32 && max_m >= 128) { bm = 128; bn = 32; }
     const int tiles_m = (max_m + bm - 1) / bm;
     const int tiles_n = (max_n + bn - 1) / bn;
-    // transposed products with 64 x 64 tiles: the pipelined kernel
-    const bool pipe = ta && !tb && bm == 64 && bn == 64;
+    // transposed products (64 x 64 and 32 x 128 tiles): the pipelined kernel
+    const bool pipe = ta && !tb && (bm == 64 || bm == 32);
     for (int b0 = 0; b0 < batch; b0 += 65535) {
         const int nb = batch - b0 < 65535 ? batch - b0 : 65535;
         const GemmDesc *dd = d_desc + b0;
         if (pipe) {
-            const size_t smem = (size_t)kTnStages * 2 * 64 * kGemmLds * sizeof(double);
-            static bool attr = false;
-            if (!attr) {
-                cudaFuncSetAttribute(k_gemm_f64_tn_pipe,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem);
-                attr = true;
-            }
             dim3 grid(tiles_m * tiles_n, nb);
-            k_gemm_f64_tn_pipe<<<grid, kGemmThreads, smem, stream>>>(dd, tiles_n);
+            constexpr size_t smem64 = (size_t)kTnStages * 128 * kGemmLds * sizeof(double);
+            constexpr size_t smem32 = (size_t)kTnStages * 160 * kGemmLds * sizeof(double);
+            static std::once_flag attr;
+            std::call_once(attr, [] {
+                cudaFuncSetAttribute(k_gemm_f64_tn_pipe<64, 64>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem64);
+                cudaFuncSetAttribute(k_gemm_f64_tn_pipe<32, 128>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem32);
+            });
+            if (bm == 64)
+                k_gemm_f64_tn_pipe<64, 64><<<grid, kGemmThreads, smem64, stream>>>(dd, tiles_n);
+            else
+                k_gemm_f64_tn_pipe<32, 128><<<grid, kGemmThreads, smem32, stream>>>(dd, tiles_n);
         } else if (bm == 32) launch_shape<32, 128>(ta, tb, dd, nb, tiles_m, tiles_n, stream);
         else if (bm == 128) launch_shape<128, 32>(ta, tb, dd, nb, tiles_m, tiles_n, stream);
         else launch_shape<64, 64>(ta, tb, dd, nb, tiles_m, tiles_n, stream);

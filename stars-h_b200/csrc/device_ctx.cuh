@@ -25,10 +25,6 @@ struct Context {
     cudaStream_t stream = nullptr;
     cudaStream_t side = nullptr;   // second stream for overlapping launches
     cudaStream_t copy = nullptr;   // device-to-host copies of finished batches
-    // a private context's second pair of streams at the device's highest
-    // priority, swapped in for short work (context_use_urgent)
-    cudaStream_t alt_stream = nullptr, alt_side = nullptr;
-    bool urgent = false;
     DeviceBuffer workspace;    // per-slot scratch of the engine
     DeviceBuffer tiles;        // TileWork array of a batch
     DeviceBuffer descs;        // GemmDesc array of a batch
@@ -57,9 +53,6 @@ Context *context();
 Context *context_new_private();
 void context_free_private(Context *c);
 void set_thread_context(Context *c);
-// Puts the private context's work on its high-priority streams (urgent)
-// or back on its normal ones; only between calls (all of its work done).
-void context_use_urgent(Context *c, bool urgent);
 
 // Stream-ordered device allocation from the device's memory pool, whose
 // freed memory stays cached for the next call (repeated approximations do

@@ -160,15 +160,9 @@ Context *context_new_private()
         cap_mb = (size_t)std::max(64LL, atoll(e));
     c->workspace_cap = cap_mb << 20;
     cudaSetDevice(c->device);
-    int least = 0, greatest = 0;
-    cudaDeviceGetStreamPriorityRange(&least, &greatest);
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&c->copy, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaStreamCreateWithPriority(&c->alt_stream, cudaStreamNonBlocking,
-                                     greatest) != cudaSuccess ||
-        cudaStreamCreateWithPriority(&c->alt_side, cudaStreamNonBlocking,
-                                     greatest) != cudaSuccess) {
+        cudaStreamCreateWithFlags(&c->copy, cudaStreamNonBlocking) != cudaSuccess) {
         cudaGetLastError();
         delete c;
         return nullptr;
@@ -176,19 +170,10 @@ Context *context_new_private()
     return c;
 }
 
-void context_use_urgent(Context *c, bool urgent)
-{
-    if (c == nullptr || c->alt_stream == nullptr || c->urgent == urgent) return;
-    std::swap(c->stream, c->alt_stream);
-    std::swap(c->side, c->alt_side);
-    c->urgent = urgent;
-}
-
 void context_free_private(Context *c)
 {
     if (c == nullptr) return;
     cudaSetDevice(c->device);
-    context_use_urgent(c, false);
     cudaStreamSynchronize(c->stream);
     cudaStreamSynchronize(c->side);
     cudaStreamSynchronize(c->copy);
@@ -215,8 +200,6 @@ void context_free_private(Context *c)
     cudaStreamDestroy(c->stream);
     cudaStreamDestroy(c->side);
     cudaStreamDestroy(c->copy);
-    if (c->alt_stream) cudaStreamDestroy(c->alt_stream);
-    if (c->alt_side) cudaStreamDestroy(c->alt_side);
     delete c;
 }
 

@@ -63,7 +63,6 @@ struct starsh_b200_server {
     int engine;
     int max_group;
     double group_entries;             // work cap of one group (entries)
-    double urgent_entries;            // groups below: high-priority streams
     std::mutex mu;
     std::condition_variable cv_work;   // worker: new requests or releases
     std::condition_variable cv_done;   // waiters: completions
@@ -130,7 +129,6 @@ static void worker_loop(starsh_b200_server *sv)
     for (;;) {
         std::vector<Request *> group;
         double group_estimate = 0.0;
-        double group_work = 0.0;
         {
             std::unique_lock<std::mutex> lk(sv->mu);
             for (;;) {
@@ -167,7 +165,6 @@ static void worker_loop(starsh_b200_server *sv)
                 }
                 if (!group.empty()) {
                     sv->inflight += group_estimate;
-                    group_work = work;
                     const auto now = std::chrono::steady_clock::now();
                     for (const Request *r : group)
                         sv->stats.queue_ms += std::chrono::duration<double, std::milli>(
@@ -179,10 +176,6 @@ static void worker_loop(starsh_b200_server *sv)
             }
             sv->stats.groups += 1;
         }
-        // short groups on the worker's high-priority streams: their blocks
-        // are scheduled ahead of a long group's on the other workers, so a
-        // large request in flight does not hold up the small ones behind it
-        context_use_urgent(own, group_work < sv->urgent_entries);
         auto t0 = std::chrono::steady_clock::now();
         const int np = (int)group.size();
         std::vector<STARSH_blrm *> mats(np, nullptr);
@@ -256,9 +249,6 @@ extern "C" int starsh_b200_server_new(starsh_b200_server **server,
     sv->group_entries = 5e8;
     if (const char *e = getenv("STARSH_B200_SERVER_GROUP_ENTRIES"))
         sv->group_entries = std::max(1.0, atof(e));
-    sv->urgent_entries = 3e8;
-    if (const char *e = getenv("STARSH_B200_SERVER_URGENT_ENTRIES"))
-        sv->urgent_entries = std::max(0.0, atof(e));
     int nw = 3;
     if (const char *e = getenv("STARSH_B200_SERVER_WORKERS"))
         nw = std::max(1, std::min(8, atoi(e)));

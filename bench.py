@@ -1351,7 +1351,11 @@ def main():
                 "last_step_host_ms": {
                     "whole_call": e2e_st.total_ms,
                     "waiting_for_batch_downloads": e2e_st.mirror_wait_ms,
-                    "after_last_batch": e2e_st.finish_ms}},
+                    "after_last_batch": e2e_st.finish_ms},
+                "last_step_device_phases_ms": {
+                    "generation": e2e_st.gen_ms, "sketch": e2e_st.sketch_ms,
+                    "basis": e2e_st.basis_ms, "project": e2e_st.project_ms,
+                    "svd": e2e_st.svd_ms, "output": e2e_st.output_ms}},
         "gpu_launches": int(sum(s.kernel_launches for s in sts)),
         "phases_ms": {"generation": last.gen_ms, "fused_gen_sketch": last.fused_ms,
                       "sketch": last.sketch_ms, "basis": last.basis_ms,

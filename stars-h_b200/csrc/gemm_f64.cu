@@ -290,6 +290,111 @@ k_gemm_f64_tn_pipe(const GemmDesc *__restrict__ descs, int tiles_n)
     }
 }
 
+// A B^T with 64 x 64 CTA tiles (the Gram B B^T of the small SVD, K = the
+// tile width) through the same three-stage cp.async pipeline as the
+// transposed products.  Here rows are contiguous in both operands and k is
+// strided, so the tiles are staged as [k][row] (row stride 68 doubles:
+// fragment reads free of bank conflicts); a 16-byte piece is two
+// consecutive rows at one k.  Same per-element accumulation order as
+// k_gemm_f64 (K steps of 16 in order), so results are identical to it.
+constexpr int kNtLds = 64 + 4;
+
+__global__ void __launch_bounds__(kGemmThreads)
+k_gemm_f64_nt_pipe(const GemmDesc *__restrict__ descs, int tiles_n)
+{
+    constexpr int BM = 64, BN = 64;
+    const GemmDesc d = descs[blockIdx.y];
+    const int tm = blockIdx.x / tiles_n, tn = blockIdx.x % tiles_n;
+    const int m0 = tm * BM, n0 = tn * BN;
+    if (m0 >= d.M || n0 >= d.N) return;
+    extern __shared__ double gemm_smem[];
+    // [stage][16 k][kNtLds] for A, then the same for B
+    double *As = gemm_smem;
+    double *Bs = gemm_smem + kTnStages * kGemmBK * kNtLds;
+    const int t = threadIdx.x;
+    const int lane = t & 31, warp = t >> 5;
+    const int g = lane >> 2, tig = lane & 3;
+    const int wm = (warp % 2) * 32, wn = (warp / 2) * 16;
+    double acc[4][2][2];
+    #pragma unroll
+    for (int i = 0; i < 4; ++i)
+        #pragma unroll
+        for (int j = 0; j < 2; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+    const bool evenA = (d.lda & 1) == 0 && ((uintptr_t)d.A & 15) == 0;
+    const bool evenB = (d.ldb & 1) == 0 && ((uintptr_t)d.B & 15) == 0;
+    // pieces 0 .. 511: A (row pair = piece % 32, k = piece / 32), 512 ..
+    // 1023: B the same way; thread t copies t, t + 256, t + 512, t + 768
+    auto issue = [&](int kt) {
+        const int st = kt % kTnStages, k0 = kt * kGemmBK;
+        #pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const int piece = t + kGemmThreads * r;
+            const bool isA = piece < 512;
+            const int q = isA ? piece : piece - 512;
+            const int row = (q & 31) * 2, kk = q >> 5;
+            const int gk = k0 + kk;
+            const double *src = isA ? d.A : d.B;
+            const int ld = isA ? d.lda : d.ldb;
+            const int lim = isA ? d.M : d.N;
+            const int g0 = (isA ? m0 : n0) + row;
+            double *dst = (isA ? As : Bs) + (st * kGemmBK + kk) * kNtLds + row;
+            if ((isA ? evenA : evenB) && g0 + 1 < lim && gk < d.K) {
+                cp_async16(dst, src + (size_t)gk * ld + g0, true);
+            } else {
+                dst[0] = (g0 < lim && gk < d.K) ? src[(size_t)gk * ld + g0] : 0.0;
+                dst[1] = (g0 + 1 < lim && gk < d.K) ? src[(size_t)gk * ld + g0 + 1] : 0.0;
+            }
+        }
+        asm volatile("cp.async.commit_group;");
+    };
+    const int ktiles = (d.K + kGemmBK - 1) / kGemmBK;
+    #pragma unroll
+    for (int p = 0; p < kTnStages - 1; ++p) {
+        if (p < ktiles) issue(p);
+        else asm volatile("cp.async.commit_group;");
+    }
+    for (int kt = 0; kt < ktiles; ++kt) {
+        asm volatile("cp.async.wait_group %0;" :: "n"(kTnStages - 2));
+        __syncthreads();
+        if (kt + kTnStages - 1 < ktiles) issue(kt + kTnStages - 1);
+        else asm volatile("cp.async.commit_group;");
+        const int st = kt % kTnStages;
+        const double *Ab = As + st * kGemmBK * kNtLds;
+        const double *Bb = Bs + st * kGemmBK * kNtLds;
+        #pragma unroll
+        for (int kk = 0; kk < kGemmBK; kk += 4) {
+            double af[4], bf[2];
+            #pragma unroll
+            for (int i = 0; i < 4; ++i) af[i] = Ab[(kk + tig) * kNtLds + wm + i * 8 + g];
+            #pragma unroll
+            for (int j = 0; j < 2; ++j) bf[j] = Bb[(kk + tig) * kNtLds + wn + j * 8 + g];
+            #pragma unroll
+            for (int i = 0; i < 4; ++i)
+                #pragma unroll
+                for (int j = 0; j < 2; ++j)
+                    dmma_8x8x4(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+        }
+    }
+    asm volatile("cp.async.wait_group 0;");
+    #pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int gm = m0 + wm + i * 8 + g;
+        if (gm >= d.M) continue;
+        #pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            #pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int gn = n0 + wn + j * 8 + 2 * tig + h;
+                if (gn >= d.N) continue;
+                double *c = d.C + (size_t)gn * d.ldc + gm;
+                double v = d.alpha * acc[i][j][h];
+                if (d.beta != 0.0) v += d.beta * *c;
+                *c = v;
+            }
+        }
+    }
+}
+
 template <int BM, int BN>
 static void launch_shape(bool ta, bool tb, const GemmDesc *dd, int nb,
                          int tiles_m, int tiles_n, cudaStream_t stream)
@@ -344,6 +449,16 @@ cudaError_t gemm_f64_batched(bool ta, bool tb, const GemmDesc *d_desc,
                 k_gemm_f64_tn_pipe<64, 64><<<grid, kGemmThreads, smem64, stream>>>(dd, tiles_n);
             else
                 k_gemm_f64_tn_pipe<32, 128><<<grid, kGemmThreads, smem32, stream>>>(dd, tiles_n);
+        } else if (!ta && tb && bm == 64) {
+            dim3 grid(tiles_m * tiles_n, nb);
+            constexpr size_t smem = (size_t)kTnStages * 2 * kGemmBK * kNtLds * sizeof(double);
+            static std::once_flag attr_nt;
+            std::call_once(attr_nt, [] {
+                cudaFuncSetAttribute(k_gemm_f64_nt_pipe,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem);
+            });
+            k_gemm_f64_nt_pipe<<<grid, kGemmThreads, smem, stream>>>(dd, tiles_n);
         } else if (bm == 32) launch_shape<32, 128>(ta, tb, dd, nb, tiles_m, tiles_n, stream);
         else if (bm == 128) launch_shape<128, 32>(ta, tb, dd, nb, tiles_m, tiles_n, stream);
         else launch_shape<64, 64>(ta, tb, dd, nb, tiles_m, tiles_n, stream);

@@ -68,15 +68,22 @@ size_t workspace_layout(Workspace &w, int m_max, int n_max, int k_max,
 
 // -------------------------------------------------------- generation
 
-// D(slot) = block of the tile, column-major with ld = m_max.  A CTA owns a
-// 64 x 64 sub-block: the coordinates of its 64 rows and 64 columns are
-// gathered through the cluster pivots into shared memory once (point-major
-// layouts and dimensions above kStageDim read global memory directly),
-// then each thread evaluates 16 entries of one row, so stores run down the
-// columns and are coalesced.  The CTA also writes the sum of squares of its
-// entries to Nrm(slot) (deterministic per-tile norms for the adaptive
-// sketch).
+// D(slot) = block of the tile, column-major with ld = m_max.  A CTA owns
+// 64 rows and kGenCb column blocks of 64: the coordinates of its rows and
+// columns are gathered through the cluster pivots into shared memory once
+// (point-major layouts and dimensions above kStageDim read global memory
+// directly), then each thread evaluates 16 entries of one row in each
+// 64 x 64 block, so stores run down the columns and are coalesced.  Per
+// 64 x 64 block the CTA writes the sum of squares of its entries to
+// Nrm(slot) and each row's largest |D_ij| to Rmx(slot), reduced in a fixed
+// order (deterministic per-tile norms for the adaptive sketch).  Several
+// blocks per CTA spread the gathers and barriers of the staging over more
+// entries.
 constexpr int kStageDim = 4;
+#ifndef GEN_CB
+#define GEN_CB 4              // 64-column blocks of one generator CTA
+#endif
+constexpr int kGenCb = GEN_CB;
 #ifndef GEN_MIN_BLOCKS
 #define GEN_MIN_BLOCKS 3      // CTAs per SM the generator is compiled for
 #endif
@@ -88,10 +95,10 @@ constexpr int kGenUnroll = GEN_UNROLL;
 // The entries of one thread in a 64 x 64 block: rows ii, columns jj0,
 // jj0 + 4, ... below jn, written to Dcol[jj * ld] (Dcol points at row ii of
 // the block's first column); returns their sum of squares.
-template <int FAM, int NDIM>
+template <int FAM, int NDIM, int LDC>
 __device__ __forceinline__ double gen_entries(
     const DevKernel &K, bool staged, const double (*rc)[64],
-    const double (*cc)[64], const long long *ri, const long long *ci, int ii,
+    const double (*cc)[LDC], const long long *ri, const long long *ci, int ii,
     int jj0, int jn, double *Dcol, int ld, double &amax)
 {
     // NDIM > 0: coordinates staged in shared memory, dimension known at
@@ -135,50 +142,85 @@ __device__ __forceinline__ double gen_entries(
 }
 
 // Dispatch on the staging dimension for one family.
-template <int FAM>
+template <int FAM, int LDC>
 __device__ __forceinline__ double gen_entries_dim(
     const DevKernel &K, bool staged, const double (*rc)[64],
-    const double (*cc)[64], const long long *ri, const long long *ci, int ii,
+    const double (*cc)[LDC], const long long *ri, const long long *ci, int ii,
     int jj0, int jn, double *Dcol, int ld, double &amax)
 {
     if (!staged)
-        return gen_entries<FAM, -1>(K, staged, rc, cc, ri, ci, ii, jj0, jn, Dcol, ld, amax);
+        return gen_entries<FAM, -1, LDC>(K, staged, rc, cc, ri, ci, ii, jj0, jn, Dcol, ld, amax);
     if (K.ndim == 2)
-        return gen_entries<FAM, 2>(K, staged, rc, cc, ri, ci, ii, jj0, jn, Dcol, ld, amax);
+        return gen_entries<FAM, 2, LDC>(K, staged, rc, cc, ri, ci, ii, jj0, jn, Dcol, ld, amax);
     if (K.ndim == 3)
-        return gen_entries<FAM, 3>(K, staged, rc, cc, ri, ci, ii, jj0, jn, Dcol, ld, amax);
-    return gen_entries<FAM, 0>(K, staged, rc, cc, ri, ci, ii, jj0, jn, Dcol, ld, amax);
+        return gen_entries<FAM, 3, LDC>(K, staged, rc, cc, ri, ci, ii, jj0, jn, Dcol, ld, amax);
+    return gen_entries<FAM, 0, LDC>(K, staged, rc, cc, ri, ci, ii, jj0, jn, Dcol, ld, amax);
+}
+
+// The 16 entries of each thread in one 64 x 64 block of a generator CTA
+// (columns jb0 .. jb0 + 63 of the tile), family dispatched once.
+template <int LDC>
+__device__ __forceinline__ double gen_block(
+    const DevKernel &K, bool staged, const double (*rc)[64],
+    const double (*cc)[LDC], const long long *ri, const long long *ci, int ii,
+    int jj0, int jn, double *Dcol, int ld, double &amax)
+{
+    switch (K.family) {
+    case FAM_EXP:
+        return gen_entries_dim<FAM_EXP, LDC>(K, staged, rc, cc, ri, ci, ii, jj0, jn, Dcol, ld, amax);
+    case FAM_SQREXP:
+        return gen_entries_dim<FAM_SQREXP, LDC>(K, staged, rc, cc, ri, ci, ii, jj0, jn, Dcol, ld, amax);
+    case FAM_MATERN:
+        return gen_entries_dim<FAM_MATERN, LDC>(K, staged, rc, cc, ri, ci, ii, jj0, jn, Dcol, ld, amax);
+    case FAM_MATERN2:
+        return gen_entries_dim<FAM_MATERN2, LDC>(K, staged, rc, cc, ri, ci, ii, jj0, jn, Dcol, ld, amax);
+    case FAM_COULOMB:
+        return gen_entries_dim<FAM_COULOMB, LDC>(K, staged, rc, cc, ri, ci, ii, jj0, jn, Dcol, ld, amax);
+    case FAM_SIN:
+        return gen_entries_dim<FAM_SIN, LDC>(K, staged, rc, cc, ri, ci, ii, jj0, jn, Dcol, ld, amax);
+    case FAM_COS:
+        return gen_entries_dim<FAM_COS, LDC>(K, staged, rc, cc, ri, ci, ii, jj0, jn, Dcol, ld, amax);
+    default:
+        return gen_entries_dim<FAM_RBF, LDC>(K, staged, rc, cc, ri, ci, ii, jj0, jn, Dcol, ld, amax);
+    }
 }
 
 __global__ void __launch_bounds__(256, GEN_MIN_BLOCKS)
 k_gen_tiles(const DevKernel *__restrict__ kernels,
             const TileWork *__restrict__ tiles, Workspace ws, int need)
 {
+    constexpr int W = 64 * kGenCb;   // columns of the CTA
     const TileWork tw = tiles[blockIdx.z];
-    if (blockIdx.x * 64 >= tw.m || blockIdx.y * 64 >= tw.n) return;
+    if (blockIdx.x * 64 >= tw.m || blockIdx.y * W >= tw.n) return;
     if (need != 0 && (tw.status & need) == 0) return;
-    __shared__ double rc[kStageDim][64], cc[kStageDim][64];
-    __shared__ long long ri[64], ci[64];
-    __shared__ double red[8];
+    __shared__ double rc[kStageDim][64], cc[kStageDim][W];
+    __shared__ long long ri[64], ci[W];
+    __shared__ double red[kGenCb][8];
+    __shared__ double rmx[kGenCb][4][64];
     __shared__ DevKernel Ks;
     const int t = threadIdx.x;
     if (t == 0) Ks = kernels[tw.prob];
     __syncthreads();
     const DevKernel &K = Ks;
-    const int i0 = blockIdx.x * 64, j0 = blockIdx.y * 64;
+    const int i0 = blockIdx.x * 64, j0 = blockIdx.y * W;
+    const int ncol = min(W, tw.n - j0);      // columns of this CTA
     const bool staged = !K.aos && K.ndim <= kStageDim;
     if (t < 64) {
         const int i = min(i0 + t, tw.m - 1);
         ri[t] = K.row_piv[tw.row0 + i];
-    } else if (t < 128) {
-        const int j = min(j0 + t - 64, tw.n - 1);
-        ci[t - 64] = K.col_piv[tw.col0 + j];
+    }
+    for (int e = t; e < W; e += 256) {
+        const int j = min(j0 + e, tw.n - 1);
+        ci[e] = K.col_piv[tw.col0 + j];
     }
     __syncthreads();
     if (staged) {
         for (int q = t; q < 64 * K.ndim; q += 256) {
             const int d = q / 64, e = q % 64;
             rc[d][e] = K.row_pt[d * K.row_count + ri[e]];
+        }
+        for (int q = t; q < W * K.ndim; q += 256) {
+            const int d = q / W, e = q % W;
             cc[d][e] = K.col_pt[d * K.col_count + ci[e]];
         }
     }
@@ -186,57 +228,42 @@ k_gen_tiles(const DevKernel *__restrict__ kernels,
     const int ii = t & 63, i = i0 + ii;
     double *D = ws.D(tw.slot);
     const int ld = ws.ldD();
-    double ss = 0.0, amax = 0.0;
-    if (i < tw.m) {
-        const int jn = min(64, tw.n - j0);
-        switch (K.family) {
-        case FAM_EXP:
-            ss = gen_entries_dim<FAM_EXP>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld, amax);
-            break;
-        case FAM_SQREXP:
-            ss = gen_entries_dim<FAM_SQREXP>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld, amax);
-            break;
-        case FAM_MATERN:
-            ss = gen_entries_dim<FAM_MATERN>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld, amax);
-            break;
-        case FAM_MATERN2:
-            ss = gen_entries_dim<FAM_MATERN2>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld, amax);
-            break;
-        case FAM_COULOMB:
-            ss = gen_entries_dim<FAM_COULOMB>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld, amax);
-            break;
-        case FAM_SIN:
-            ss = gen_entries_dim<FAM_SIN>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld, amax);
-            break;
-        case FAM_COS:
-            ss = gen_entries_dim<FAM_COS>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld, amax);
-            break;
-        default:
-            ss = gen_entries_dim<FAM_RBF>(K, staged, rc, cc, ri, ci, ii, t >> 6, jn, D + (size_t)j0 * ld + i, ld, amax);
-        }
+    #pragma unroll 1
+    for (int b = 0; b < kGenCb; ++b) {
+        const int jb = b * 64;                // first column of the block
+        if (jb >= ncol) break;
+        double ss = 0.0, amax = 0.0;
+        if (i < tw.m)
+            ss = gen_block<W>(K, staged, rc, (const double (*)[W])&cc[0][jb],
+                              ri, ci + jb, ii, t >> 6, min(64, ncol - jb),
+                              D + (size_t)(j0 + jb) * ld + i, ld, amax);
+        // largest |D_ij| of each row of the block (the int8 sketch's row
+        // scales): the four threads of a row combine through shared memory
+        rmx[b][t >> 6][ii] = amax;
+        #pragma unroll
+        for (int o = 16; o > 0; o >>= 1) ss += __shfl_down_sync(0xffffffffu, ss, o);
+        if ((t & 31) == 0) red[b][t >> 5] = ss;
     }
-    // largest |D_ij| of each row of the sub-block (for the int8 sketch's
-    // row scales): the four threads of a row combine through shared memory
-    __shared__ double rmx[4][64];
-    rmx[t >> 6][ii] = amax;
-    #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) ss += __shfl_down_sync(0xffffffffu, ss, o);
-    if ((t & 31) == 0) red[t >> 5] = ss;
     __syncthreads();
-    if (t < 64 && i0 + t < tw.m)
-        ws.Rmx(tw.slot)[(size_t)(i0 + t) * ((ws.n_max + 63) / 64) + blockIdx.y] =
-            fmax(fmax(rmx[0][t], rmx[1][t]), fmax(rmx[2][t], rmx[3][t]));
-    if (t == 0) {
+    const int nbc = (ws.n_max + 63) / 64;     // 64-column blocks of a tile row
+    const int nblk = (ncol + 63) / 64;
+    for (int q = t; q < 64 * nblk; q += 256) {
+        const int b = q / 64, r = q % 64;
+        if (i0 + r < tw.m)
+            ws.Rmx(tw.slot)[(size_t)(i0 + r) * nbc + blockIdx.y * kGenCb + b] =
+                fmax(fmax(rmx[b][0][r], rmx[b][1][r]), fmax(rmx[b][2][r], rmx[b][3][r]));
+    }
+    if (t < nblk) {
         double a = 0.0;
-        for (int w = 0; w < 8; ++w) a += red[w];
-        ws.Nrm(tw.slot)[blockIdx.x * ((ws.n_max + 63) / 64) + blockIdx.y] = a;
+        for (int w = 0; w < 8; ++w) a += red[t][w];
+        ws.Nrm(tw.slot)[blockIdx.x * nbc + blockIdx.y * kGenCb + t] = a;
     }
 }
 
 void launch_gen_tiles(const DevKernel *d_kernels, const TileWork *d_tiles,
                       int ntiles, Workspace ws, cudaStream_t stream, int need)
 {
-    dim3 grid((ws.m_max + 63) / 64, (ws.n_max + 63) / 64, ntiles);
+    dim3 grid((ws.m_max + 63) / 64, (ws.n_max + 64 * kGenCb - 1) / (64 * kGenCb), ntiles);
     k_gen_tiles<<<grid, 256, 0, stream>>>(d_kernels, d_tiles, ws, need);
 }
 

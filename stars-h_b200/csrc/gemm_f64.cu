@@ -140,6 +140,26 @@ k_gemm_f64(const GemmDesc *__restrict__ descs, int tiles_n)
     }
 
     // Accumulator (i, j, h) holds C(wm + 8i + g, wn + 8j + 2 tig + h).
+    // With beta != 0 the old C values are all read before the first store
+    // (the stores may alias later loads, so loads interleaved with them
+    // would each wait a full memory round trip).
+    double cold[4][2][2];
+    const bool upd = d.beta != 0.0;
+    if (upd) {
+        #pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int gm = m0 + wm + i * 8 + g;
+            #pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                #pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int gn = n0 + wn + j * 8 + 2 * tig + h;
+                    cold[i][j][h] = gm < d.M && gn < d.N
+                                        ? d.C[(size_t)gn * d.ldc + gm] : 0.0;
+                }
+            }
+        }
+    }
     #pragma unroll
     for (int i = 0; i < 4; ++i) {
         const int gm = m0 + wm + i * 8 + g;
@@ -152,7 +172,7 @@ k_gemm_f64(const GemmDesc *__restrict__ descs, int tiles_n)
                 if (gn >= d.N) continue;
                 double *c = d.C + (size_t)gn * d.ldc + gm;
                 double v = d.alpha * acc[i][j][h];
-                if (d.beta != 0.0) v += d.beta * *c;
+                if (upd) v += d.beta * cold[i][j][h];
                 *c = v;
             }
         }

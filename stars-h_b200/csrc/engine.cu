@@ -790,8 +790,14 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
         const bool compact = round_count >= 0;
         make_gemm_descs(step, dt, nt, ws, omega, n_max, out, dd, s, compact);
         count_launch(2);
+        // the transposed products of the adaptive rounds (outputs of a few
+        // basis or sample columns, K = the tile height) split K inside
+        // the CTA where a tile has few columns
+        const bool split_k = step == STEP_A_RES_Z || step == STEP_A_GRAM ||
+                             step == STEP_A_RES_Z2 || step == STEP_A_GRAM2 ||
+                             step == STEP_A_ORTH_Z || step == STEP_A_GRAM_R;
         return gemm_f64_batched(ta, tb, dd, compact ? round_count : nt, mm, nn,
-                                s) == cudaSuccess
+                                s, split_k) == cudaSuccess
                    ? STARSH_SUCCESS
                    : cuda_fail(cudaGetLastError(), "gemm_f64_batched");
     };

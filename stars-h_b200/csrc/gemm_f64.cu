@@ -187,9 +187,12 @@ k_gemm_f64(const GemmDesc *__restrict__ descs, int tiles_n)
 // one K step in flight and waits on memory latency every step.  Operand
 // tiles land in shared memory directly (16-byte cp.async, k contiguous in
 // both operands), two steps ahead of the multiply (60 or 75 KB of shared
-// memory).  Same per-element
-// accumulation order as k_gemm_f64 (K steps of 16 in order, the DMMA's
-// k-order inside a step), so results are identical to it.
+// memory).  Where a tile fills every warp's output region, the per-element
+// accumulation order is that of k_gemm_f64 (K steps of 16 in order, the
+// DMMA's k-order inside a step), so results are identical to it; in a
+// launch that asks for it (split_k), a 64 x 64 tile with at most 32 rows or
+// 48 columns of its own splits K over the spare warps (fixed slice order,
+// deterministic).
 constexpr int kTnStages = 3;
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem, bool pred)
@@ -202,7 +205,7 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem, bool pr
 
 template <int BM, int BN>
 __global__ void __launch_bounds__(kGemmThreads)
-k_gemm_f64_tn_pipe(const GemmDesc *__restrict__ descs, int tiles_n)
+k_gemm_f64_tn_pipe(const GemmDesc *__restrict__ descs, int tiles_n, int split_k)
 {
     constexpr int WARPS_M = BM / 32;
     static_assert(WARPS_M * (BN / 16) == kGemmThreads / 32, "warp grid");
@@ -219,7 +222,25 @@ k_gemm_f64_tn_pipe(const GemmDesc *__restrict__ descs, int tiles_n)
     const int t = threadIdx.x;
     const int lane = t & 31, warp = t >> 5;
     const int g = lane >> 2, tig = lane & 3;
-    const int wm = (warp % WARPS_M) * 32, wn = (warp / WARPS_M) * 16;
+    // Output regions of 32 x 16, one per warp when the tile's own rows and
+    // columns fill the CTA tile.  A 64 x 64 tile with fewer (the products
+    // onto a narrow basis, Grams of a few columns) gives the spare warps a
+    // share of K instead: nreg regions (rounded up to rp, a power of two),
+    // warp w works on region w % rp over the k4 steps q = w / rp modulo
+    // nsl = 8 / rp, and the nsl partial sums are added in slice order
+    // through shared memory.  Every scheduler keeps the same share of the
+    // DMMA work.
+    int rh = WARPS_M, rp = 8, nsl = 1;
+    if constexpr (BM == 64 && BN == 64) if (split_k) {
+        rh = d.M - m0 > 32 ? 2 : 1;
+        const int cq = min(4, (d.N - n0 + 15) / 16);
+        const int nreg = rh * cq;
+        rp = nreg <= 1 ? 1 : nreg <= 2 ? 2 : nreg <= 4 ? 4 : 8;
+        nsl = 8 / rp;
+    }
+    const int reg = warp % rp, slice = warp / rp;
+    const int wm = (reg % rh) * 32, wn = (reg / rh) * 16;
+    const bool live = wm < BM && wn < BN && m0 + wm < d.M && n0 + wn < d.N;
     double acc[4][2][2];
     #pragma unroll
     for (int i = 0; i < 4; ++i)
@@ -277,7 +298,10 @@ k_gemm_f64_tn_pipe(const GemmDesc *__restrict__ descs, int tiles_n)
         const double *Ab = As + st * BM * kGemmLds;
         const double *Bb = Bs + st * BN * kGemmLds;
         #pragma unroll
-        for (int kk = 0; kk < kGemmBK; kk += 4) {
+        for (int k4 = 0; k4 < kGemmBK / 4; ++k4) {
+            // this warp's k4 steps (warp-uniform)
+            if (!live || ((kt * (kGemmBK / 4) + k4 - slice) & (nsl - 1)) != 0) continue;
+            const int kk = k4 * 4;
             double af[4], bf[2];
             #pragma unroll
             for (int i = 0; i < 4; ++i) af[i] = Ab[(wm + i * 8 + g) * kGemmLds + kk + tig];
@@ -291,6 +315,30 @@ k_gemm_f64_tn_pipe(const GemmDesc *__restrict__ descs, int tiles_n)
         }
     }
     asm volatile("cp.async.wait_group 0;");
+    if (nsl > 1) {
+        // partial sums of the slices, [warp][16 accumulators][32 lanes]
+        // over the stage buffers, added by slice 0 in slice order
+        __syncthreads();
+        double *part = gemm_smem + warp * 512;
+        #pragma unroll
+        for (int i = 0; i < 4; ++i)
+            #pragma unroll
+            for (int j = 0; j < 2; ++j)
+                #pragma unroll
+                for (int h = 0; h < 2; ++h) part[((i * 2 + j) * 2 + h) * 32 + lane] = acc[i][j][h];
+        __syncthreads();
+        if (slice != 0) return;
+        for (int q = 1; q < nsl; ++q) {
+            const double *pq = gemm_smem + (warp + q * rp) * 512;
+            #pragma unroll
+            for (int i = 0; i < 4; ++i)
+                #pragma unroll
+                for (int j = 0; j < 2; ++j)
+                    #pragma unroll
+                    for (int h = 0; h < 2; ++h) acc[i][j][h] += pq[((i * 2 + j) * 2 + h) * 32 + lane];
+        }
+    }
+    if (!live) return;
     #pragma unroll
     for (int i = 0; i < 4; ++i) {
         const int gm = m0 + wm + i * 8 + g;
@@ -435,15 +483,17 @@ static void launch_shape(bool ta, bool tb, const GemmDesc *dd, int nb,
 
 cudaError_t gemm_f64_batched(bool ta, bool tb, const GemmDesc *d_desc,
                              int batch, int max_m, int max_n,
-                             cudaStream_t stream)
+                             cudaStream_t stream, bool split_k)
 {
     if (batch <= 0 || max_m <= 0 || max_n <= 0) return cudaSuccess;
+    split_k = split_k && ta && !tb;
     // CTA shape: 64 x 64, or 32 x 128 when the output is wide and (as for
     // the projection B = Q^T D and the rotation C = W^T B) its rows are a
     // basis much narrower than the batch maximum, or 128 x 32 for narrow
-    // outputs (sketch blocks of 32 columns)
+    // outputs (sketch blocks of 32 columns); 64 x 64 always with split_k
     int bm = 64, bn = 64;
-    if (ta && !tb && max_n >= 256) { bm = 32; bn = 128; }
+    if (split_k) { }
+    else if (ta && !tb && max_n >= 256) { bm = 32; bn = 128; }
     else if (max_n <= 32 && max_m >= 128) { bm = 128; bn = 32; }
     const int tiles_m = (max_m + bm - 1) / bm;
     const int tiles_n = (max_n + bn - 1) / bn;
@@ -466,9 +516,9 @@ cudaError_t gemm_f64_batched(bool ta, bool tb, const GemmDesc *d_desc,
                                      (int)smem32);
             });
             if (bm == 64)
-                k_gemm_f64_tn_pipe<64, 64><<<grid, kGemmThreads, smem64, stream>>>(dd, tiles_n);
+                k_gemm_f64_tn_pipe<64, 64><<<grid, kGemmThreads, smem64, stream>>>(dd, tiles_n, split_k ? 1 : 0);
             else
-                k_gemm_f64_tn_pipe<32, 128><<<grid, kGemmThreads, smem32, stream>>>(dd, tiles_n);
+                k_gemm_f64_tn_pipe<32, 128><<<grid, kGemmThreads, smem32, stream>>>(dd, tiles_n, 0);
         } else if (!ta && tb && bm == 64) {
             dim3 grid(tiles_m * tiles_n, nb);
             constexpr size_t smem = (size_t)kTnStages * 2 * kGemmBK * kNtLds * sizeof(double);

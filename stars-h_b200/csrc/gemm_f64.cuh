@@ -29,9 +29,13 @@ constexpr int kGemmLds = kGemmBK + 4;
 
 // Launches one GEMM per descriptor; entries whose M, N or K is 0 are
 // skipped (beta is still applied when K == 0).  max_m/max_n bound the
-// shapes of all entries.  Returns the CUDA error of the launch.
+// shapes of all entries.  split_k (A^T B only): every entry runs on 64 x 64
+// CTA tiles whatever the bounds, and a tile with few rows or columns of
+// its own splits K over the spare warps; an entry's result then depends on
+// its own shape alone, never on the bounds of the batch it is in.
+// Returns the CUDA error of the launch.
 cudaError_t gemm_f64_batched(bool ta, bool tb, const GemmDesc *d_desc,
                              int batch, int max_m, int max_n,
-                             cudaStream_t stream);
+                             cudaStream_t stream, bool split_k = false);
 
 }  // namespace b200

@@ -2,10 +2,14 @@
 //
 // CTA tile 64 x 64, 32 x 128 or 128 x 32, K step 16, 8 warps of 32 x 16
 // output each (4 x 2 fragments of the m8n8k4 DMMA).  Operand tiles are staged
-// in shared memory as [row][k] (A) and [col][k] (B) with row stride 20,
-// double-buffered, the next K tile is fetched into registers while the
-// current one is multiplied.  Global loads are coalesced along whichever
-// dimension is contiguous for the given transpose flag.
+// in shared memory double-buffered, the next K tile is fetched into
+// registers while the current one is multiplied.  Global loads are
+// coalesced along whichever dimension is contiguous for the given transpose
+// flag, and the staging layout follows it: [row][k] with row stride 20 where
+// k is contiguous, [k][row] with stride rows + 4 where rows are, so that
+// both the stores and the fragment reads are free of bank conflicts.  Warps
+// skip the DMMAs of output regions outside the tile's own M x N and of k4
+// steps past its K (those would add exact zeros).
 #include <cstdint>
 #include <mutex>
 #include "gemm_f64.cuh"
@@ -22,8 +26,10 @@ __device__ __forceinline__ void dmma_8x8x4(double &c0, double &c1, double a,
         : "d"(a), "d"(b));
 }
 
+// The A B products (basis updates with K <= 64 and beta updates) keep
+// three CTAs per SM: their short K makes them latency-bound.
 template <bool TA, bool TB, int BM, int BN>
-__global__ void __launch_bounds__(kGemmThreads)
+__global__ void __launch_bounds__(kGemmThreads, (!TA && !TB) ? 3 : 0)
 k_gemm_f64(const GemmDesc *__restrict__ descs, int tiles_n)
 {
     // 8 warps of 32 x 16 output each, BM / 32 along M and BN / 16 along N
@@ -94,18 +100,26 @@ k_gemm_f64(const GemmDesc *__restrict__ descs, int tiles_n)
             rb[r] = v;
         }
     };
+    // shared-memory index of (row, k) of A and (col, k) of B
+    constexpr int LDA_K = BM + 4, LDB_K = BN + 4;   // [k][row] strides
+    auto a_at = [](int row, int kk) {
+        return TA ? row * kGemmLds + kk : kk * LDA_K + row;
+    };
+    auto b_at = [](int col, int kk) {
+        return TB ? kk * LDB_K + col : col * kGemmLds + kk;
+    };
     auto store_tiles = [&](int buf) {
         #pragma unroll
         for (int r = 0; r < RA; ++r) {
             int row, kk;
             a_coord(r, row, kk);
-            As[buf][row * kGemmLds + kk] = ra[r];
+            As[buf][a_at(row, kk)] = ra[r];
         }
         #pragma unroll
         for (int r = 0; r < RB; ++r) {
             int col, kk;
             b_coord(r, col, kk);
-            Bs[buf][col * kGemmLds + kk] = rb[r];
+            Bs[buf][b_at(col, kk)] = rb[r];
         }
     };
 
@@ -115,18 +129,25 @@ k_gemm_f64(const GemmDesc *__restrict__ descs, int tiles_n)
         store_tiles(0);
         __syncthreads();
     }
+    // this warp's 32 x 16 output region holds part of the tile's M x N
+    const bool live = m0 + wm < d.M && n0 + wn < d.N;
     for (int kt = 0; kt < ktiles; ++kt) {
         const int buf = kt & 1;
         if (kt + 1 < ktiles) load_tiles((kt + 1) * kGemmBK);
+        // k4 steps of this warp in the K step (warp-uniform; A B products
+        // only, the other forms keep every step)
+        const int kend = (TA || TB) ? kGemmBK
+                         : live ? min(kGemmBK, d.K - kt * kGemmBK) : 0;
         #pragma unroll
         for (int kk = 0; kk < kGemmBK; kk += 4) {
+            if (kk >= kend) break;
             double af[4], bf[2];
             #pragma unroll
             for (int i = 0; i < 4; ++i)
-                af[i] = As[buf][(wm + i * 8 + g) * kGemmLds + kk + tig];
+                af[i] = As[buf][a_at(wm + i * 8 + g, kk + tig)];
             #pragma unroll
             for (int j = 0; j < 2; ++j)
-                bf[j] = Bs[buf][(wn + j * 8 + g) * kGemmLds + kk + tig];
+                bf[j] = Bs[buf][b_at(wn + j * 8 + g, kk + tig)];
             #pragma unroll
             for (int i = 0; i < 4; ++i)
                 #pragma unroll

@@ -791,11 +791,13 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
         make_gemm_descs(step, dt, nt, ws, omega, n_max, out, dd, s, compact);
         count_launch(2);
         // the transposed products of the adaptive rounds (outputs of a few
-        // basis or sample columns, K = the tile height) split K inside
-        // the CTA where a tile has few columns
+        // basis or sample columns, K = the tile height) and the Gram B B^T
+        // of the small SVD (K = the tile width) split K inside the CTA
+        // where a tile has few rows or columns
         const bool split_k = step == STEP_A_RES_Z || step == STEP_A_GRAM ||
                              step == STEP_A_RES_Z2 || step == STEP_A_GRAM2 ||
-                             step == STEP_A_ORTH_Z || step == STEP_A_GRAM_R;
+                             step == STEP_A_ORTH_Z || step == STEP_A_GRAM_R ||
+                             step == STEP_GRAM_B;
         return gemm_f64_batched(ta, tb, dd, compact ? round_count : nt, mm, nn,
                                 s, split_k) == cudaSuccess
                    ? STARSH_SUCCESS

@@ -384,12 +384,14 @@ k_gemm_f64_tn_pipe(const GemmDesc *__restrict__ descs, int tiles_n, int split_k)
 // transposed products.  Here rows are contiguous in both operands and k is
 // strided, so the tiles are staged as [k][row] (row stride 68 doubles:
 // fragment reads free of bank conflicts); a 16-byte piece is two
-// consecutive rows at one k.  Same per-element accumulation order as
-// k_gemm_f64 (K steps of 16 in order), so results are identical to it.
+// consecutive rows at one k.  Without split_k the per-element accumulation
+// order is that of k_gemm_f64 (K steps of 16 in order), so results are
+// identical to it; with it, K is split over the warps of empty output
+// regions as in the transposed kernel.
 constexpr int kNtLds = 64 + 4;
 
 __global__ void __launch_bounds__(kGemmThreads)
-k_gemm_f64_nt_pipe(const GemmDesc *__restrict__ descs, int tiles_n)
+k_gemm_f64_nt_pipe(const GemmDesc *__restrict__ descs, int tiles_n, int split_k)
 {
     constexpr int BM = 64, BN = 64;
     const GemmDesc d = descs[blockIdx.y];
@@ -403,7 +405,19 @@ k_gemm_f64_nt_pipe(const GemmDesc *__restrict__ descs, int tiles_n)
     const int t = threadIdx.x;
     const int lane = t & 31, warp = t >> 5;
     const int g = lane >> 2, tig = lane & 3;
-    const int wm = (warp % 2) * 32, wn = (warp / 2) * 16;
+    // output regions, K slices and 8-row fragments as in the transposed
+    // kernel above
+    int rh = 2, rp = 8, nsl = 1;
+    if (split_k) {
+        rh = d.M - m0 > 32 ? 2 : 1;
+        const int cq = min(4, (d.N - n0 + 15) / 16);
+        const int nreg = rh * cq;
+        rp = nreg <= 1 ? 1 : nreg <= 2 ? 2 : nreg <= 4 ? 4 : 8;
+        nsl = 8 / rp;
+    }
+    const int reg = warp % rp, slice = warp / rp;
+    const int wm = (reg % rh) * 32, wn = (reg / rh) * 16;
+    const bool live = wm < BM && wn < BN && m0 + wm < d.M && n0 + wn < d.N;
     double acc[4][2][2];
     #pragma unroll
     for (int i = 0; i < 4; ++i)
@@ -451,7 +465,9 @@ k_gemm_f64_nt_pipe(const GemmDesc *__restrict__ descs, int tiles_n)
         const double *Ab = As + st * kGemmBK * kNtLds;
         const double *Bb = Bs + st * kGemmBK * kNtLds;
         #pragma unroll
-        for (int kk = 0; kk < kGemmBK; kk += 4) {
+        for (int k4 = 0; k4 < kGemmBK / 4; ++k4) {
+            if (!live || ((kt * (kGemmBK / 4) + k4 - slice) & (nsl - 1)) != 0) continue;
+            const int kk = k4 * 4;
             double af[4], bf[2];
             #pragma unroll
             for (int i = 0; i < 4; ++i) af[i] = Ab[(kk + tig) * kNtLds + wm + i * 8 + g];
@@ -465,6 +481,28 @@ k_gemm_f64_nt_pipe(const GemmDesc *__restrict__ descs, int tiles_n)
         }
     }
     asm volatile("cp.async.wait_group 0;");
+    if (nsl > 1) {
+        __syncthreads();
+        double *part = gemm_smem + warp * 512;
+        #pragma unroll
+        for (int i = 0; i < 4; ++i)
+            #pragma unroll
+            for (int j = 0; j < 2; ++j)
+                #pragma unroll
+                for (int h = 0; h < 2; ++h) part[((i * 2 + j) * 2 + h) * 32 + lane] = acc[i][j][h];
+        __syncthreads();
+        if (slice != 0) return;
+        for (int q = 1; q < nsl; ++q) {
+            const double *pq = gemm_smem + (warp + q * rp) * 512;
+            #pragma unroll
+            for (int i = 0; i < 4; ++i)
+                #pragma unroll
+                for (int j = 0; j < 2; ++j)
+                    #pragma unroll
+                    for (int h = 0; h < 2; ++h) acc[i][j][h] += pq[((i * 2 + j) * 2 + h) * 32 + lane];
+        }
+    }
+    if (!live) return;
     #pragma unroll
     for (int i = 0; i < 4; ++i) {
         const int gm = m0 + wm + i * 8 + g;
@@ -507,7 +545,7 @@ cudaError_t gemm_f64_batched(bool ta, bool tb, const GemmDesc *d_desc,
                              cudaStream_t stream, bool split_k)
 {
     if (batch <= 0 || max_m <= 0 || max_n <= 0) return cudaSuccess;
-    split_k = split_k && ta && !tb;
+    split_k = split_k && ta != tb;
     // CTA shape: 64 x 64, or 32 x 128 when the output is wide and (as for
     // the projection B = Q^T D and the rotation C = W^T B) its rows are a
     // basis much narrower than the batch maximum, or 128 x 32 for narrow
@@ -549,7 +587,7 @@ cudaError_t gemm_f64_batched(bool ta, bool tb, const GemmDesc *d_desc,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)smem);
             });
-            k_gemm_f64_nt_pipe<<<grid, kGemmThreads, smem, stream>>>(dd, tiles_n);
+            k_gemm_f64_nt_pipe<<<grid, kGemmThreads, smem, stream>>>(dd, tiles_n, split_k ? 1 : 0);
         } else if (bm == 32) launch_shape<32, 128>(ta, tb, dd, nb, tiles_m, tiles_n, stream);
         else if (bm == 128) launch_shape<128, 32>(ta, tb, dd, nb, tiles_m, tiles_n, stream);
         else launch_shape<64, 64>(ta, tb, dd, nb, tiles_m, tiles_n, stream);

@@ -29,7 +29,7 @@ constexpr int kGemmLds = kGemmBK + 4;
 
 // Launches one GEMM per descriptor; entries whose M, N or K is 0 are
 // skipped (beta is still applied when K == 0).  max_m/max_n bound the
-// shapes of all entries.  split_k (A^T B only): every entry runs on 64 x 64
+// shapes of all entries.  split_k (A^T B and A B^T): every entry runs on 64 x 64
 // CTA tiles whatever the bounds, and a tile with few rows or columns of
 // its own splits K over the spare warps; an entry's result then depends on
 // its own shape alone, never on the bounds of the batch it is in.

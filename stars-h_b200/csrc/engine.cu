@@ -335,35 +335,60 @@ void fill_kernel(DevKernel &K, const b200_kspec &sp)
     }
 }
 
-// Chebyshev coefficients of G(x) = x^nu e^x K_nu(x) on each interval
-// [2^E, 2^(E+1)], E = q + kMaternTabEmin (one CTA per interval q): G at
-// the kMaternTabDeg + 1 Chebyshev points of the first kind u_j = cos(pi
-// (j + 1/2) / (deg + 1)), x_j = 2^(E-1) (u_j + 3), then c_k = 2 / (deg + 1)
-// sum_j G(x_j) cos(pi k (j + 1/2) / (deg + 1)), c_0 halved (the discrete
-// cosine transform of Chebyshev interpolation).  Node values come from the
-// trapezoidal integral for x >= 2 and from Temme's series below.  The
-// interpolant is accurate to a few units of 1e-15 relative on every
-// interval (G is analytic in the right half-plane, the nearest
-// singularity is at x = 0).
+// Polynomial pieces of G(x) = x^nu e^x K_nu(x) (one CTA per piece q:
+// octave E = q / kMaternTabSub + kMaternTabEmin, eighth j = q %
+// kMaternTabSub, x = 2^E (1 + (2 j + 1 + u) / 16), u in [-1, 1)).  G at
+// the kMaternTabDeg + 1 Chebyshev points of the first kind u_i = cos(pi
+// (i + 1/2) / (deg + 1)) gives the interpolant's Chebyshev coefficients
+// c_k = 2 / (deg + 1) sum_i G(x_i) cos(pi k (i + 1/2) / (deg + 1)), c_0
+// halved (the discrete cosine transform of Chebyshev interpolation); one
+// thread turns them into monomial coefficients in u through the
+// recurrence T_{k+1} = 2 u T_k - T_{k-1} (integer coefficients, exact in
+// double; the terms decay like 34^-k, so the sum loses no digits).  Node
+// values come from the trapezoidal integral for x >= 2 and from Temme's
+// series below.
 __global__ void k_matern_table(double nu, double *tab)
 {
     constexpr int N1 = kMaternTabDeg + 1;
-    __shared__ double g[N1];
-    const int q = blockIdx.x, j = threadIdx.x;
-    if (j < N1) {
-        // node j of interval [2^E, 2^(E+1)), E = q + kMaternTabEmin
-        const double u = cospi((j + 0.5) / N1);
-        const double x = ldexp(u + 3.0, q + kMaternTabEmin - 1);
-        g[j] = x >= 2.0
+    __shared__ double g[N1], cc[N1];
+    const int q = blockIdx.x, i = threadIdx.x;
+    const int E = q / kMaternTabSub + kMaternTabEmin, jp = q % kMaternTabSub;
+    if (i < N1) {
+        const double u = cospi((i + 0.5) / N1);
+        const double x = ldexp(1.0 + (2 * jp + 1 + u) / (2.0 * kMaternTabSub), E);
+        g[i] = x >= 2.0
             ? exp(nu * log(x)) * bessel_k_large_scaled(nu, x, 2.0)
             : exp(nu * log(x) + x) * bessel_knu(nu, x);
     }
     __syncthreads();
-    if (j < N1) {
+    if (i < N1) {
         double c = 0.0;
-        for (int i = 0; i < N1; ++i) c += g[i] * cospi(j * (i + 0.5) / N1);
+        for (int k = 0; k < N1; ++k) c += g[k] * cospi(i * (k + 0.5) / N1);
         c *= 2.0 / N1;
-        tab[q * N1 + j] = j == 0 ? 0.5 * c : c;
+        cc[i] = i == 0 ? 0.5 * c : c;
+    }
+    __syncthreads();
+    if (i == 0) {
+        double a[N1], t0[N1], t1[N1];
+        #pragma unroll
+        for (int k = 0; k < N1; ++k) { a[k] = 0.0; t0[k] = 0.0; t1[k] = 0.0; }
+        t0[0] = 1.0;                 // T_0
+        t1[1] = 1.0;                 // T_1
+        a[0] = cc[0];
+        a[1] = cc[1];
+        #pragma unroll
+        for (int k = 2; k < N1; ++k) {
+            #pragma unroll
+            for (int e = N1 - 1; e >= 0; --e) {
+                const double t2 = (e > 0 ? 2.0 * t1[e - 1] : 0.0) - t0[e];
+                t0[e] = t1[e];
+                t1[e] = t2;
+                a[e] += cc[k] * t2;
+            }
+        }
+        #pragma unroll
+        for (int k = 0; k < kMaternTabStride; ++k)
+            tab[(size_t)q * kMaternTabStride + k] = k < N1 ? a[k] : 0.0;
     }
 }
 
@@ -375,12 +400,12 @@ static int prepare_kernel_tables(DevicePoints &dp, cudaStream_t s)
     K.matern_tab = nullptr;
     if ((K.family == FAM_MATERN || K.family == FAM_MATERN2) &&
         K.matern_half == 0 && K.nu > 0.0) {
-        const size_t n = (size_t)kMaternTabIntervals * (kMaternTabDeg + 1);
+        const size_t n = (size_t)kMaternTabPieces * kMaternTabStride;
         double *tab = (double *)pool_alloc(n * sizeof(double), s);
         if (tab == nullptr)
             return cuda_fail(cudaErrorMemoryAllocation, "Matern table");
         dp.owned.push_back(tab);
-        k_matern_table<<<kMaternTabIntervals, 32, 0, s>>>(K.nu, tab);
+        k_matern_table<<<kMaternTabPieces, 32, 0, s>>>(K.nu, tab);
         count_launch();
         B200_CUDA(cudaGetLastError(), "k_matern_table");
         K.matern_tab = tab;

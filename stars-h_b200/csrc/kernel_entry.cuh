@@ -34,9 +34,9 @@ struct DevKernel {
     double sigma, beta, nu, noise;
     double matern_coef, matern_scale;
     int matern_half;          // 1, 2, 3 for nu = 1/2, 3/2, 5/2; else 0
-    // Matérn with other nu: Chebyshev coefficients of x^nu e^x K_nu(x) on
-    // [2^E, 2^(E+1)), kMaternTabEmin <= E < kMaternTabEmin +
-    // kMaternTabIntervals (device, or null)
+    // Matérn with other nu: polynomial pieces of x^nu e^x K_nu(x) on the
+    // eighths of [2^E, 2^(E+1)), kMaternTabEmin <= E < kMaternTabEmin +
+    // kMaternTabIntervals (device, 16-byte aligned, or null)
     const double *matern_tab;
     double inv_neg_beta;      // -1/beta (exp)
     double inv_neg_2beta2;    // 1/((-2 beta) beta) (square exponential)
@@ -50,13 +50,20 @@ struct DevKernel {
 };
 
 // Matérn table: kMaternTabIntervals dyadic intervals covering
-// [2^-10, 1024), each with kMaternTabDeg + 1 Chebyshev coefficients.  On
-// every interval [a, 2a) the function is analytic except at x = 0, which
-// lies at u = -3 of the interval's [-1, 1): the same Bernstein ellipse
-// (rho = 3 + 2 sqrt 2) at every scale, so one degree serves all of them.
-constexpr int kMaternTabDeg = 18;
+// [2^-10, 1024), each cut into kMaternTabSub equal pieces (the top three
+// mantissa bits of x), each piece a polynomial of degree kMaternTabDeg in
+// the piece's own variable u in [-1, 1), monomial coefficients, stored
+// kMaternTabStride doubles apart (the last slot zero).  The function is
+// analytic except at x = 0, which lies at u <= -17 for every piece: a
+// Bernstein ellipse of rho >= 17 + 12 sqrt 2 ~ 34 at every scale, so
+// degree 10 interpolates it to rounding (<= 2.1e-16 relative against
+// mpmath for 0.2 <= nu <= 4.7, Horner in double).
+constexpr int kMaternTabDeg = 10;
+constexpr int kMaternTabSub = 8;
+constexpr int kMaternTabStride = 12;
 constexpr int kMaternTabEmin = -10;
 constexpr int kMaternTabIntervals = 20;
+constexpr int kMaternTabPieces = kMaternTabIntervals * kMaternTabSub;
 constexpr double kMaternTabLo = 0.0009765625;   // 2^kMaternTabEmin
 
 // Taylor coefficients of 1/Gamma(1+z) about z = 0 (a_0 = 1, a_1 = Euler's
@@ -189,23 +196,37 @@ __device__ inline double bessel_k_large(double nu, double x)
     return bessel_k_large_scaled(nu, x, 1.0) * exp(-x);
 }
 
-// x^nu e^x K_nu(x) for 2^-10 <= x < 1024 from the problem's Chebyshev
-// table: x = 2^E m, m in [1, 2), lies in interval E - kMaternTabEmin, at
-// u = 2 m - 3 in [-1, 1) (exact); Clenshaw's recurrence sums the series.
+// x^nu e^x K_nu(x) for 2^-10 <= x < 1024 from the problem's table.  With
+// x = 2^E (1 + (j + f) / 8), j the top three mantissa bits and f in [0, 1)
+// the other 49, the piece is 8 (E - kMaternTabEmin) + j (the high word
+// shifted right by 17 holds the biased exponent and j) and u = 2 f - 1,
+// formed exactly from the mantissa bits; Horner's rule sums the piece.
 __device__ __forceinline__ double matern_tab_eval(const double *tab, double x)
 {
-    const int E = (__double2hiint(x) >> 20) - 1023;
-    const double *c = tab + (size_t)(E - kMaternTabEmin) * (kMaternTabDeg + 1);
-    const double u = x * __hiloint2double((1024 - E) << 20, 0) - 3.0;
-    const double u2 = 2.0 * u;
-    double b1 = 0.0, b2 = 0.0;
-    #pragma unroll
-    for (int k = kMaternTabDeg; k >= 1; --k) {
-        const double b0 = fma(u2, b1, c[k] - b2);
-        b2 = b1;
-        b1 = b0;
-    }
-    return fma(u, b1, c[0] - b2);
+    const int hi = __double2hiint(x), lo = __double2loint(x);
+    const int piece = (hi >> 17) - ((1023 + kMaternTabEmin) << 3);
+    // 1 + f: the low 49 mantissa bits moved to the top, exponent of 1.0
+    const double z = __hiloint2double(
+        0x3FF00000 | (int)(__funnelshift_l((unsigned)lo, (unsigned)hi, 3) & 0x000FFFFFu),
+        (int)((unsigned)lo << 3));
+    const double u = fma(z, 2.0, -3.0);
+    const double2 *c = reinterpret_cast<const double2 *>(
+        tab + (size_t)piece * kMaternTabStride);
+    const double2 c01 = __ldg(c), c23 = __ldg(c + 1), c45 = __ldg(c + 2),
+                  c67 = __ldg(c + 3), c89 = __ldg(c + 4), c10 = __ldg(c + 5);
+    static_assert(kMaternTabDeg == 10 && kMaternTabStride == 12,
+                  "Horner chain written for degree 10");
+    double p = c10.x;
+    p = fma(p, u, c89.y);
+    p = fma(p, u, c89.x);
+    p = fma(p, u, c67.y);
+    p = fma(p, u, c67.x);
+    p = fma(p, u, c45.y);
+    p = fma(p, u, c45.x);
+    p = fma(p, u, c23.y);
+    p = fma(p, u, c23.x);
+    p = fma(p, u, c01.y);
+    return fma(p, u, c01.x);
 }
 
 // K_nu(x), nu >= 0, x > 0.  Small arguments: Temme's series at

@@ -91,6 +91,9 @@ constexpr int kGenCb = GEN_CB;
 #define GEN_UNROLL 8          // entries of a thread evaluated together
 #endif
 constexpr int kGenUnroll = GEN_UNROLL;
+#ifndef GEN_UNROLL_MATERN
+#define GEN_UNROLL_MATERN 2   // the same for the Matérn families
+#endif
 
 // The entries of one thread in a 64 x 64 block: rows ii, columns jj0,
 // jj0 + 4, ... below jn, written to Dcol[jj * ld] (Dcol points at row ii of
@@ -112,10 +115,10 @@ __device__ __forceinline__ double gen_entries(
     }
     double ss = 0.0;
     amax = 0.0;
-    // the Matern entry (series or table per entry) keeps the shorter
-    // unroll: eight of its bodies cost more registers than they save
+    // the Matern entry (table piece per entry) keeps a shorter unroll:
+    // more of its bodies cost more registers than they save
     constexpr int kUnroll =
-        FAM == FAM_MATERN || FAM == FAM_MATERN2 ? 4 : kGenUnroll;
+        FAM == FAM_MATERN || FAM == FAM_MATERN2 ? GEN_UNROLL_MATERN : kGenUnroll;
     #pragma unroll kUnroll
     for (int jj = jj0; jj < jn; jj += 4) {
         double dist = 0.0;

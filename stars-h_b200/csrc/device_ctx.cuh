@@ -42,6 +42,12 @@ struct Context {
     // that their uploads do not wait for the stream)
     void *tiles_pin[2] = {nullptr, nullptr};
     size_t tiles_pin_bytes = 0;
+    // page-locked host memory mapped into the device, for the small reads
+    // the host waits on (a round's sampling count, a batch's tile
+    // records): a kernel stores them there, so they do not queue on a copy
+    // engine behind the batch downloads of `copy`
+    void *mapped = nullptr;
+    void *mapped_dev = nullptr;
     std::mutex lock;           // one approximation / dmml at a time
 };
 

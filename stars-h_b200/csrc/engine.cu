@@ -192,6 +192,7 @@ void context_free_private(Context *c)
     c->act.release();
     c->kernels.release();
     c->omega8.release();
+    if (c->mapped) cudaFreeHost(c->mapped);
     for (int i = 0; i < 2; ++i) {
         if (c->stage[i]) cudaFreeHost(c->stage[i]);
         if (c->stage_ev[i]) cudaEventDestroy(c->stage_ev[i]);
@@ -562,6 +563,43 @@ static void cluster_boxes(const double *pts, long long count, int ndim,
         }
 }
 
+// The context's mapped host area: the round count at offset 0, a batch's
+// tile records (at most kMaxBatchTiles) from offset 256.  Allocated once
+// per context at its first approximation.
+constexpr long long kMaxBatchTiles = 4096;
+constexpr size_t kMappedRecords = 256;
+
+static int mapped_area(Context &ctx)
+{
+    if (ctx.mapped != nullptr) return STARSH_SUCCESS;
+    const size_t bytes = kMappedRecords + (size_t)kMaxBatchTiles * sizeof(TileWork);
+    void *h = nullptr, *d = nullptr;
+    B200_CUDA(cudaHostAlloc(&h, bytes, cudaHostAllocMapped), "cudaHostAlloc(mapped)");
+    const cudaError_t e = cudaHostGetDevicePointer(&d, h, 0);
+    if (e != cudaSuccess) {
+        cudaFreeHost(h);
+        return cuda_fail(e, "cudaHostGetDevicePointer");
+    }
+    ctx.mapped = h;
+    ctx.mapped_dev = d;
+    return STARSH_SUCCESS;
+}
+
+// Stores `words` 8-byte words of device memory into mapped host memory
+// (visible to the host once the stream has passed the kernel).
+__global__ void k_store_to_host(const unsigned long long *__restrict__ src,
+                                unsigned long long *dst, size_t words)
+{
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < words;
+         i += (size_t)gridDim.x * blockDim.x)
+        dst[i] = src[i];
+}
+
+__global__ void k_count_to_host(const int *__restrict__ src, int *dst)
+{
+    *dst = *src;
+}
+
 // Runs the device pipeline over the far blocks of every problem of `jobs`
 // in shared batches: tiles of different problems (kernels, sizes, tol,
 // maxrank) share every launch.  Fills each job's ranks and the per-block
@@ -584,6 +622,7 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
         }
     } drain{ctx.copy};
     cudaStream_t s = ctx.stream;
+    if (const int e = mapped_area(ctx)) return e;
     starsh_b200_stats &st = thread_stats();
     std::vector<TileWork> all;
     std::vector<std::pair<int, STARSH_int>> owner;   // (job, far block)
@@ -742,7 +781,7 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
         int bm = all[b0].m, bn = all[b0].n, bk = all[b0].k;
         size_t stride = workspace_layout(probe, bm, bn, bk, true, proj_i8);
         long long cap = (long long)(budget / (stride * sizeof(double)));
-        cap = std::max<long long>(1, std::min<long long>({cap, ntot - b0, 4096}));
+        cap = std::max<long long>(1, std::min<long long>({cap, ntot - b0, kMaxBatchTiles}));
         for (long long q = b0; q < b0 + cap; ++q) {
             bm = std::max(bm, all[q].m);
             bn = std::max(bn, all[q].n);
@@ -965,10 +1004,11 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
             // without waiting for the flag; later rounds read how many
             // tiles sample and run their GEMMs over those alone
             if (round > 0 || !any_width) {
-                int active = 0;
-                B200_CUDA(cudaMemcpyAsync(&active, d_active, sizeof(int),
-                                          cudaMemcpyDeviceToHost, s), "round flag");
+                k_count_to_host<<<1, 1, 0, s>>>(d_active, (int *)ctx.mapped_dev);
+                count_launch();
+                B200_CUDA(cudaGetLastError(), "k_count_to_host");
                 B200_CUDA(cudaStreamSynchronize(s), "round flag");
+                const int active = *(volatile int *)ctx.mapped;
                 if (!active) break;
                 round_count = active;
             }
@@ -1042,10 +1082,18 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
         launch_rank_cut(dt, nt, ws, s);
         count_launch();
         cudaEventRecord(ev[6], s);
-        B200_CUDA(cudaMemcpyAsync(&all[b0], dt, nt * sizeof(TileWork),
-                                  cudaMemcpyDeviceToHost, s),
-                  "cudaMemcpyAsync(tiles)");
+        {
+            static_assert(sizeof(TileWork) % 8 == 0, "TileWork in 8-byte words");
+            const size_t words = (size_t)nt * sizeof(TileWork) / 8;
+            k_store_to_host<<<(unsigned)std::min<size_t>(296, (words + 255) / 256), 256, 0, s>>>(
+                (const unsigned long long *)dt,
+                (unsigned long long *)((char *)ctx.mapped_dev + kMappedRecords), words);
+            count_launch();
+            B200_CUDA(cudaGetLastError(), "k_store_to_host");
+        }
         B200_CUDA(cudaStreamSynchronize(s), "compression pipeline");
+        memcpy(&all[b0], (const char *)ctx.mapped + kMappedRecords,
+               (size_t)nt * sizeof(TileWork));
         st.project_ms += phase_ms(2, 3);
         st.gen_ms += phase_ms(4, 5);
         if (fused) {

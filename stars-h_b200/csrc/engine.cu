@@ -693,6 +693,11 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
                               kernels.size() * sizeof(DevKernel),
                               cudaMemcpyHostToDevice, s), "kernel table");
     const DevKernel *d_kernels = (const DevKernel *)ctx.kernels.ptr;
+    // the kernel family every problem of the call shares, or 0 (the
+    // generator then reads each tile's family)
+    int one_family = kernels.empty() ? 0 : kernels[0].family;
+    for (const DevKernel &K : kernels)
+        if (K.family != one_family) one_family = 0;
     // Gaussian sketch, shared by every tile (as the reference reuses the
     // same iseed for every block): n_max x k_max, ld n_max.
     if (ctx.omega_rows != n_max || ctx.omega_cols != k_max) {
@@ -901,7 +906,8 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
             launch_round_setup(dt, nt, ep.block, (int *)ctx.flag.ptr,
                                (int *)ctx.act.ptr, s);
             if (any_separate) {
-                launch_gen_tiles(d_kernels, dt, nt, ws, s, TILE_GEN_SEPARATE);
+                launch_gen_tiles(d_kernels, dt, nt, ws, s, TILE_GEN_SEPARATE,
+                                 one_family);
                 count_launch();
             }
             if (!launch_gen_sketch_i8(d_kernels, dt, nt, ws, om8, ld_om8,
@@ -916,7 +922,7 @@ static int compress_multi(Context &ctx, std::vector<ProblemJob> &jobs,
             const cudaError_t ce = cudaGetLastError();
             if (ce != cudaSuccess) { info = cuda_fail(ce, "k_gen_sketch_i8"); break; }
         } else {
-            launch_gen_tiles(d_kernels, dt, nt, ws, s);
+            launch_gen_tiles(d_kernels, dt, nt, ws, s, 0, one_family);
             count_launch();
         }
         cudaEventRecord(ev[5], s);

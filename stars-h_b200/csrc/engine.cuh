@@ -148,9 +148,11 @@ void make_gemm_descs(GemmStep step, const TileWork *d_tiles, int ntiles,
 // Thresholds come from each tile's tol and maxrank; the generator reads
 // the tile's kernel from d_kernels[tile.prob].
 // need != 0: only tiles whose status has a bit of `need`.
+// family != 0: every tile has that kernel family (a kernel compiled for
+// it alone, where one exists).
 void launch_gen_tiles(const DevKernel *d_kernels, const TileWork *d_tiles,
                       int ntiles, Workspace ws, cudaStream_t stream,
-                      int need = 0);
+                      int need = 0, int family = 0);
 // launch_pivchol and launch_jacobi return the number of kernels launched.
 int launch_pivchol(int phase, const TileWork *d_tiles, TileWork *d_tiles_rw,
                    int ntiles, Workspace ws, cudaStream_t s);

@@ -87,6 +87,12 @@ constexpr int kGenCb = GEN_CB;
 #ifndef GEN_MIN_BLOCKS
 #define GEN_MIN_BLOCKS 3      // CTAs per SM the generator is compiled for
 #endif
+#ifndef GEN_MIN_BLOCKS_FIX
+#define GEN_MIN_BLOCKS_FIX 4  // the same for a launch of one kernel family
+#endif
+#ifndef GEN_MIN_BLOCKS_MATERN
+#define GEN_MIN_BLOCKS_MATERN 4   // ... of the Matérn family (its rare
+#endif                            // series path spills; measured faster)
 #ifndef GEN_UNROLL
 #define GEN_UNROLL 8          // entries of a thread evaluated together
 #endif
@@ -188,7 +194,11 @@ __device__ __forceinline__ double gen_block(
     }
 }
 
-__global__ void __launch_bounds__(256, GEN_MIN_BLOCKS)
+// FIX != 0: every tile of the launch has kernel family FIX (the family's
+// entry code alone, compiled for MINB CTAs per SM); FIX == 0: the family
+// is read per CTA.
+template <int FIX, int MINB>
+__global__ void __launch_bounds__(256, MINB)
 k_gen_tiles(const DevKernel *__restrict__ kernels,
             const TileWork *__restrict__ tiles, Workspace ws, int need)
 {
@@ -237,9 +247,14 @@ k_gen_tiles(const DevKernel *__restrict__ kernels,
         if (jb >= ncol) break;
         double ss = 0.0, amax = 0.0;
         if (i < tw.m)
-            ss = gen_block<W>(K, staged, rc, (const double (*)[W])&cc[0][jb],
-                              ri, ci + jb, ii, t >> 6, min(64, ncol - jb),
-                              D + (size_t)(j0 + jb) * ld + i, ld, amax);
+            ss = FIX == 0
+                ? gen_block<W>(K, staged, rc, (const double (*)[W])&cc[0][jb],
+                               ri, ci + jb, ii, t >> 6, min(64, ncol - jb),
+                               D + (size_t)(j0 + jb) * ld + i, ld, amax)
+                : gen_entries_dim<FIX == 0 ? FAM_EXP : FIX, W>(
+                      K, staged, rc, (const double (*)[W])&cc[0][jb], ri,
+                      ci + jb, ii, t >> 6, min(64, ncol - jb),
+                      D + (size_t)(j0 + jb) * ld + i, ld, amax);
         // largest |D_ij| of each row of the block (the int8 sketch's row
         // scales): the four threads of a row combine through shared memory
         rmx[b][t >> 6][ii] = amax;
@@ -264,10 +279,29 @@ k_gen_tiles(const DevKernel *__restrict__ kernels,
 }
 
 void launch_gen_tiles(const DevKernel *d_kernels, const TileWork *d_tiles,
-                      int ntiles, Workspace ws, cudaStream_t stream, int need)
+                      int ntiles, Workspace ws, cudaStream_t stream, int need,
+                      int family)
 {
     dim3 grid((ws.m_max + 63) / 64, (ws.n_max + 64 * kGenCb - 1) / (64 * kGenCb), ntiles);
-    k_gen_tiles<<<grid, 256, 0, stream>>>(d_kernels, d_tiles, ws, need);
+    switch (family) {
+    case FAM_EXP:
+        k_gen_tiles<FAM_EXP, GEN_MIN_BLOCKS_FIX><<<grid, 256, 0, stream>>>(d_kernels, d_tiles, ws, need);
+        break;
+    case FAM_SQREXP:
+        k_gen_tiles<FAM_SQREXP, GEN_MIN_BLOCKS_FIX><<<grid, 256, 0, stream>>>(d_kernels, d_tiles, ws, need);
+        break;
+    case FAM_MATERN:
+        k_gen_tiles<FAM_MATERN, GEN_MIN_BLOCKS_MATERN><<<grid, 256, 0, stream>>>(d_kernels, d_tiles, ws, need);
+        break;
+    case FAM_COULOMB:
+        k_gen_tiles<FAM_COULOMB, GEN_MIN_BLOCKS_FIX><<<grid, 256, 0, stream>>>(d_kernels, d_tiles, ws, need);
+        break;
+    case FAM_SIN:
+        k_gen_tiles<FAM_SIN, GEN_MIN_BLOCKS_FIX><<<grid, 256, 0, stream>>>(d_kernels, d_tiles, ws, need);
+        break;
+    default:
+        k_gen_tiles<0, GEN_MIN_BLOCKS><<<grid, 256, 0, stream>>>(d_kernels, d_tiles, ws, need);
+    }
 }
 
 // ---------------------------------------------------- Gaussian sketch

@@ -214,7 +214,10 @@ k_gemm_f64(const GemmDesc *__restrict__ descs, int tiles_n)
 // launch that asks for it (split_k), a 64 x 64 tile with at most 32 rows or
 // 48 columns of its own splits K over the spare warps (fixed slice order,
 // deterministic).
-constexpr int kTnStages = 3;
+#ifndef GEMM_TN_STAGES
+#define GEMM_TN_STAGES 3      // four measured slower on the projection
+#endif
+constexpr int kTnStages = GEMM_TN_STAGES;
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem, bool pred)
 {
